@@ -1,0 +1,2 @@
+// Empty host stand-in for a Poplar header (oracle shim, test infrastructure only).
+#pragma once
