@@ -1,0 +1,465 @@
+"""Benchmark: bit-exact GCUPS of the batched affine-gap Smith-Waterman engine.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
+    python bench.py --impl reference ...
+
+One step = one pass of the engine over the whole synthetic batch (default:
+1,000,000 DNA pairs, |A| ~ U[50,250], |B| lognormal median 300 clipped to
+[100, 1000], +1/-1, gap open/extend 1/1, forward pass, score + end
+coordinates).  `value` times the persistent cost-binned engine on
+device-resident inputs (ipuma_gpu_compare_device); `e2e` times the host-buffer
+C ABI call ipuma_gpu_compare with pinned inputs and outputs, copies included.
+`plain` times the one-launch-per-batch kernel on the same pairs laid out in
+the reference wire format.  Multi-GPU runs are weak scaling: every rank
+aligns its own batch, no collective on the data path.
+
+`--impl reference` times the reference's CPU implementation of the path
+(its vendored StripedSmithWaterman library driven like its cpusw benchmark,
+oracle/_ref/libref_ssw.so, all host threads) on bounded samples.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "ipuma-lib_b200", "python"))
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+
+LANE_OPS_PER_CELL = 7  # E: 2, F: 2, H: 2, running max: 1 (int lane-ops)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="dna_batched",
+                    choices=["dna_plain", "dna_batched", "protein", "protein_mixed"])
+    ap.add_argument("--pairs", type=int, default=0, help="override the pair count")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def make_workload(name, pairs, seed_offset=0):
+    import workloads
+    fn = workloads.CONFIGS[name]
+    kw = {}
+    if pairs:
+        kw["n"] = pairs
+    base_seed = {"dna_plain": 1000, "dna_batched": 1001, "protein": 1002, "protein_mixed": 1003}[name]
+    return fn(seed=base_seed + seed_offset, **kw)
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def algorithmic_bytes(wl):
+    """Bytes a launch must move: packed sequences (2-bit DNA, 5-bit protein),
+    16 B of pair descriptor in and 12 B of results out per pair."""
+    bits = 2 if wl.datatype == "na" else 5
+    seq = (wl.a_len.astype(np.int64) + wl.b_len.astype(np.int64)) * bits / 8.0
+    return float(seq.sum() + wl.n * (16 + 12))
+
+
+def build_wire(wl, max_batches=128):
+    """Reference wire buffer (Seqs || Meta) with `max_batches` consecutive
+    pairs per tile and bufsize = the largest tile's bytes."""
+    n = wl.n
+    tiles = (n + max_batches - 1) // max_batches
+    need = (wl.a_len.astype(np.int64) + wl.b_len.astype(np.int64))
+    tile_of = np.arange(n) // max_batches
+    slot = np.arange(n) % max_batches
+    tile_bytes = np.bincount(tile_of, weights=need, minlength=tiles).astype(np.int64)
+    bufsize = int(((tile_bytes.max() + 15) // 16) * 16)
+    words_per_tile = (bufsize + 3) // 4
+    inputs = np.zeros(tiles * words_per_tile + tiles * max_batches * 4, dtype=np.int32)
+    seq = inputs[: tiles * words_per_tile].view(np.uint8)
+    start_in_tile = np.cumsum(need) - need - np.repeat(
+        np.concatenate([[0], np.cumsum(tile_bytes)[:-1]]), np.bincount(tile_of, minlength=tiles))
+    a_pos = tile_of * (words_per_tile * 4) + start_in_tile
+    b_pos = a_pos + wl.a_len
+    import workloads as w
+    a_codes = w._gather(wl.codes, wl.a_off, wl.a_len)
+    b_codes = w._gather(wl.codes, wl.b_off, wl.b_len)
+    def scatter(pos, ln, src):
+        ln = ln.astype(np.int64)
+        idx = np.repeat(pos - np.concatenate([[0], np.cumsum(ln)[:-1]]), ln) + np.arange(int(ln.sum()))
+        seq[idx] = src
+    scatter(a_pos, wl.a_len, a_codes)
+    scatter(b_pos, wl.b_len, b_codes)
+    meta = inputs[tiles * words_per_tile:].reshape(tiles * max_batches, 4)
+    g = tile_of * max_batches + slot
+    meta[g, 0] = wl.a_len
+    meta[g, 1] = start_in_tile
+    meta[g, 2] = wl.b_len
+    meta[g, 3] = start_in_tile + wl.a_len
+    return tiles, max_batches, bufsize, inputs, g
+
+
+def cpu_baseline(wl, seconds, sw):
+    """The reference codelet compiled for the host (oracle/_ref), all cores,
+    on a bounded sample of the same workload (or the oracle port if the
+    reference library is absent)."""
+    import oracle
+    sim = oracle.select_matrix(wl.similarity, wl.match, wl.mismatch, wl.ambiguity)
+    use_ref = oracle.have_ref()
+    cores = os.cpu_count() or 1
+    run = (lambda sub: oracle.ref_codelet_pairs(sub.codes, sub.a_off, sub.a_len, sub.b_off,
+                                                sub.b_len, sim, wl.gap_init, wl.gap_extend,
+                                                forward_only=True, nthreads=cores)) if use_ref else \
+          (lambda sub: oracle.sw_batch(sub.codes, sub.a_off, sub.a_len, sub.b_off, sub.b_len, sim,
+                                       wl.gap_init, wl.gap_extend, forward_only=True,
+                                       nthreads=cores))
+    rng = np.random.default_rng(99)
+    idx = rng.choice(wl.n, size=min(wl.n, 2000), replace=False)
+    cal = wl.subset(np.sort(idx))
+    t0 = time.perf_counter()
+    run(cal)
+    dt = time.perf_counter() - t0
+    rate = cal.cells / max(dt, 1e-6)
+    target = max(int(rate * seconds), cal.cells)
+    frac = min(1.0, target / wl.cells)
+    m = max(1, int(wl.n * frac))
+    idx = np.sort(rng.choice(wl.n, size=m, replace=False))
+    sub = wl.subset(idx)
+    t0 = time.perf_counter()
+    run(sub)
+    dt = time.perf_counter() - t0
+    return {"value": sub.cells / dt / 1e9, "unit": "GCUPS", "cores": cores,
+            "kind": "reference" if use_ref else "port",
+            "sample": "%d of %d pairs drawn uniformly (%.3g cells, %.1f s), forward pass; %s" % (
+                m, wl.n, sub.cells, dt,
+                "reference SWAffine codelet compiled for the host, OpenMP over pair chunks"
+                if use_ref else "oracle restatement (C), OpenMP over pairs")}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    import oracle
+    if not oracle.have_ssw():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libref_ssw.so not built (needs the reference tree at build time)"}))
+        return 0
+    wl = make_workload(args.workload, args.pairs)
+    sim = oracle.select_matrix(wl.similarity, wl.match, wl.mismatch, wl.ambiguity)
+    gap_open = -(wl.gap_init + wl.gap_extend)
+    gap_ext = -wl.gap_extend
+    cores = os.cpu_count() or 1
+    rng = np.random.default_rng(7)
+    # calibrate a per-step sample of ~4 s
+    cal = wl.subset(np.sort(rng.choice(wl.n, size=min(wl.n, 4000), replace=False)))
+    t0 = time.perf_counter()
+    oracle.ref_ssw_pairs(cal.codes, cal.a_off, cal.a_len, cal.b_off, cal.b_len, sim, gap_open,
+                         gap_ext, report_begin=False, nthreads=cores)
+    rate = cal.cells / max(time.perf_counter() - t0, 1e-6)
+    m = max(1000, min(wl.n, int(wl.n * min(1.0, rate * 4.0 / wl.cells))))
+    subs = [wl.subset(np.sort(rng.choice(wl.n, size=m, replace=False)))
+            for _ in range(min(3, args.steps + args.warmup))]
+    times, cells = [], []
+    for k in range(args.warmup + args.steps):
+        sub = subs[k % len(subs)]
+        t0 = time.perf_counter()
+        oracle.ref_ssw_pairs(sub.codes, sub.a_off, sub.a_len, sub.b_off, sub.b_len, sim,
+                             gap_open, gap_ext, report_begin=False, nthreads=cores)
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            times.append(dt)
+            cells.append(sub.cells)
+    value = sum(cells) / sum(times) / 1e9
+    line = {
+        "impl": "reference", "metric": "bit-exact GCUPS (forward pass, score + end coordinates)",
+        "value": value, "unit": "GCUPS", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16/int32",
+        "data": "synthetic", "config": {"workload": wl.name, "pairs": wl.n, "cells": wl.cells,
+                                        "sample_pairs_per_step": m},
+        "cpu_baseline": {"value": value, "unit": "GCUPS", "cores": cores, "kind": "reference",
+                         "sample": "%d of %d pairs per step; reference StripedSmithWaterman "
+                                   "(extern/include/ssw) driven like cpusw/aligners.hpp, "
+                                   "ssw_init per pair, %d threads" % (m, wl.n, cores)},
+        "e2e": {"value": value, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import ipuma_b200 as ib
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+
+    wl = make_workload(args.workload, args.pairs, seed_offset=rank)
+    sw = ib.sw_config(wl.gap_init, wl.gap_extend, wl.match, wl.mismatch, wl.ambiguity,
+                      wl.similarity, wl.datatype)
+    eng = ib.Engine(sw, ib.algo_config(forward_only=True), device=local)
+    pairs_np = ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len)
+    d_codes = torch.from_numpy(wl.codes).to(dev)
+    d_pairs = torch.from_numpy(pairs_np.view(np.uint8)).to(dev)
+    d_out = torch.zeros(3, wl.n, dtype=torch.int32, device=dev)
+    max_a, max_b = int(wl.a_len.max()), int(wl.b_len.max())
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        eng.compare_device(d_codes.data_ptr(), d_codes.numel(), d_pairs.data_ptr(), wl.n, max_a,
+                           max_b, d_out[0].data_ptr(), d_out[1].data_ptr(), d_out[2].data_ptr(),
+                           stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    launches_per_step = eng.stats().launches
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    total_cells = wl.cells * ws
+    value = total_cells / (ms_step * 1e-3) / 1e9
+
+    # Per-launch timing of one extra step (outside the timed region).
+    eng.set_option("time_launches", 1)
+    step()
+    st = eng.stats()
+    eng.set_option("time_launches", 0)
+    timed = [(ib.KERNEL_NAMES.get(st.timed_kind[k], str(st.timed_kind[k])), st.timed_ms[k],
+              st.timed_cells[k]) for k in range(st.n_timed)]
+    dom = max(timed, key=lambda x: x[1]) if timed else None
+
+    # Parity of the timed results: a sample against the oracle (bit-exact).
+    import oracle
+    got = d_out.cpu().numpy()
+    rng = np.random.default_rng(3)
+    chk = np.sort(rng.choice(wl.n, size=min(wl.n, 3000), replace=False))
+    sub = wl.subset(chk)
+    sim = oracle.select_matrix(wl.similarity, wl.match, wl.mismatch, wl.ambiguity)
+    want = oracle.sw_batch(sub.codes, sub.a_off, sub.a_len, sub.b_off, sub.b_len, sim,
+                           wl.gap_init, wl.gap_extend, forward_only=True)
+    mism = int(sum((got[k][chk] != want[k]).sum() for k in range(3)))
+
+    result = {}
+    # Plain one-launch-per-batch kernel on the same pairs (wire format).
+    if not args.no_plain:
+        tiles, mb, bufsize, inputs, slot_of = build_wire(wl)
+        algo = ib.algo_config(tiles_used=tiles, max_batches=mb, bufsize=bufsize, max_ab=max_a,
+                              forward_only=True)
+        peng = ib.Engine(sw, algo, device=local)
+        d_in = torch.from_numpy(inputs).to(dev)
+        d_res = torch.zeros(3 * tiles * mb, dtype=torch.int32, device=dev)
+        res = {}
+        for sched in (1, 0):
+            peng.set_option("scheduler", sched)
+            for _ in range(max(1, args.warmup)):
+                peng.run_buffer_device(d_in.data_ptr(), d_in.numel(), d_res.data_ptr(),
+                                       d_res.numel(), stream.cuda_stream)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            reps = max(1, min(args.steps, 5))
+            e0.record(stream)
+            for _ in range(reps):
+                peng.run_buffer_device(d_in.data_ptr(), d_in.numel(), d_res.data_ptr(),
+                                       d_res.numel(), stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            pms = e0.elapsed_time(e1) / reps
+            r = d_res.cpu().numpy()
+            total = tiles * mb
+            same = all(np.array_equal(r[k * total + slot_of], got[k]) for k in range(3))
+            res[sched] = {"gcups": wl.cells / (pms * 1e-3) / 1e9, "ms_per_batch": pms,
+                          "bit_identical_to_pair_api": bool(same)}
+        result["plain"] = {"kernel": "k_plain (one launch per batch, warp per comparison slot, "
+                                     "s32 lanes, static slot order)",
+                           "gcups": res[1]["gcups"], "ms_per_batch": res[1]["ms_per_batch"],
+                           "bit_identical_to_batched": res[1]["bit_identical_to_pair_api"],
+                           "wire_layout": {"tiles": tiles, "max_batches": mb, "bufsize": bufsize},
+                           "batched_on_wire_gcups": res[0]["gcups"],
+                           "speedup_batched_vs_plain": value / ws / res[1]["gcups"]}
+        del d_in, d_res
+        peng.close()
+
+    # End to end through the host-buffer C ABI call, pinned host memory.
+    e2e = None
+    if not args.no_e2e:
+        h_codes = torch.from_numpy(wl.codes).pin_memory()
+        h_pairs = torch.from_numpy(pairs_np.view(np.uint8)).pin_memory()
+        h_out = torch.zeros(3, wl.n, dtype=torch.int32).pin_memory()
+        codes_np = h_codes.numpy()
+        pairs_view = h_pairs.numpy().view(ib.PAIR_DTYPE)
+        out_np = h_out.numpy()
+        for _ in range(max(1, args.warmup)):
+            eng.compare_into(codes_np, pairs_view, out_np[0], out_np[1], out_np[2])
+        if dist:
+            dist.barrier()
+        reps = max(1, min(args.steps, 5))
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            eng.compare_into(codes_np, pairs_view, out_np[0], out_np[1], out_np[2])
+        wall = (time.perf_counter() - t0) / reps
+        if dist:
+            t = torch.tensor([wall], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            wall = float(t.item())
+        e2e_same = bool(np.array_equal(out_np, got))
+        e2e = {"value": total_cells / wall / 1e9, "unit": "GCUPS",
+               "h2d_bytes_per_step": int(wl.codes.nbytes + pairs_np.nbytes),
+               "d2h_bytes_per_step": int(3 * 4 * wl.n), "ms_per_step": wall * 1e3,
+               "bit_identical_to_device_run": e2e_same,
+               "timing": "host wall clock around ipuma_gpu_compare (validation, H2D, kernels, D2H)"}
+
+    peaks, peak_src = measured_peaks()
+    int_peak = ib.measure_int_peak(local)
+    rl = None
+    if dom:
+        name, dms, dcells = dom
+        achieved = dcells * LANE_OPS_PER_CELL / (dms * 1e-3) / 1e9
+        rl = {"bound": "int_issue", "kernel": name, "achieved": achieved,
+              "peak": int_peak / 1e9, "unit": "G int lane-ops/s", "frac": achieved * 1e9 / int_peak,
+              "per_unit": "%d lane-ops per cell; %d cells in this launch" % (LANE_OPS_PER_CELL, dcells),
+              "launch_ms": dms, "peak_source": "ipuma_measure_int_peak (s16x2 DPX mix, this GPU)",
+              "traffic": None}
+    algo_bytes = algorithmic_bytes(wl)
+    roof_hbm = {"bound": "hbm", "achieved": algo_bytes / (ms_step * 1e-3) / 1e9,
+                "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                "frac": algo_bytes / (ms_step * 1e-3) / 1e9 / peaks.get("hbm_gbs", 1.0),
+                "traffic": None, "peak_source": peak_src,
+                "per_unit": "packed sequence bytes + 28 B per pair"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(wl, args.cpu_seconds, sw)
+
+    if rank == 0:
+        line = {
+            "metric": "bit-exact GCUPS (forward pass, score + end coordinates)",
+            "value": value, "unit": "GCUPS", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "s16x2 (int32 rerun)",
+            "data": "synthetic",
+            "config": {"workload": wl.name, "pairs_per_gpu": wl.n, "cells_per_gpu": wl.cells,
+                       "seed": wl.seed, "scoring": "%s match %d mismatch %d gapInit %d gapExtend %d"
+                       % (wl.similarity, wl.match, wl.mismatch, wl.gap_init, wl.gap_extend),
+                       "l2": "inputs larger than L2 (%.0f MB codes per GPU)" % (wl.codes.nbytes / 1e6),
+                       "engine": "persistent cost-binned (compare_device)"},
+            "e2e": e2e,
+            "gpu_launches": launches_per_step * args.steps,
+            "roofline": rl,
+            "roofline_hbm": roof_hbm,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "parity": {"checked_pairs": int(chk.size), "mismatching_fields": mism,
+                       "against": "oracle (C restatement of SWAffine::compute)"},
+            "launch_breakdown_ms": [{"kernel": n, "ms": m, "cells": c} for n, m, c in timed],
+        }
+        line.update(result)
+        print(json.dumps(line))
+    eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

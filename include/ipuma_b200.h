@@ -1,0 +1,218 @@
+/*
+ * ipuma_b200.h -- C ABI of the B200 batched Smith-Waterman (Gotoh) engine.
+ *
+ * Plain C: POD structs, raw pointers and sizes; no exceptions cross it.
+ * Every entry point returns IPUMA_OK (0) or a negative IPUMA_ERR_* code;
+ * ipuma_last_error() returns the message of the last failure on the calling
+ * thread.  The C++ drop-in layer (ipuma-lib_b200/host, namespace ipu) is
+ * built on these calls and rethrows failures as std::runtime_error with the
+ * reference's messages.
+ *
+ * Reference interfaces replaced (paths relative to the ipuma-lib tree):
+ *   ipuma_sw_config         ipu::SWConfig              src/ipu_config.h:11-19
+ *   ipuma_algo_config       ipu::IPUAlgoConfig         src/ipu_config.h:21-42
+ *   ipuma_gpu_create        SWAlgorithm::SWAlgorithm   src/ipu_batch_affine.cpp:372-403
+ *                           (device attach ipu_base.cpp:127-148, engine build
+ *                           ipu_batch_affine.cpp:388-400, executor :992-1012)
+ *   ipuma_gpu_destroy       SWAlgorithm::~SWAlgorithm  src/ipu_batch_affine.cpp:1014-1022
+ *   ipuma_gpu_run_buffer    prepared_remote_compare    src/ipu_batch_affine.cpp:558-562
+ *                           (one engine run over the Seqs||Meta wire buffer,
+ *                           FillCallback/RecvCallback :32-144, program :340-355)
+ *   ipuma_gpu_submit_buffer async_submit_prepared_remote_compare  :496-506
+ *   ipuma_gpu_join          blocking_join_prepared_remote_compare :508-556
+ *   ipuma_gpu_poll          (non-blocking form of Job::join, :489-494)
+ *   ipuma_gpu_compare       compare_local minus the host partitioning
+ *                           (:564-663): pairs straight from a code array
+ *   ipuma_gpu_compare_device  the same with device-resident buffers
+ *   ipuma_encode            swatlib::Encoding::encode  src/swatlib/encoding.cpp:38-60
+ *   ipuma_select_matrix     swatlib::selectMatrix      src/swatlib/similarity.cpp:89-105
+ */
+#ifndef IPUMA_B200_H
+#define IPUMA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define IPUMA_OK 0
+#define IPUMA_ERR_INVALID_ARG -1   /* bad pointer, size or config value     */
+#define IPUMA_ERR_CUDA -2          /* a CUDA runtime call failed            */
+#define IPUMA_ERR_NO_DEVICE -3     /* no usable CUDA device                 */
+#define IPUMA_ERR_TOO_LONG -4      /* a sequence exceeds a stated maximum   */
+#define IPUMA_ERR_OUT_OF_BUCKETS -5 /* partitioning capacity exhausted      */
+#define IPUMA_ERR_BAD_SEQUENCE -6  /* a character has no code in the alphabet */
+#define IPUMA_ERR_TIMEOUT -7       /* a bounded wait expired                */
+#define IPUMA_ERR_NO_MEMORY -8     /* admission refused: not enough memory  */
+#define IPUMA_ERR_UNKNOWN_JOB -9   /* job id not issued by this engine      */
+#define IPUMA_ERR_DEVICE -10       /* a kernel reported an error status     */
+#define IPUMA_ERR_CLOSED -11       /* engine or queue already closed        */
+
+/* ---- enums, numbered like the reference's ------------------------------ */
+/* swatlib::Similarity (src/swatlib/similarity.h:108-113) */
+#define IPUMA_SIM_NUCLEIC_ACID 0
+#define IPUMA_SIM_BLOSUM50 1
+#define IPUMA_SIM_BLOSUM62 2
+#define IPUMA_SIM_SIMPLE 3
+/* swatlib::DataType (src/swatlib/encoding.h:12-16) */
+#define IPUMA_DT_NUCLEIC_ACID 0
+#define IPUMA_DT_AMINO_ACID 1
+#define IPUMA_DT_STRING 2
+/* ipu::VertexType (src/types.h:19) -- accepted, all compute the same result */
+#define IPUMA_VTYPE_CPP 0
+#define IPUMA_VTYPE_ASSEMBLY 1
+#define IPUMA_VTYPE_MULTI 2
+#define IPUMA_VTYPE_MULTIASM 3
+/* ipu::Algorithm (src/types.h:21) -- host bucket policy of prepare_remote */
+#define IPUMA_FILL_FIRST 0
+#define IPUMA_FILL_ROUND_ROBIN 1
+#define IPUMA_FILL_GREEDY 2
+
+/* ---- configuration ------------------------------------------------------ */
+/* ipu::SWConfig (src/ipu_config.h:11-19); defaults 0, -1, 1, -1, -1, NA, NA. */
+typedef struct ipuma_sw_config {
+  int32_t gap_init;
+  int32_t gap_extend;
+  int32_t match_value;
+  int32_t mismatch_value;
+  int32_t ambiguity_value;
+  int32_t similarity; /* IPUMA_SIM_* */
+  int32_t datatype;   /* IPUMA_DT_*  */
+} ipuma_sw_config;
+
+/* ipu::IPUAlgoConfig (src/ipu_config.h:21-42); defaults 1, 300, 20, 3000,
+ * cpp, fillFirst, false, false, 1, 0.  tiles_used * max_batches comparison
+ * slots and bufsize bytes of sequence per tile define the wire buffer of
+ * ipuma_gpu_run_buffer; the other API ignores the layout fields. */
+typedef struct ipuma_algo_config {
+  int32_t tiles_used;
+  int32_t max_ab;
+  int32_t max_batches;
+  int32_t bufsize;
+  int32_t vtype;
+  int32_t fill_algo;
+  int32_t forward_only;
+  int32_t use_remote_buffer;
+  int32_t transmission_programs;
+  int32_t io_tiles;
+} ipuma_algo_config;
+
+/* One comparison of the pair API: A = codes[a_off .. a_off + a_len), B likewise.
+ * Codes are the swatlib codes of the engine's datatype (ipuma_encode). */
+typedef struct ipuma_pair {
+  int64_t a_off;
+  int64_t b_off;
+  int32_t a_len;
+  int32_t b_len;
+} ipuma_pair;
+
+/* Timing and work counters of the last completed call on an engine. */
+typedef struct ipuma_stats {
+  double kernel_ms;     /* device time of the alignment kernels (CUDA events) */
+  double total_ms;      /* device time including copies                      */
+  int64_t cells;        /* sum of |A|*|B| (forward pass, ipuma's definition) */
+  int64_t pairs;
+  int64_t s32_pairs;    /* pairs aligned in exact 32-bit lanes               */
+  int64_t overflow_reruns; /* s16x2 pairs that were rerun in 32-bit          */
+  int32_t launches;     /* kernels launched by the call                      */
+  int32_t used_graph;   /* 1 when the call replayed a captured CUDA graph     */
+  /* With option "time_launches" = 1: device time and forward-pass cells of
+   * each alignment-kernel launch of the call, in launch order. */
+  int32_t n_timed;
+  int32_t timed_kind[8];   /* IPUMA_KERNEL_* */
+  double timed_ms[8];
+  int64_t timed_cells[8];
+} ipuma_stats;
+
+/* Kernel kinds reported in ipuma_stats.timed_kind. */
+#define IPUMA_KERNEL_S32_K16 0     /* s32 lanes, 16 columns per lane        */
+#define IPUMA_KERNEL_S16_K16 1     /* s16x2 lanes (2 pairs), 16 columns     */
+#define IPUMA_KERNEL_S16_K8 2
+#define IPUMA_KERNEL_S16_K4 3
+#define IPUMA_KERNEL_S32_RERUN 4   /* s32 rerun of s16x2 give-ups           */
+#define IPUMA_KERNEL_PLAIN 5       /* one-launch-per-batch wire kernel      */
+#define IPUMA_KERNEL_EXACT 6       /* per-thread exact kernel               */
+
+typedef struct ipuma_engine ipuma_engine;
+
+/* ---- library ------------------------------------------------------------ */
+const char* ipuma_last_error(void);
+const char* ipuma_version(void);
+/* Number of CUDA devices (0 when none is usable). */
+int32_t ipuma_device_count(void);
+
+/* Host-only helpers (no GPU needed). */
+/* Encodes n chars into codes; unknown NA characters (code 16, which has no
+ * row in the 16x16 NA matrix) are rejected with IPUMA_ERR_BAD_SEQUENCE. */
+int ipuma_encode(int32_t datatype, const char* s, size_t n, uint8_t* out);
+/* Writes the m x n substitution matrix (row = A code, column = B code). */
+int ipuma_select_matrix(int32_t similarity, int32_t match, int32_t mismatch, int32_t ambiguity,
+                        int8_t* out, size_t out_cap, int32_t* m, int32_t* n);
+/* Size of the wire input buffer in int32 words
+ * (IPUAlgoConfig::getInputBufferSize32b, src/ipu_config.cpp:6-14). */
+int64_t ipuma_input_buffer_words(const ipuma_algo_config* algo);
+
+/* ---- engine ------------------------------------------------------------- */
+int ipuma_gpu_create(const ipuma_sw_config* sw, const ipuma_algo_config* algo, int32_t device,
+                     ipuma_engine** out);
+void ipuma_gpu_destroy(ipuma_engine* e);
+
+/* Engine options (names and values documented in INTEGRATION.md):
+ *   "scheduler"   0 = persistent cost-binned engine (default), 1 = plain
+ *                 one-launch-per-batch kernel (wire-buffer API only)
+ *   "graphs"      1 = capture and replay CUDA graphs for repeated shapes
+ *   "tile_k"      force the columns-per-lane of the wavefront kernels
+ *   "time_launches" 1 = time every alignment-kernel launch (ipuma_stats) */
+int ipuma_gpu_set_option(ipuma_engine* e, const char* name, int64_t value);
+
+/* Runs one batch in the reference wire format and waits for it.
+ *   inputs  : n_inputs int32 = Seqs (tiles_used x ceil(bufsize/4) words of
+ *             uint8 codes) || Meta (tiles_used x max_batches x {a_len, a_off,
+ *             b_len, b_off}), as written by SWAlgorithm::prepare_remote
+ *   results : n_results = 3 * tiles_used * max_batches int32 =
+ *             scores || a_ranges || b_ranges, indexed tile*max_batches+slot;
+ *             ranges pack start | end << 16 (uint16 halves). */
+int ipuma_gpu_run_buffer(ipuma_engine* e, const int32_t* inputs, size_t n_inputs, int32_t* results,
+                         size_t n_results);
+/* Asynchronous form: the buffers must stay valid until ipuma_gpu_join. */
+int ipuma_gpu_submit_buffer(ipuma_engine* e, const int32_t* inputs, size_t n_inputs,
+                            int32_t* results, size_t n_results, uint64_t* job);
+/* *done = 1 once the job's results are in place (results are only
+ * guaranteed after ipuma_gpu_join). */
+int ipuma_gpu_poll(ipuma_engine* e, uint64_t job, int32_t* done);
+/* Waits for a job (bounded by timeout_ms; < 0 waits without limit). */
+int ipuma_gpu_join(ipuma_engine* e, uint64_t job, int64_t timeout_ms);
+
+/* Aligns n pairs from host memory; results in input order. */
+int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes,
+                      const ipuma_pair* pairs, int32_t n, int32_t* score, int32_t* arange,
+                      int32_t* brange);
+/* Same with every buffer in device memory, enqueued on `stream`
+ * (cudaStream_t, NULL = the engine's stream); max_a_len / max_b_len bound
+ * the pair lengths (checked on the device). */
+int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_codes,
+                             const ipuma_pair* d_pairs, int32_t n, int32_t max_a_len,
+                             int32_t max_b_len, int32_t* d_score, int32_t* d_arange,
+                             int32_t* d_brange, void* stream);
+
+/* Wire-buffer batch with inputs and results already in device memory,
+ * enqueued on `stream` (NULL = the engine's stream); the call returns once
+ * the batch has finished.  Sizes as for ipuma_gpu_run_buffer; the Meta
+ * section is validated on the device. */
+int ipuma_gpu_run_buffer_device(ipuma_engine* e, const int32_t* d_inputs, size_t n_inputs,
+                                int32_t* d_results, size_t n_results, void* stream);
+
+int ipuma_gpu_last_stats(ipuma_engine* e, ipuma_stats* out);
+
+/* Measures, on `device`, the issue rate of the s16x2 instruction mix of one
+ * cell update (3 add, 2 viaddmax, 1 vimax3.relu, 1 max) in lane-ops per
+ * second: the peak against which the kernels' roofline fraction is taken. */
+int ipuma_measure_int_peak(int32_t device, double* lane_ops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IPUMA_B200_H */

@@ -1,0 +1,827 @@
+// engine.cu -- the C ABI of include/ipuma_b200.h: engine lifecycle, device
+// buffers, the cost-binned scheduling pipeline and the kernel launches.
+//
+// One engine = one CUDA device + one stream.  Calls on an engine are
+// serialised by its mutex; device buffers grow on demand and are reused.
+// Jobs (ipuma_gpu_submit_buffer) are stream-ordered and tracked by events.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "ipuma_b200.h"
+#include "sw_kernels.cuh"
+#include "../host/swatlib/encoding.h"
+#include "../host/swatlib/similarity.h"
+
+using namespace ipuma_dev;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                   \
+  do {                                                                                   \
+    cudaError_t _e = (expr);                                                             \
+    if (_e != cudaSuccess)                                                               \
+      return fail(IPUMA_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(_e));       \
+  } while (0)
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes, cudaStream_t s) {
+    if (bytes <= cap && p) return IPUMA_OK;
+    if (p) {
+      cudaStreamSynchronize(s);
+      cudaFree(p);
+      p = nullptr;
+      cap = 0;
+    }
+    size_t want = std::max<size_t>(bytes, 256);
+    want = (want + (1u << 20) - 1) & ~(size_t)((1u << 20) - 1);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return fail(IPUMA_ERR_NO_MEMORY, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
+    }
+    cap = want;
+    return IPUMA_OK;
+  }
+  template <class T>
+  T* as() const {
+    return reinterpret_cast<T*>(p);
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+// Columns per lane of the s16x2 classes and their |A| limits.
+constexpr int kS16K[3] = {4, 8, 16};
+constexpr int kS32K = 16;
+constexpr int kWarpsPerBlock = 4;
+constexpr int kThreads = 32 * kWarpsPerBlock;
+
+struct Job {
+  cudaEvent_t done = nullptr;
+  bool finished = false;
+};
+
+}  // namespace
+
+struct ipuma_engine {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int nsm = 0;
+  ipuma_sw_config sw{};
+  ipuma_algo_config algo{};
+  std::vector<int8_t> sim;
+  int M = 0;
+  int maxSub = 0;
+  SwConst sc{};
+  bool fast_ok = false;  // wavefront kernels valid for this scoring
+  bool s16_ok = false;   // s16x2 lanes valid for this scoring
+  int s16_max_len = 0;
+
+  // options
+  int scheduler = 0;
+  int graphs = 0;
+  int tile_k = 0;
+  int time_launches = 0;
+
+  // per-launch timing of the current call (time_launches)
+  cudaEvent_t tev[2 * 8] = {};
+  int n_timed = 0;
+  int timed_kind[8] = {};
+  int timed_cls[8] = {};
+
+  DevBuf d_sim, d_codes, d_pairs, d_list, d_res, d_scratch, d_cf, d_ovf, d_ctl, d_inputs, d_wres, d_flag;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  ipuma_stats stats{};
+  std::mutex mu;
+  std::map<uint64_t, Job> jobs;
+  uint64_t next_job = 1;
+};
+
+namespace {
+
+// Layout of the control block (ints): status, class ranges, queue heads,
+// histogram, offsets.
+constexpr int CTL_STATUS = 0;                       // DevStatus (4 ints)
+constexpr int CTL_RANGES = 4;                       // 2 * NCLASS_MAX
+constexpr int CTL_HEADS = CTL_RANGES + 2 * NCLASS_MAX;  // NCLASS_MAX + 1
+constexpr int CTL_INFO = 30;                        // wire check {maxA, maxB, bad} (+1 pad)
+constexpr int CTL_CELLS = 34;                       // 8-byte aligned: NCLASS_MAX + 2 uint64
+constexpr int CTL_HIST = CTL_CELLS + 2 * (NCLASS_MAX + 2);  // NCLASS_MAX * NBUCKET
+constexpr int CTL_OFFS = CTL_HIST + NCLASS_MAX * NBUCKET;
+constexpr int CTL_INTS = CTL_OFFS + NCLASS_MAX * NBUCKET;
+constexpr int CELLS_RERUN = NCLASS_MAX;             // index of the rerun cells
+constexpr int CELLS_WIRE = NCLASS_MAX + 1;          // cells found by the wire check
+
+template <class K>
+int occupancy_grid(ipuma_engine* e, K kernel, int smem) {
+  int nb = 0;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, kThreads, smem);
+  if (nb < 1) nb = 1;
+  return nb * e->nsm;
+}
+
+template <class T, int K>
+int smem_for(const ipuma_engine* e) {
+  return SmemLayout<T, K>::total(e->M, kWarpsPerBlock);
+}
+
+// Grid of a k_batched<T, K> launch and the warps it runs.
+template <class T, int K>
+int batched_grid(ipuma_engine* e) {
+  return occupancy_grid(e, k_batched<T, K>, smem_for<T, K>(e));
+}
+
+int max_batched_warps(ipuma_engine* e) {
+  int g = 0;
+  g = std::max(g, batched_grid<LaneS16x2, 4>(e));
+  g = std::max(g, batched_grid<LaneS16x2, 8>(e));
+  g = std::max(g, batched_grid<LaneS16x2, 16>(e));
+  g = std::max(g, batched_grid<LaneS32, 16>(e));
+  return g * kWarpsPerBlock;
+}
+
+// Brackets one alignment-kernel launch with events when time_launches is set.
+int timed_begin(ipuma_engine* e, cudaStream_t s, int kind, int cls) {
+  if (!e->time_launches || e->n_timed >= 8) return IPUMA_OK;
+  if (!e->tev[2 * e->n_timed]) {
+    CUDA_TRY(cudaEventCreate(&e->tev[2 * e->n_timed]));
+    CUDA_TRY(cudaEventCreate(&e->tev[2 * e->n_timed + 1]));
+  }
+  e->timed_kind[e->n_timed] = kind;
+  e->timed_cls[e->n_timed] = cls;
+  CUDA_TRY(cudaEventRecord(e->tev[2 * e->n_timed], s));
+  return IPUMA_OK;
+}
+
+int timed_end(ipuma_engine* e, cudaStream_t s) {
+  if (!e->time_launches || e->n_timed >= 8) return IPUMA_OK;
+  CUDA_TRY(cudaEventRecord(e->tev[2 * e->n_timed + 1], s));
+  e->n_timed++;
+  return IPUMA_OK;
+}
+
+template <class T, int K>
+int launch_batched(ipuma_engine* e, cudaStream_t s, const uint8_t* codes, const PairDesc* pairs,
+                   const int* list, const int* range, int* head, long rowsCap, int* score,
+                   int* arange, int* brange, int kind, int cls) {
+  const int smem = smem_for<T, K>(e);
+  const int grid = batched_grid<T, K>(e);
+  int* ctl = e->d_ctl.as<int>();
+  auto* cells = reinterpret_cast<unsigned long long*>(ctl + CTL_CELLS);
+  int rc;
+  if ((rc = timed_begin(e, s, kind, cls))) return rc;
+  k_batched<T, K><<<grid, kThreads, smem, s>>>(
+      e->sc, e->d_sim.as<int8_t>(), codes, pairs, list, range, head, e->d_scratch.as<int2>(),
+      rowsCap, score, arange, brange, e->d_ovf.as<int>(), cells + CELLS_RERUN,
+      reinterpret_cast<DevStatus*>(ctl + CTL_STATUS));
+  CUDA_TRY(cudaGetLastError());
+  return timed_end(e, s);
+}
+
+// Runs the persistent cost-binned pipeline over n device-resident pairs.
+// Results land at score[p], arange[p], brange[p].
+int run_batched(ipuma_engine* e, cudaStream_t s, const uint8_t* codes, const PairDesc* pairs, int n,
+                int maxA, int maxB, int* score, int* arange, int* brange, int* launches) {
+  int rc;
+  if (n <= 0) return IPUMA_OK;
+  int* ctl = e->d_ctl.as<int>();
+  DevStatus* st = reinterpret_cast<DevStatus*>(ctl + CTL_STATUS);
+
+  if (!e->fast_ok) {
+    // Exact per-thread kernel; C and F rows in global scratch.
+    const long maxAcap = std::max(1, maxA);
+    long threads = std::min<long>(n, std::max<long>(1024, (512l << 20) / (8 * maxAcap)));
+    threads = ((threads + 127) / 128) * 128;
+    if ((rc = e->d_cf.ensure(sizeof(int) * 2 * maxAcap * threads, s))) return rc;
+    if ((rc = timed_begin(e, s, IPUMA_KERNEL_EXACT, -1))) return rc;
+    k_exact<<<(int)(threads / 128), 128, 0, s>>>(e->sc, e->d_sim.as<int8_t>(), codes, pairs, n,
+                                                  nullptr, 0, 0, 1, e->d_cf.as<int>(), maxAcap,
+                                                  score, arange, brange);
+    CUDA_TRY(cudaGetLastError());
+    if ((rc = timed_end(e, s))) return rc;
+    *launches += 1;
+    return IPUMA_OK;
+  }
+
+  // Scratch for strip boundaries and the lists.
+  const long rowsCap = std::max(1, maxB);
+  const long warps = max_batched_warps(e);
+  if ((rc = e->d_scratch.ensure(sizeof(int2) * 2 * rowsCap * warps, s))) return rc;
+  if ((rc = e->d_list.ensure(sizeof(int) * (size_t)n + 64, s))) return rc;
+  if ((rc = e->d_ovf.ensure(sizeof(int) * (size_t)n + 64, s))) return rc;
+
+  BinParams bp{};
+  const int ns16 = 3;
+  bp.n_s16_classes = ns16;
+  bp.cls_s32 = ns16;
+  bp.nclass = ns16 + 1;
+  bp.s16_max_len = e->s16_max_len;
+  bp.force_s32 = e->s16_ok ? 0 : 1;
+  for (int c = 0; c < ns16; ++c) bp.k_limit[c] = 32 * kS16K[c];
+  if (e->tile_k > 0) {
+    // Force one s16x2 class: all pairs use the chosen columns per lane.
+    for (int c = 0; c < ns16; ++c) bp.k_limit[c] = (kS16K[c] == e->tile_k) ? (1 << 30) : -1;
+  }
+  bp.max_a = maxA;
+  bp.max_b = maxB;
+  bp.M = e->M;
+  bp.s16_limit = e->sc.s16Limit;
+  if ((rc = e->d_flag.ensure((size_t)n + 64, s))) return rc;
+  const int nkeys = bp.nclass * NBUCKET;
+  const int tb = 256;
+  const int gb = std::min<int>((n + tb - 1) / tb, e->nsm * 8);
+  k_bin_count<<<gb, tb, 0, s>>>(bp, codes, e->d_sim.as<int8_t>(), pairs, n, ctl + CTL_HIST,
+                                e->d_flag.as<uint8_t>(),
+                                reinterpret_cast<unsigned long long*>(ctl + CTL_CELLS), st, score,
+                                arange, brange);
+  k_bin_scan<<<1, 1024, 0, s>>>(nkeys, ctl + CTL_HIST, ctl + CTL_OFFS, ctl + CTL_RANGES);
+  k_bin_scatter<<<gb, tb, 0, s>>>(bp, pairs, n, e->d_flag.as<uint8_t>(), ctl + CTL_OFFS,
+                                  e->d_list.as<int>());
+  CUDA_TRY(cudaGetLastError());
+  *launches += 3;
+
+  int* list = e->d_list.as<int>();
+  int* heads = ctl + CTL_HEADS;
+  // Long-tail first: the s32 class holds the longest high-scoring pairs.
+  if ((rc = launch_batched<LaneS32, kS32K>(e, s, codes, pairs, list, ctl + CTL_RANGES + 2 * 3,
+                                           heads + 3, rowsCap, score, arange, brange,
+                                           IPUMA_KERNEL_S32_K16, 3)))
+    return rc;
+  if ((rc = launch_batched<LaneS16x2, 16>(e, s, codes, pairs, list, ctl + CTL_RANGES + 2 * 2,
+                                          heads + 2, rowsCap, score, arange, brange,
+                                          IPUMA_KERNEL_S16_K16, 2)))
+    return rc;
+  if ((rc = launch_batched<LaneS16x2, 8>(e, s, codes, pairs, list, ctl + CTL_RANGES + 2 * 1,
+                                         heads + 1, rowsCap, score, arange, brange,
+                                         IPUMA_KERNEL_S16_K8, 1)))
+    return rc;
+  if ((rc = launch_batched<LaneS16x2, 4>(e, s, codes, pairs, list, ctl + CTL_RANGES + 2 * 0,
+                                         heads + 0, rowsCap, score, arange, brange,
+                                         IPUMA_KERNEL_S16_K4, 0)))
+    return rc;
+  // Exact 32-bit rerun of the s16x2 pairs whose score may have overflowed.
+  if ((rc = launch_batched<LaneS32, kS32K>(e, s, codes, pairs, e->d_ovf.as<int>(),
+                                           ctl + CTL_STATUS + 1, heads + 4, rowsCap, score,
+                                           arange, brange, IPUMA_KERNEL_S32_RERUN, CELLS_RERUN)))
+    return rc;
+  *launches += 5;
+  return IPUMA_OK;
+}
+
+// Clears the control block at the start of every call.
+int reset_ctl(ipuma_engine* e, cudaStream_t s) {
+  int rc;
+  if ((rc = e->d_ctl.ensure(sizeof(int) * CTL_INTS, s))) return rc;
+  CUDA_TRY(cudaMemsetAsync(e->d_ctl.p, 0, sizeof(int) * CTL_INTS, s));
+  e->n_timed = 0;
+  return IPUMA_OK;
+}
+
+int check_status(ipuma_engine* e, cudaStream_t s) {
+  DevStatus st{};
+  unsigned long long cells[NCLASS_MAX + 2] = {};
+  CUDA_TRY(cudaMemcpyAsync(&st, e->d_ctl.as<int>() + CTL_STATUS, sizeof(st), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(cells, e->d_ctl.as<int>() + CTL_CELLS, sizeof(cells), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  e->stats.overflow_reruns = st.overflow_count;
+  e->stats.n_timed = e->n_timed;
+  for (int k = 0; k < e->n_timed; ++k) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->tev[2 * k], e->tev[2 * k + 1]);
+    e->stats.timed_kind[k] = e->timed_kind[k];
+    e->stats.timed_ms[k] = ms;
+    const int c = e->timed_cls[k];
+    e->stats.timed_cells[k] = (c >= 0 && c < NCLASS_MAX + 2) ? (int64_t)cells[c] : 0;
+  }
+  e->n_timed = 0;
+  if (st.error == ERR_LENGTH) return fail(IPUMA_ERR_TOO_LONG, "a pair exceeds the stated maximum length");
+  if (st.error) return fail(IPUMA_ERR_DEVICE, "kernel status error %d", st.error);
+  return IPUMA_OK;
+}
+
+int plain_k_for(int maxAB) {
+  if (maxAB <= 128) return 4;
+  if (maxAB <= 256) return 8;
+  return 16;
+}
+
+// Launches the one-launch-per-batch kernel over a wire buffer on the device.
+int run_plain_wire(ipuma_engine* e, cudaStream_t s, const int* d_inputs, long seqWordsPerTile,
+                   long metaOffset, int maxBatches, int totalSlots, int maxB, int* d_results,
+                   int* launches) {
+  int rc;
+  int* ctl = e->d_ctl.as<int>();
+  DevStatus* st = reinterpret_cast<DevStatus*>(ctl + CTL_STATUS);
+  const long rowsCap = std::max(1, maxB);
+  const int K = e->tile_k > 0 ? e->tile_k : plain_k_for(e->algo.max_ab);
+  auto go = [&](auto kern, int smem) -> int {
+    const int grid = occupancy_grid(e, kern, smem);
+    const long warps = (long)grid * kWarpsPerBlock;
+    int r;
+    if ((r = e->d_scratch.ensure(sizeof(int2) * 2 * rowsCap * warps, s))) return r;
+    if ((r = timed_begin(e, s, IPUMA_KERNEL_PLAIN, CELLS_WIRE))) return r;
+    kern<<<grid, kThreads, smem, s>>>(e->sc, e->d_sim.as<int8_t>(), d_inputs, seqWordsPerTile,
+                                      metaOffset, maxBatches, totalSlots, e->d_scratch.as<int2>(),
+                                      rowsCap, d_results, st);
+    CUDA_TRY(cudaGetLastError());
+    return timed_end(e, s);
+  };
+  if (K == 4) rc = go(k_plain<4>, smem_for<LaneS32, 4>(e));
+  else if (K == 8) rc = go(k_plain<8>, smem_for<LaneS32, 8>(e));
+  else rc = go(k_plain<16>, smem_for<LaneS32, 16>(e));
+  *launches += 1;
+  return rc;
+}
+
+int validate_algo(const ipuma_algo_config* a) {
+  if (a->tiles_used < 0 || a->max_batches < 0 || a->bufsize < 0 || a->max_ab < 0)
+    return fail(IPUMA_ERR_INVALID_ARG, "negative size in IPUAlgoConfig");
+  if (a->transmission_programs != 1 && a->transmission_programs != 0)
+    return fail(IPUMA_ERR_INVALID_ARG, "transmissionPrograms other than 1 is not supported");
+  return IPUMA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ipuma_last_error(void) { return g_last_error.c_str(); }
+
+const char* ipuma_version(void) { return "ipuma-b200 0.1 (sm_100a)"; }
+
+int32_t ipuma_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int ipuma_encode(int32_t datatype, const char* s, size_t n, uint8_t* out) {
+  if ((!s || !out) && n) return fail(IPUMA_ERR_INVALID_ARG, "null pointer");
+  if (datatype < 0 || datatype > 2) return fail(IPUMA_ERR_INVALID_ARG, "invalid datatype %d", datatype);
+  const auto enc = swatlib::getEncoder(static_cast<swatlib::DataType>(datatype));
+  const auto table = enc.getCodeTable();
+  for (size_t i = 0; i < n; ++i) {
+    const unsigned char c = static_cast<unsigned char>(s[i]);
+    const uint8_t v = c < 127 ? table[c] : enc.get_terminator();
+    if (datatype == IPUMA_DT_NUCLEIC_ACID && v == 16)
+      return fail(IPUMA_ERR_BAD_SEQUENCE, "character 0x%02x at %zu is not a nucleic-acid code", c, i);
+    out[i] = v;
+  }
+  return IPUMA_OK;
+}
+
+int ipuma_select_matrix(int32_t similarity, int32_t match, int32_t mismatch, int32_t ambiguity,
+                        int8_t* out, size_t out_cap, int32_t* m, int32_t* n) {
+  try {
+    auto mat = swatlib::selectMatrix(static_cast<swatlib::Similarity>(similarity), (int8_t)match,
+                                     (int8_t)mismatch, (int8_t)ambiguity);
+    auto [mm, nn] = mat.shape();
+    if (m) *m = (int32_t)mm;
+    if (n) *n = (int32_t)nn;
+    if (out) {
+      if (out_cap < mm * nn) return fail(IPUMA_ERR_INVALID_ARG, "output too small");
+      std::memcpy(out, mat.data(), mm * nn);
+    }
+  } catch (const std::exception& ex) {
+    return fail(IPUMA_ERR_INVALID_ARG, "%s", ex.what());
+  }
+  return IPUMA_OK;
+}
+
+int64_t ipuma_input_buffer_words(const ipuma_algo_config* a) {
+  if (!a) return 0;
+  const int64_t bufWords = (a->bufsize + 3) / 4;
+  return (int64_t)a->tiles_used * bufWords + (int64_t)a->tiles_used * a->max_batches * 4;
+}
+
+int ipuma_gpu_create(const ipuma_sw_config* sw, const ipuma_algo_config* algo, int32_t device,
+                     ipuma_engine** out) {
+  if (!sw || !algo || !out) return fail(IPUMA_ERR_INVALID_ARG, "null argument");
+  int rc;
+  if ((rc = validate_algo(algo))) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(IPUMA_ERR_NO_DEVICE, "no CUDA device available");
+  }
+  if (device < 0 || device >= ndev) return fail(IPUMA_ERR_NO_DEVICE, "device %d out of range", device);
+  std::unique_ptr<ipuma_engine> e(new ipuma_engine());
+  e->device = device;
+  e->sw = *sw;
+  e->algo = *algo;
+  CUDA_TRY(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10)
+    return fail(IPUMA_ERR_NO_DEVICE, "device %d is sm_%d%d; this library is built for sm_100a",
+                device, prop.major, prop.minor);
+  e->nsm = prop.multiProcessorCount;
+  CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+  for (auto& ev : e->ev) CUDA_TRY(cudaEventCreate(&ev));
+
+  // Substitution matrix (swatlib::selectMatrix, ipu_batch_affine.cpp:390).
+  int32_t m = 0, n = 0;
+  int8_t buf[32 * 32];
+  if ((rc = ipuma_select_matrix(sw->similarity, sw->match_value, sw->mismatch_value,
+                                sw->ambiguity_value, buf, sizeof(buf), &m, &n)))
+    return rc;
+  e->M = m;
+  e->sim.assign(buf, buf + m * n);
+  e->maxSub = 0;
+  int minSub = 0;
+  for (auto v : e->sim) {
+    e->maxSub = std::max<int>(e->maxSub, v);
+    minSub = std::min<int>(minSub, v);
+  }
+  if ((rc = e->d_sim.ensure(e->sim.size(), e->stream))) return rc;
+  CUDA_TRY(cudaMemcpy(e->d_sim.p, e->sim.data(), e->sim.size(), cudaMemcpyHostToDevice));
+
+  const int gI = sw->gap_init, gE = sw->gap_extend;
+  e->sc.gI = gI;
+  e->sc.gE = gE;
+  e->sc.gIgE = gI + gE;
+  e->sc.M = m;
+  e->sc.forwardOnly = algo->forward_only ? 1 : 0;
+  // Wavefront kernels: padding cells must stay below real ones (gI+gE < 0,
+  // gE <= 0) and profile entries sim - (gI+gE) must fit int8.
+  e->fast_ok = (gI + gE < 0) && (gE <= 0) && (e->maxSub - (gI + gE) <= 127) &&
+               (minSub - (gI + gE) >= -128) && (gI + gE > -1000) && (gE > -1000);
+  // s16x2 lanes: H <= 32767 - maxSub guarantees no halfword overflow.
+  e->sc.s16Limit = 32767 - std::max(0, e->maxSub);
+  e->s16_ok = e->fast_ok;
+  e->s16_max_len = e->maxSub > 0 ? (e->sc.s16Limit / e->maxSub) : (1 << 30);
+  *out = e.release();
+  return IPUMA_OK;
+}
+
+void ipuma_gpu_destroy(ipuma_engine* e) {
+  if (!e) return;
+  cudaSetDevice(e->device);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  for (auto& kv : e->jobs)
+    if (kv.second.done) cudaEventDestroy(kv.second.done);
+  for (auto* b : {&e->d_sim, &e->d_codes, &e->d_pairs, &e->d_list, &e->d_res, &e->d_scratch, &e->d_cf,
+                  &e->d_ovf, &e->d_ctl, &e->d_inputs, &e->d_wres, &e->d_flag})
+    b->release();
+  for (auto& ev : e->ev)
+    if (ev) cudaEventDestroy(ev);
+  for (auto& ev : e->tev)
+    if (ev) cudaEventDestroy(ev);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+int ipuma_gpu_set_option(ipuma_engine* e, const char* name, int64_t value) {
+  if (!e || !name) return fail(IPUMA_ERR_INVALID_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(e->mu);
+  const std::string k(name);
+  if (k == "scheduler") {
+    if (value != 0 && value != 1) return fail(IPUMA_ERR_INVALID_ARG, "scheduler must be 0 or 1");
+    e->scheduler = (int)value;
+  } else if (k == "graphs") {
+    e->graphs = value ? 1 : 0;
+  } else if (k == "time_launches") {
+    e->time_launches = value ? 1 : 0;
+  } else if (k == "tile_k") {
+    if (value != 0 && value != 4 && value != 8 && value != 16)
+      return fail(IPUMA_ERR_INVALID_ARG, "tile_k must be 0, 4, 8 or 16");
+    e->tile_k = (int)value;
+  } else {
+    return fail(IPUMA_ERR_INVALID_ARG, "unknown option '%s'", name);
+  }
+  return IPUMA_OK;
+}
+
+int ipuma_gpu_last_stats(ipuma_engine* e, ipuma_stats* out) {
+  if (!e || !out) return fail(IPUMA_ERR_INVALID_ARG, "null argument");
+  *out = e->stats;
+  return IPUMA_OK;
+}
+
+int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_codes,
+                             const ipuma_pair* d_pairs, int32_t n, int32_t max_a_len,
+                             int32_t max_b_len, int32_t* d_score, int32_t* d_arange,
+                             int32_t* d_brange, void* stream) {
+  if (!e) return fail(IPUMA_ERR_INVALID_ARG, "null engine");
+  if (n < 0) return fail(IPUMA_ERR_INVALID_ARG, "negative pair count");
+  if (n > 0 && (!d_codes || !d_pairs || !d_score || !d_arange || !d_brange))
+    return fail(IPUMA_ERR_INVALID_ARG, "null buffer");
+  (void)n_codes;
+  std::lock_guard<std::mutex> lk(e->mu);
+  CUDA_TRY(cudaSetDevice(e->device));
+  cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : e->stream;
+  e->stats = ipuma_stats{};
+  int launches = 0;
+  int rc;
+  if ((rc = reset_ctl(e, s))) return rc;
+  CUDA_TRY(cudaEventRecord(e->ev[1], s));
+  rc = run_batched(e, s, d_codes, reinterpret_cast<const PairDesc*>(d_pairs), n, max_a_len,
+                   max_b_len, d_score, d_arange, d_brange, &launches);
+  if (rc) return rc;
+  CUDA_TRY(cudaEventRecord(e->ev[2], s));
+  if ((rc = check_status(e, s))) return rc;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e->ev[1], e->ev[2]);
+  e->stats.kernel_ms = ms;
+  e->stats.total_ms = ms;
+  e->stats.pairs = n;
+  e->stats.launches = launches;
+  return IPUMA_OK;
+}
+
+int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes, const ipuma_pair* pairs,
+                      int32_t n, int32_t* score, int32_t* arange, int32_t* brange) {
+  if (!e) return fail(IPUMA_ERR_INVALID_ARG, "null engine");
+  if (n < 0) return fail(IPUMA_ERR_INVALID_ARG, "negative pair count");
+  if (n == 0) return IPUMA_OK;
+  if (!codes || !pairs || !score || !arange || !brange) return fail(IPUMA_ERR_INVALID_ARG, "null buffer");
+  // Host-side bounds check of every pair (the kernels trust the descriptors).
+  int maxA = 0, maxB = 0;
+  int64_t cells = 0;
+  for (int32_t p = 0; p < n; ++p) {
+    const ipuma_pair& d = pairs[p];
+    if (d.a_len < 0 || d.b_len < 0 || d.a_off < 0 || d.b_off < 0 ||
+        (size_t)d.a_off + (size_t)d.a_len > n_codes || (size_t)d.b_off + (size_t)d.b_len > n_codes)
+      return fail(IPUMA_ERR_INVALID_ARG, "pair %d lies outside the code array", p);
+    maxA = std::max(maxA, d.a_len);
+    maxB = std::max(maxB, d.b_len);
+    cells += (int64_t)d.a_len * d.b_len;
+  }
+  if (maxA > 65535 || maxB > 65535)
+    return fail(IPUMA_ERR_TOO_LONG, "sequence longer than 65535 (ranges are uint16)");
+  std::lock_guard<std::mutex> lk(e->mu);
+  CUDA_TRY(cudaSetDevice(e->device));
+  cudaStream_t s = e->stream;
+  int rc;
+  if ((rc = e->d_codes.ensure(std::max<size_t>(n_codes, 1), s))) return rc;
+  if ((rc = e->d_pairs.ensure(sizeof(ipuma_pair) * (size_t)n, s))) return rc;
+  if ((rc = e->d_res.ensure(sizeof(int32_t) * 3 * (size_t)n, s))) return rc;
+  e->stats = ipuma_stats{};
+  int launches = 0;
+  if ((rc = reset_ctl(e, s))) return rc;
+  CUDA_TRY(cudaEventRecord(e->ev[0], s));
+  CUDA_TRY(cudaMemcpyAsync(e->d_codes.p, codes, n_codes, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(e->d_pairs.p, pairs, sizeof(ipuma_pair) * (size_t)n, cudaMemcpyHostToDevice, s));
+  int32_t* d_score = e->d_res.as<int32_t>();
+  int32_t* d_ar = d_score + n;
+  int32_t* d_br = d_ar + n;
+  CUDA_TRY(cudaEventRecord(e->ev[1], s));
+  rc = run_batched(e, s, e->d_codes.as<uint8_t>(), e->d_pairs.as<PairDesc>(), n, maxA, maxB, d_score,
+                   d_ar, d_br, &launches);
+  if (rc) return rc;
+  CUDA_TRY(cudaEventRecord(e->ev[2], s));
+  CUDA_TRY(cudaMemcpyAsync(score, d_score, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(arange, d_ar, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(brange, d_br, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaEventRecord(e->ev[3], s));
+  if ((rc = check_status(e, s))) return rc;
+  float kms = 0, tms = 0;
+  cudaEventElapsedTime(&kms, e->ev[1], e->ev[2]);
+  cudaEventElapsedTime(&tms, e->ev[0], e->ev[3]);
+  e->stats.kernel_ms = kms;
+  e->stats.total_ms = tms;
+  e->stats.cells = cells;
+  e->stats.pairs = n;
+  e->stats.launches = launches;
+  return IPUMA_OK;
+}
+
+// Launches the alignment work of a wire buffer already on the device
+// (plain kernel or wire -> pair list -> batched pipeline).
+static int launch_wire(ipuma_engine* e, cudaStream_t s, const int* d_in, int* d_res, int maxA, int maxB,
+                       int* launches) {
+  const ipuma_algo_config& a = e->algo;
+  const long seqWordsPerTile = (a.bufsize + 3) / 4;
+  const long metaOffset = (long)a.tiles_used * seqWordsPerTile;
+  const long totalSlots = (long)a.tiles_used * a.max_batches;
+  int rc;
+  if (totalSlots <= 0) return IPUMA_OK;
+  if (e->scheduler == 1 && e->fast_ok) {
+    return run_plain_wire(e, s, d_in, seqWordsPerTile, metaOffset, a.max_batches, (int)totalSlots, maxB,
+                          d_res, launches);
+  }
+  if ((rc = e->d_pairs.ensure(sizeof(PairDesc) * totalSlots, s))) return rc;
+  const int gb = (int)std::min<long>((totalSlots + 255) / 256, e->nsm * 8);
+  k_wire_to_pairs<<<gb, 256, 0, s>>>(d_in, seqWordsPerTile, metaOffset, a.max_batches, (int)totalSlots,
+                                     e->d_pairs.as<PairDesc>());
+  CUDA_TRY(cudaGetLastError());
+  *launches += 1;
+  return run_batched(e, s, reinterpret_cast<const uint8_t*>(d_in), e->d_pairs.as<PairDesc>(),
+                     (int)totalSlots, maxA, maxB, d_res, d_res + totalSlots, d_res + 2 * totalSlots, launches);
+}
+
+static int check_wire_sizes(const ipuma_algo_config& a, size_t n_inputs, size_t n_results) {
+  const long totalSlots = (long)a.tiles_used * a.max_batches;
+  if ((int64_t)n_inputs != ipuma_input_buffer_words(&a))
+    return fail(IPUMA_ERR_INVALID_ARG, "input buffer has %zu words, config needs %lld", n_inputs,
+                (long long)ipuma_input_buffer_words(&a));
+  if ((long)n_results != 3 * totalSlots) return fail(IPUMA_ERR_INVALID_ARG, "Results buffer not 3 aligned.");
+  if (totalSlots > 0x7fffffffL) return fail(IPUMA_ERR_INVALID_ARG, "too many comparison slots");
+  return IPUMA_OK;
+}
+
+// Wire-buffer path shared by run/submit: enqueue everything on the stream.
+static int enqueue_buffer(ipuma_engine* e, const int32_t* inputs, size_t n_inputs, int32_t* results,
+                          size_t n_results, int* launches, int64_t* cells_out) {
+  const ipuma_algo_config& a = e->algo;
+  const long seqWordsPerTile = (a.bufsize + 3) / 4;
+  const long metaOffset = (long)a.tiles_used * seqWordsPerTile;
+  const long totalSlots = (long)a.tiles_used * a.max_batches;
+  int rc;
+  if ((rc = check_wire_sizes(a, n_inputs, n_results))) return rc;
+  // Host-side validation of Meta (the kernels trust offsets and lengths).
+  const int32_t* meta = inputs + metaOffset;
+  int maxB = 0, maxA = 0;
+  int64_t cells = 0;
+  const long tileBytes = seqWordsPerTile * 4;
+  for (long g = 0; g < totalSlots; ++g) {
+    const int32_t al = meta[4 * g], ao = meta[4 * g + 1], bl = meta[4 * g + 2], bo = meta[4 * g + 3];
+    if (al == 0 || bl == 0) continue;
+    if (al < 0 || bl < 0 || ao < 0 || bo < 0 || (long)ao + al > tileBytes || (long)bo + bl > tileBytes)
+      return fail(IPUMA_ERR_INVALID_ARG, "Meta slot %ld points outside its tile", g);
+    maxA = std::max(maxA, al);
+    maxB = std::max(maxB, bl);
+    cells += (int64_t)al * bl;
+  }
+  if (maxA > 65535 || maxB > 65535)
+    return fail(IPUMA_ERR_TOO_LONG, "sequence longer than 65535 (ranges are uint16)");
+  *cells_out = cells;
+  cudaStream_t s = e->stream;
+  if ((rc = e->d_inputs.ensure(sizeof(int32_t) * std::max<size_t>(n_inputs, 1), s))) return rc;
+  if ((rc = e->d_wres.ensure(sizeof(int32_t) * std::max<size_t>(n_results, 1), s))) return rc;
+  if ((rc = reset_ctl(e, s))) return rc;
+  CUDA_TRY(cudaMemcpyAsync(e->d_inputs.p, inputs, sizeof(int32_t) * n_inputs, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaEventRecord(e->ev[1], s));
+  int* d_res = e->d_wres.as<int>();
+  if ((rc = launch_wire(e, s, e->d_inputs.as<int>(), d_res, maxA, maxB, launches))) return rc;
+  CUDA_TRY(cudaEventRecord(e->ev[2], s));
+  CUDA_TRY(cudaMemcpyAsync(results, d_res, sizeof(int32_t) * n_results, cudaMemcpyDeviceToHost, s));
+  return IPUMA_OK;
+}
+
+int ipuma_gpu_run_buffer_device(ipuma_engine* e, const int32_t* d_inputs, size_t n_inputs, int32_t* d_results,
+                                size_t n_results, void* stream) {
+  if (!e) return fail(IPUMA_ERR_INVALID_ARG, "null engine");
+  if ((n_inputs && !d_inputs) || (n_results && !d_results)) return fail(IPUMA_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> lk(e->mu);
+  CUDA_TRY(cudaSetDevice(e->device));
+  const ipuma_algo_config& a = e->algo;
+  int rc;
+  if ((rc = check_wire_sizes(a, n_inputs, n_results))) return rc;
+  cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : e->stream;
+  const long seqWordsPerTile = (a.bufsize + 3) / 4;
+  const long metaOffset = (long)a.tiles_used * seqWordsPerTile;
+  const long totalSlots = (long)a.tiles_used * a.max_batches;
+  e->stats = ipuma_stats{};
+  if ((rc = reset_ctl(e, s))) return rc;
+  int* ctl = e->d_ctl.as<int>();
+  auto* cells = reinterpret_cast<unsigned long long*>(ctl + CTL_CELLS);
+  // Device-side validation of Meta; the host needs maxA/maxB for scratch.
+  const int gb = (int)std::max<long>(1, std::min<long>((totalSlots + 255) / 256, e->nsm * 8));
+  k_wire_check<<<gb, 256, 0, s>>>(d_inputs, metaOffset, seqWordsPerTile * 4, (int)totalSlots, ctl + CTL_INFO,
+                                  cells + CELLS_WIRE);
+  CUDA_TRY(cudaGetLastError());
+  int info[3] = {0, 0, 0};
+  unsigned long long wcells = 0;
+  CUDA_TRY(cudaMemcpyAsync(info, ctl + CTL_INFO, sizeof(info), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(&wcells, cells + CELLS_WIRE, sizeof(wcells), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (info[2]) return fail(IPUMA_ERR_INVALID_ARG, "%d Meta slots point outside their tile", info[2]);
+  if (info[0] > 65535 || info[1] > 65535)
+    return fail(IPUMA_ERR_TOO_LONG, "sequence longer than 65535 (ranges are uint16)");
+  int launches = 1;
+  CUDA_TRY(cudaEventRecord(e->ev[1], s));
+  if ((rc = launch_wire(e, s, d_inputs, d_results, info[0], info[1], &launches))) return rc;
+  CUDA_TRY(cudaEventRecord(e->ev[2], s));
+  if ((rc = check_status(e, s))) return rc;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e->ev[1], e->ev[2]);
+  e->stats.kernel_ms = ms;
+  e->stats.total_ms = ms;
+  e->stats.cells = (int64_t)wcells;
+  e->stats.pairs = totalSlots;
+  e->stats.launches = launches;
+  return IPUMA_OK;
+}
+
+int ipuma_gpu_run_buffer(ipuma_engine* e, const int32_t* inputs, size_t n_inputs, int32_t* results,
+                         size_t n_results) {
+  uint64_t job = 0;
+  int rc = ipuma_gpu_submit_buffer(e, inputs, n_inputs, results, n_results, &job);
+  if (rc) return rc;
+  return ipuma_gpu_join(e, job, -1);
+}
+
+int ipuma_gpu_submit_buffer(ipuma_engine* e, const int32_t* inputs, size_t n_inputs,
+                            int32_t* results, size_t n_results, uint64_t* job) {
+  if (!e || !job) return fail(IPUMA_ERR_INVALID_ARG, "null argument");
+  if ((n_inputs && !inputs) || (n_results && !results)) return fail(IPUMA_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> lk(e->mu);
+  CUDA_TRY(cudaSetDevice(e->device));
+  e->stats = ipuma_stats{};
+  int launches = 0;
+  int64_t cells = 0;
+  CUDA_TRY(cudaEventRecord(e->ev[0], e->stream));
+  int rc = enqueue_buffer(e, inputs, n_inputs, results, n_results, &launches, &cells);
+  if (rc) return rc;
+  Job j;
+  CUDA_TRY(cudaEventCreateWithFlags(&j.done, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventRecord(j.done, e->stream));
+  CUDA_TRY(cudaEventRecord(e->ev[3], e->stream));
+  e->stats.cells = cells;
+  e->stats.pairs = (int64_t)e->algo.tiles_used * e->algo.max_batches;
+  e->stats.launches = launches;
+  *job = e->next_job++;
+  e->jobs[*job] = j;
+  return IPUMA_OK;
+}
+
+int ipuma_gpu_poll(ipuma_engine* e, uint64_t job, int32_t* done) {
+  if (!e || !done) return fail(IPUMA_ERR_INVALID_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(e->mu);
+  auto it = e->jobs.find(job);
+  if (it == e->jobs.end()) return fail(IPUMA_ERR_UNKNOWN_JOB, "unknown job %llu", (unsigned long long)job);
+  cudaError_t q = cudaEventQuery(it->second.done);
+  if (q == cudaSuccess) {
+    *done = 1;
+  } else if (q == cudaErrorNotReady) {
+    *done = 0;
+  } else {
+    return fail(IPUMA_ERR_CUDA, "job %llu failed: %s", (unsigned long long)job, cudaGetErrorString(q));
+  }
+  return IPUMA_OK;
+}
+
+int ipuma_gpu_join(ipuma_engine* e, uint64_t job, int64_t timeout_ms) {
+  if (!e) return fail(IPUMA_ERR_INVALID_ARG, "null engine");
+  cudaEvent_t ev;
+  {
+    std::lock_guard<std::mutex> lk(e->mu);
+    auto it = e->jobs.find(job);
+    if (it == e->jobs.end()) return fail(IPUMA_ERR_UNKNOWN_JOB, "unknown job %llu", (unsigned long long)job);
+    ev = it->second.done;
+  }
+  CUDA_TRY(cudaSetDevice(e->device));
+  const auto t0 = std::chrono::steady_clock::now();
+  while (true) {
+    cudaError_t q = cudaEventQuery(ev);
+    if (q == cudaSuccess) break;
+    if (q != cudaErrorNotReady) return fail(IPUMA_ERR_CUDA, "job failed: %s", cudaGetErrorString(q));
+    if (timeout_ms >= 0 &&
+        std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(timeout_ms))
+      return fail(IPUMA_ERR_TIMEOUT, "job %llu not finished after %lld ms", (unsigned long long)job,
+                  (long long)timeout_ms);
+    if (timeout_ms < 0) {
+      CUDA_TRY(cudaEventSynchronize(ev));
+      break;
+    }
+    std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+  std::lock_guard<std::mutex> lk(e->mu);
+  int rc = check_status(e, e->stream);
+  float kms = 0, tms = 0;
+  cudaEventElapsedTime(&kms, e->ev[1], e->ev[2]);
+  cudaEventElapsedTime(&tms, e->ev[0], e->ev[3]);
+  e->stats.kernel_ms = kms;
+  e->stats.total_ms = tms;
+  auto it = e->jobs.find(job);
+  if (it != e->jobs.end()) {
+    cudaEventDestroy(it->second.done);
+    e->jobs.erase(it);
+  }
+  return rc;
+}
+
+}  // extern "C"

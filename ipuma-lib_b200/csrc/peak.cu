@@ -1,0 +1,82 @@
+// peak.cu -- measures the integer/DPX issue peak that bounds the alignment
+// kernels: the instruction mix of one s16x2 cell update
+//   3 x add.s16x2, 2 x viaddmax.s16x2, 1 x vimax3.relu.s16x2, 1 x max.s16x2
+// (7 instructions = 14 lane-ops, two cells), run as independent chains by
+// every thread of a full-occupancy grid.  Reported as lane-ops per second.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "ipuma_b200.h"
+#include "sw_device.cuh"
+
+namespace {
+
+constexpr int kChains = 8;
+constexpr int kIters = 4096;
+
+__global__ void __launch_bounds__(256) k_int_peak(uint32_t seed, uint32_t* sink) {
+  using T = ipuma_dev::LaneS16x2;
+  uint32_t e[kChains], f[kChains], h[kChains];
+  const uint32_t g = T::splat(-1), go = T::splat(-2);
+#pragma unroll
+  for (int c = 0; c < kChains; ++c) {
+    e[c] = seed ^ (threadIdx.x * 2654435761u) ^ c;
+    f[c] = e[c] * 3u;
+    h[c] = e[c] * 7u;
+  }
+  uint32_t rm = 0;
+  for (int it = 0; it < kIters; ++it) {
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) {
+      const uint32_t hg = T::add(h[c], go);                 // add
+      e[c] = T::addmax(e[c], g, hg);                        // viaddmax
+      f[c] = T::addmax(f[c], g, hg);                        // viaddmax
+      const uint32_t t = T::add(h[c], f[c]);                // add
+      h[c] = T::max3relu(t, e[c], f[c]);                    // vimax3.relu
+      h[c] = T::add(h[c], go);                              // add
+      rm = T::max2(rm, h[c]);                               // max
+    }
+  }
+  uint32_t acc = rm;
+#pragma unroll
+  for (int c = 0; c < kChains; ++c) acc ^= e[c] ^ f[c] ^ h[c];
+  if (acc == 0x12345678u) sink[threadIdx.x] = acc;  // keeps the work alive
+}
+
+}  // namespace
+
+extern "C" int ipuma_measure_int_peak(int32_t device, double* lane_ops_per_s) {
+  if (!lane_ops_per_s) return IPUMA_ERR_INVALID_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) return IPUMA_ERR_NO_DEVICE;
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, device) != cudaSuccess) return IPUMA_ERR_CUDA;
+  int nb = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_int_peak, 256, 0);
+  if (nb < 1) nb = 1;
+  const int grid = nb * p.multiProcessorCount;
+  uint32_t* sink = nullptr;
+  if (cudaMalloc(&sink, 256 * sizeof(uint32_t)) != cudaSuccess) return IPUMA_ERR_NO_MEMORY;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  k_int_peak<<<grid, 256>>>(1u, sink);  // warm-up
+  float best = 1e30f;
+  for (int r = 0; r < 5; ++r) {
+    cudaEventRecord(a);
+    k_int_peak<<<grid, 256>>>(2u + r, sink);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    if (ms < best) best = ms;
+  }
+  cudaError_t err = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(sink);
+  if (err != cudaSuccess) return IPUMA_ERR_CUDA;
+  const double instr = (double)grid * 256 * kIters * kChains * 7.0;
+  *lane_ops_per_s = instr * 2.0 / (best * 1e-3);
+  return IPUMA_OK;
+}

@@ -1,0 +1,422 @@
+// sw_device.cuh -- device-side building blocks of the affine-gap
+// Smith-Waterman (Gotoh) kernels for sm_100a.
+//
+// The recurrence is the one of the ipuma codelet SWAffine::compute
+// (src/codelets/codelet_batch_affine.cpp:65-85):
+//
+//   E      = max(Hleft + gI + gE, E + gE)         E starts at gI on every row
+//   F[j]   = max(Hup[j] + gI + gE, F[j] + gE)     F starts at 0
+//   H      = max(Hdiag + sim[a[j]][b[i]], E, F[j], 0)
+//   best   : first strict maximum in (i over B, j over A) row-major order
+//
+// Kernels keep every H in the shifted form HG = H + (gI + gE).  One add per
+// cell then serves both the E update of the next column and the F update of
+// the next row, and the diagonal term becomes HG_diag + sub' with the query
+// profile holding sub' = sim - (gI + gE).
+//
+// Layout of the work: one warp aligns one pair (s32 lanes) or two pairs
+// (s16x2 lanes, pair P in the low and pair Q in the high halfword).  Lane l
+// owns K consecutive A columns of a 32*K wide strip; B rows stream through
+// the warp as an anti-diagonal wavefront (lane l works on row t - l at step
+// t) and the left neighbour's last-column (HG, E) arrives through
+// __shfl_up_sync.  A longer than one strip is processed strip by strip; the
+// last column of a strip is handed to the next one through per-warp global
+// scratch.  Substitution scores come from a per-strip query profile in
+// shared memory (int8, one row per B letter plus a padding row).
+//
+// Invalid cells (columns past |A|, rows past |B| of the shorter pair of an
+// s16x2 couple) get the profile value SUB_PAD.  With gI + gE < 0 and
+// gE <= 0 every such cell stays strictly below the best valid cell seen so
+// far, so it can never win or tie the maximum; configurations outside that
+// range run on the exact per-thread kernel instead.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ipuma_dev {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int SUB_PAD = -64;  // profile value of padding columns and rows
+
+// Scoring constants shared by all kernels of one launch.
+struct SwConst {
+  int gI;       // gap init (ipu::SWConfig::gapInit)
+  int gE;       // gap extend (ipu::SWConfig::gapExtend)
+  int gIgE;     // gI + gE
+  int M;        // alphabet size (rows/cols of the substitution matrix)
+  int forwardOnly;
+  int s16Limit; // a pair whose score exceeds this is rerun in s32
+};
+
+// -------------------------------------------------------------------------
+// Lane types
+// -------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
+  uint32_t d;
+  asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(sel));
+  return d;
+}
+
+// One pair per warp, exact int32 arithmetic.
+struct LaneS32 {
+  using V = int;
+  static constexpr int NP = 1;
+  __device__ __forceinline__ static V splat(int x) { return x; }
+  __device__ __forceinline__ static V add(V a, V b) { return a + b; }
+  // max(a + b, c)
+  __device__ __forceinline__ static V addmax(V a, V b, V c) { return __viaddmax_s32(a, b, c); }
+  // max(a, b, c, 0)
+  __device__ __forceinline__ static V max3relu(V a, V b, V c) { return __vimax3_s32_relu(a, b, c); }
+  __device__ __forceinline__ static V max2(V a, V b) { return max(a, b); }
+  __device__ __forceinline__ static V max3(V a, V b, V c) { return __vimax3_s32(a, b, c); }
+  // Substitution value of byte `c` (0..3) of the profile word, sign-extended.
+  template <int C>
+  __device__ __forceinline__ static V sub(uint32_t wp, uint32_t /*wq*/) {
+    return (int)prmt(wp, 0u, (uint32_t)(C | ((C | 8) << 4) | ((C | 8) << 8) | ((C | 8) << 12)));
+  }
+  __device__ __forceinline__ static int half(V v, int /*h*/) { return v; }
+  __device__ __forceinline__ static V shfl_up(V v) { return __shfl_up_sync(FULL, v, 1); }
+};
+
+// Two pairs per warp in s16x2 halves (pair P low, pair Q high).
+struct LaneS16x2 {
+  using V = uint32_t;
+  static constexpr int NP = 2;
+  __device__ __forceinline__ static V splat(int x) {
+    return (uint32_t)(x & 0xffff) | ((uint32_t)(x & 0xffff) << 16);
+  }
+  __device__ __forceinline__ static V add(V a, V b) {
+    V d;
+    asm("add.s16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+  }
+  __device__ __forceinline__ static V addmax(V a, V b, V c) { return __viaddmax_s16x2(a, b, c); }
+  __device__ __forceinline__ static V max3relu(V a, V b, V c) { return __vimax3_s16x2_relu(a, b, c); }
+  __device__ __forceinline__ static V max2(V a, V b) {
+    V d;
+    asm("max.s16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+  }
+  __device__ __forceinline__ static V max3(V a, V b, V c) { return __vimax3_s16x2(a, b, c); }
+  template <int C>
+  __device__ __forceinline__ static V sub(uint32_t wp, uint32_t wq) {
+    return prmt(wp, wq, (uint32_t)(C | ((C | 8) << 4) | ((4 + C) << 8) | (((4 + C) | 8) << 12)));
+  }
+  __device__ __forceinline__ static int half(V v, int h) {
+    return h == 0 ? (int)(int16_t)(v & 0xffff) : (int)(int16_t)(v >> 16);
+  }
+  __device__ __forceinline__ static V shfl_up(V v) { return __shfl_up_sync(FULL, v, 1); }
+};
+
+// -------------------------------------------------------------------------
+// Pair views
+// -------------------------------------------------------------------------
+
+// One sequence pair as seen by a pass: A[j] = a[j * da], B[i] = b[i * db].
+// The reverse pass reads a[Aend..0] and b[Bend..0] with da = db = -1.
+struct PassSeq {
+  const uint8_t* a;
+  const uint8_t* b;
+  int alen;
+  int blen;
+  int da;
+  int db;
+};
+
+// Best cell of a pass: score, row (B index), column (A index).
+struct Best {
+  int s, i, j;
+};
+
+// The reference keeps the first strict maximum in (i, j) row-major order.
+__device__ __forceinline__ bool better(int s1, int i1, int j1, int s2, int i2, int j2) {
+  return s1 > s2 || (s1 == s2 && (i1 < i2 || (i1 == i2 && j1 < j2)));
+}
+
+__device__ __forceinline__ void warp_best_reduce(int& s, int& i, int& j) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    int s2 = __shfl_xor_sync(FULL, s, off);
+    int i2 = __shfl_xor_sync(FULL, i, off);
+    int j2 = __shfl_xor_sync(FULL, j, off);
+    if (better(s2, i2, j2, s, i, j)) {
+      s = s2;
+      i = i2;
+      j = j2;
+    }
+  }
+}
+
+// -------------------------------------------------------------------------
+// Query profile: prof[x * (32K) + col] = sim[A[col]][x] - (gI + gE), int8.
+// Row M (the padding letter) and columns past |A| hold SUB_PAD.
+// -------------------------------------------------------------------------
+template <int K>
+__device__ __forceinline__ void build_profile(uint8_t* prof, const int8_t* s_simp, int M,
+                                              const PassSeq& ps, int col0, int lane) {
+  // s_simp[a * (M + 1) + x] = clamp(sim[a][x] - gIgE) and SUB_PAD for x == M.
+  constexpr int SW = 32 * K;
+  int acode[K];
+#pragma unroll
+  for (int c = 0; c < K; ++c) {
+    const int col = col0 + lane * K + c;
+    acode[c] = (col < ps.alen) ? (int)ps.a[(long)col * ps.da] : -1;
+  }
+  for (int x = 0; x <= M; ++x) {
+#pragma unroll
+    for (int w = 0; w < K / 4; ++w) {
+      uint32_t word = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int a = acode[4 * w + q];
+        const int v = (a >= 0) ? (int)s_simp[a * (M + 1) + x] : SUB_PAD;
+        word |= ((uint32_t)(uint8_t)(int8_t)v) << (8 * q);
+      }
+      *reinterpret_cast<uint32_t*>(prof + x * SW + lane * K + 4 * w) = word;
+    }
+  }
+}
+
+template <int K>
+__device__ __forceinline__ void load_profile_row(uint32_t (&w)[K / 4], const uint8_t* p) {
+  if constexpr (K % 16 == 0) {
+#pragma unroll
+    for (int q = 0; q < K / 16; ++q) {
+      uint4 v = reinterpret_cast<const uint4*>(p)[q];
+      w[4 * q + 0] = v.x;
+      w[4 * q + 1] = v.y;
+      w[4 * q + 2] = v.z;
+      w[4 * q + 3] = v.w;
+    }
+  } else if constexpr (K % 8 == 0) {
+#pragma unroll
+    for (int q = 0; q < K / 8; ++q) {
+      uint2 v = reinterpret_cast<const uint2*>(p)[q];
+      w[2 * q + 0] = v.x;
+      w[2 * q + 1] = v.y;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < K / 4; ++q) w[q] = reinterpret_cast<const uint32_t*>(p)[q];
+  }
+}
+
+// -------------------------------------------------------------------------
+// One full pass (forward or reverse) of one warp over NP pairs.
+// Returns false when s16x2 lanes gave up because a running best passed
+// sc.s16Limit (checked every 32 steps, warp-uniformly); the caller reruns
+// both pairs in s32 lanes.
+//
+//   s_prof   : this warp's profile area, NP * (M + 1) * 32K bytes
+//   s_simp   : shifted substitution table (see build_profile)
+//   s_bring  : this warp's 64-entry ring of B letters (P low byte, Q high)
+//   scr      : this warp's scratch, 2 * rowsCap int2 (only used when the
+//              pass needs more than one strip)
+//   out      : best cell per pair, in pass coordinates
+// -------------------------------------------------------------------------
+template <class T, int K>
+__device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, const int8_t* s_simp,
+                                        uint16_t* s_bring, const PassSeq (&ps)[T::NP], int2* scr,
+                                        long rowsCap, Best (&out)[T::NP]) {
+  using V = typename T::V;
+  constexpr int SW = 32 * K;
+  constexpr int NP = T::NP;
+  const int lane = threadIdx.x & 31;
+  const int M = sc.M;
+  const int profStride = (M + 1) * SW;
+
+  int rows = 0, amax = 0;
+#pragma unroll
+  for (int h = 0; h < NP; ++h) {
+    rows = max(rows, ps[h].blen);
+    amax = max(amax, ps[h].alen);
+    out[h].s = 0;
+    out[h].i = 0;
+    out[h].j = 0;
+  }
+  const int nstrips = (amax + SW - 1) / SW;
+  const V vgE = T::splat(sc.gE);
+  const V vgIgE = T::splat(sc.gIgE);
+  const V vgI = T::splat(sc.gI);
+
+  for (int strip = 0; strip < nstrips; ++strip) {
+    const int col0 = strip * SW;
+    const bool hasIn = strip > 0;
+    const bool hasOut = strip + 1 < nstrips;
+    const int2* scrIn = scr + ((strip & 1) ? rowsCap : 0);
+    int2* scrOut = scr + ((strip & 1) ? 0 : rowsCap);
+
+    __syncwarp();
+#pragma unroll
+    for (int h = 0; h < NP; ++h) build_profile<K>(s_prof + h * profStride, s_simp, M, ps[h], col0, lane);
+    __threadfence_block();
+    __syncwarp();
+
+    V HG[K], F[K], snap[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+      HG[c] = vgIgE;
+      F[c] = T::splat(0);
+      snap[c] = vgIgE;
+    }
+    V outHG = vgIgE, outE = vgI, diagIn = vgIgE;
+    V bestG = vgIgE;
+    int brow[NP];
+#pragma unroll
+    for (int h = 0; h < NP; ++h) brow[h] = 0;
+
+    // Boundary (HG, E) of the previous strip's last column: lane k of the
+    // chunk registers holds row (chunkBase + k).
+    int2 chunk = make_int2(0, 0), chunkNext = make_int2(0, 0);
+    if (hasIn) {
+      if (lane < rows) chunk = scrIn[lane];
+      if (32 + lane < rows) chunkNext = scrIn[32 + lane];
+    }
+
+    // B letters, 32 rows at a time: lane k of `bnext` holds the letters of
+    // row (t + 32 + k) and is parked in the shared ring every 32 steps.
+    auto fetch_letters = [&](int r) -> uint32_t {
+      uint32_t v = 0;
+#pragma unroll
+      for (int h = 0; h < NP; ++h) {
+        const int x = (r < ps[h].blen) ? (int)ps[h].b[(long)r * ps[h].db] : M;
+        v |= (uint32_t)x << (8 * h);
+      }
+      return v;
+    };
+    uint32_t bnext = fetch_letters(lane);
+
+    const int nsteps = rows + 31;
+    bool gaveUp = false;
+    for (int t = 0; t < nsteps; ++t) {
+      if ((t & 31) == 0) {
+        if constexpr (NP == 2) {
+          // hG of a cell above s16Limit could overflow the next additions.
+          const int lim = sc.s16Limit + sc.gIgE;
+          const bool hi = T::half(bestG, 0) > lim || T::half(bestG, 1) > lim;
+          if (__any_sync(FULL, hi)) {
+            gaveUp = true;
+            break;
+          }
+        }
+        s_bring[(t + lane) & 63] = (uint16_t)bnext;
+        bnext = fetch_letters(t + 32 + lane);
+        __syncwarp();
+      }
+      V recvHG = T::shfl_up(outHG);
+      V recvE = T::shfl_up(outE);
+      if (hasIn) {
+        if ((t & 31) == 0 && t > 0) {
+          chunk = chunkNext;
+          const int r = t + 32 + lane;
+          chunkNext = (r < rows) ? scrIn[r] : make_int2(0, 0);
+        }
+        const int bx = __shfl_sync(FULL, chunk.x, t & 31);
+        const int by = __shfl_sync(FULL, chunk.y, t & 31);
+        if (lane == 0) {
+          recvHG = (V)bx;
+          recvE = (V)by;
+        }
+      } else if (lane == 0) {
+        recvHG = vgIgE;
+        recvE = vgI;
+      }
+      const V diag0 = diagIn;
+      diagIn = recvHG;
+      const int i = t - lane;
+      if (i >= 0 && i < rows) {
+        // Profile words for this row's B letters.
+        uint32_t wp[K / 4], wq[K / 4];
+        const uint32_t letters = s_bring[i & 63];
+        load_profile_row<K>(wp, s_prof + (letters & 0xff) * SW + lane * K);
+        if constexpr (NP == 2) {
+          load_profile_row<K>(wq, s_prof + profStride + (letters >> 8) * SW + lane * K);
+        } else {
+#pragma unroll
+          for (int q = 0; q < K / 4; ++q) wq[q] = 0;
+        }
+        V hl = recvHG;
+        V e = recvE;
+        V diag = diag0;
+        V rm;
+#pragma unroll
+        for (int c = 0; c < K; ++c) {
+          V s;
+          switch (c & 3) {
+            case 0: s = T::template sub<0>(wp[c >> 2], wq[c >> 2]); break;
+            case 1: s = T::template sub<1>(wp[c >> 2], wq[c >> 2]); break;
+            case 2: s = T::template sub<2>(wp[c >> 2], wq[c >> 2]); break;
+            default: s = T::template sub<3>(wp[c >> 2], wq[c >> 2]); break;
+          }
+          e = T::addmax(e, vgE, hl);
+          const V f = T::addmax(F[c], vgE, HG[c]);
+          const V tt = T::add(diag, s);
+          const V hv = T::max3relu(tt, e, f);
+          diag = HG[c];
+          const V hg = T::add(hv, vgIgE);
+          HG[c] = hg;
+          F[c] = f;
+          hl = hg;
+          rm = (c == 0) ? hg : T::max2(rm, hg);
+        }
+        outHG = hl;
+        outE = e;
+        // Running best of this lane: strict > keeps the first row.
+        const V nb = T::max2(bestG, rm);
+        if (nb != bestG) {
+          uint32_t mask = 0;
+#pragma unroll
+          for (int h = 0; h < NP; ++h) {
+            if (T::half(rm, h) > T::half(bestG, h)) {
+              mask |= (NP == 1) ? 0xffffffffu : (h == 0 ? 0x0000ffffu : 0xffff0000u);
+              brow[h] = i;
+            }
+          }
+#pragma unroll
+          for (int c = 0; c < K; ++c) snap[c] = (V)(((uint32_t)HG[c] & mask) | ((uint32_t)snap[c] & ~mask));
+          bestG = nb;
+        }
+        if (hasOut && lane == 31) scrOut[i] = make_int2((int)outHG, (int)outE);
+      }
+    }
+
+    if constexpr (NP == 2) {
+      if (!gaveUp) {
+        const int lim = sc.s16Limit + sc.gIgE;
+        gaveUp = __any_sync(FULL, T::half(bestG, 0) > lim || T::half(bestG, 1) > lim);
+      }
+      if (gaveUp) return false;
+    }
+    // Strip result: first column of the lane's snapshot that holds its best.
+#pragma unroll
+    for (int h = 0; h < NP; ++h) {
+      const int bg = T::half(bestG, h);
+      int s = bg - sc.gIgE;
+      int jj = 0;
+#pragma unroll
+      for (int c = K - 1; c >= 0; --c)
+        if (T::half(snap[c], h) == bg) jj = c;
+      int ii = brow[h];
+      int j = col0 + lane * K + jj;
+      if (s <= 0) {
+        s = 0;
+        ii = 0;
+        j = 0;
+      }
+      warp_best_reduce(s, ii, j);
+      if (better(s, ii, j, out[h].s, out[h].i, out[h].j)) {
+        out[h].s = s;
+        out[h].i = ii;
+        out[h].j = j;
+      }
+    }
+    if (hasOut) {
+      __threadfence_block();
+      __syncwarp();
+    }
+  }
+  return true;
+}
+
+}  // namespace ipuma_dev

@@ -1,0 +1,464 @@
+// sw_kernels.cuh -- the __global__ kernels of the engine.
+//
+//   k_batched<T, K>   persistent kernel over a cost-ordered work list; each
+//                     warp pulls work items (one pair for s32 lanes, two for
+//                     s16x2) from an atomic queue head.  s16x2 items whose
+//                     score could have left int16 are appended to an overflow
+//                     list that a second k_batched<LaneS32, K> launch reruns.
+//   k_plain<K>        the one-launch-per-batch kernel over the reference's
+//                     wire buffer (Seqs || Meta, ipu_batch_affine.cpp:287) with
+//                     results in its Scores || ARanges || BRanges layout; one
+//                     warp per comparison slot in slot order, s32 lanes.
+//   k_exact           one thread per pair with the recurrence written out
+//                     cell by cell in int32; used for scoring configurations
+//                     that the wavefront kernels do not cover (gI + gE >= 0 or
+//                     gE > 0).
+//   k_bin_*           the cost-binning pre-pass that orders the work list.
+#pragma once
+#include "sw_device.cuh"
+
+namespace ipuma_dev {
+
+// Pair descriptor of the batched API (matches ipuma_pair in ipuma_b200.h).
+struct PairDesc {
+  long long a_off;
+  long long b_off;
+  int a_len;
+  int b_len;
+};
+
+// Packs (start, end) like codelet_batch_affine.cpp:117-123 (uint16 halves).
+__device__ __forceinline__ int pack_range(int start, int end) {
+  return (int)(((uint32_t)(uint16_t)start) | (((uint32_t)(uint16_t)end) << 16));
+}
+
+// Device-side status words (bounded error reporting, no traps).
+struct DevStatus {
+  int error;           // first error code seen by any warp (0 = none)
+  int overflow_start;  // always 0: {overflow_start, overflow_count} is the
+  int overflow_count;  // range of the overflow list for the s32 rerun
+  int pad;
+};
+
+constexpr int ERR_SCRATCH = 1;  // a pass needed more scratch rows than provided
+constexpr int ERR_LENGTH = 2;   // a pair exceeded the stated maximum lengths
+
+// Shared-memory layout of the wavefront kernels.
+template <class T, int K>
+struct SmemLayout {
+  static constexpr int SW = 32 * K;
+  __host__ __device__ static int simp_bytes(int M) { return ((M * (M + 1)) + 15) & ~15; }
+  __host__ __device__ static int prof_bytes(int M) { return T::NP * (M + 1) * SW; }
+  __host__ __device__ static int ring_bytes() { return 64 * 2; }
+  __host__ __device__ static int warp_bytes(int M) { return prof_bytes(M) + ring_bytes(); }
+  __host__ __device__ static int total(int M, int warps) { return simp_bytes(M) + warps * warp_bytes(M); }
+};
+
+// Loads the shifted substitution table: simp[a][x] = sim[a][x] - gIgE for
+// x < M, SUB_PAD for x == M.
+__device__ __forceinline__ void load_simp(int8_t* s_simp, const int8_t* sim, const SwConst& sc) {
+  const int M = sc.M;
+  for (int k = threadIdx.x; k < M * (M + 1); k += blockDim.x) {
+    const int a = k / (M + 1), x = k % (M + 1);
+    int v = (x < M) ? (int)sim[a * M + x] - sc.gIgE : SUB_PAD;
+    v = v < -128 ? -128 : (v > 127 ? 127 : v);
+    s_simp[k] = (int8_t)v;
+  }
+}
+
+// Forward pass (+ reverse pass unless forwardOnly) for the NP pairs held
+// by one warp.  For s16x2 lanes a pair whose score exceeds sc.s16Limit is
+// flagged in `ovf` and gets no reverse pass (the s32 rerun redoes it).
+template <class T, int K>
+__device__ __forceinline__ void align_pairs(const SwConst& sc, uint8_t* s_prof,
+                                            const int8_t* s_simp, uint16_t* s_bring,
+                                            const uint8_t* const (&a0)[T::NP],
+                                            const uint8_t* const (&b0)[T::NP],
+                                            const int (&alen)[T::NP], const int (&blen)[T::NP],
+                                            int2* scr, long rowsCap, Best (&fw)[T::NP],
+                                            Best (&rv)[T::NP], bool (&ovf)[T::NP]) {
+  constexpr int NP = T::NP;
+  PassSeq ps[NP];
+#pragma unroll
+  for (int h = 0; h < NP; ++h) {
+    const bool empty = alen[h] <= 0 || blen[h] <= 0;
+    ps[h] = PassSeq{a0[h], b0[h], empty ? 0 : alen[h], empty ? 0 : blen[h], 1, 1};
+  }
+  const bool done = sw_pass<T, K>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, fw);
+#pragma unroll
+  for (int h = 0; h < NP; ++h) {
+    ovf[h] = (NP == 2) && (!done || fw[h].s > sc.s16Limit);
+    rv[h] = Best{0, 0, 0};
+  }
+  if (!sc.forwardOnly) {
+    PassSeq rs[NP];
+    bool any = false;
+#pragma unroll
+    for (int h = 0; h < NP; ++h) {
+      const bool run = !ovf[h] && fw[h].s > 0;
+      any |= run;
+      rs[h] = run ? PassSeq{a0[h] + fw[h].j, b0[h] + fw[h].i, fw[h].j + 1, fw[h].i + 1, -1, -1}
+                  : PassSeq{a0[h], b0[h], 0, 0, 1, 1};
+    }
+    if (any) sw_pass<T, K>(sc, s_prof, s_simp, s_bring, rs, scr, rowsCap, rv);
+  }
+}
+
+__device__ __forceinline__ void write_result(const SwConst& sc, const Best& fw, const Best& rv,
+                                             int* score, int* arange, int* brange, long idx) {
+  const int aend = fw.j, bend = fw.i;
+  const int astart = sc.forwardOnly ? 0 : aend - rv.j;
+  const int bstart = sc.forwardOnly ? 0 : bend - rv.i;
+  score[idx] = fw.s;
+  arange[idx] = pack_range(astart, aend);
+  brange[idx] = pack_range(bstart, bend);
+}
+
+// Persistent batched kernel.  `list` holds pair ids in processing order;
+// item k covers list[NP*k .. NP*k+NP-1] (ids < 0 are padding).
+template <class T, int K>
+__global__ void __launch_bounds__(128) k_batched(SwConst sc, const int8_t* __restrict__ sim,
+                                                 const uint8_t* __restrict__ codes,
+                                                 const PairDesc* __restrict__ pairs,
+                                                 const int* __restrict__ list,
+                                                 const int* __restrict__ range, int* queue_head,
+                                                 int2* scratch, long rowsCap, int* score,
+                                                 int* arange, int* brange, int* overflow_list,
+                                                 unsigned long long* rerun_cells, DevStatus* st) {
+  using L = SmemLayout<T, K>;
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int warps = blockDim.x >> 5;
+  const int wib = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  int8_t* s_simp = reinterpret_cast<int8_t*>(smem);
+  uint8_t* wbase = smem + L::simp_bytes(sc.M) + wib * L::warp_bytes(sc.M);
+  uint8_t* s_prof = wbase;
+  uint16_t* s_bring = reinterpret_cast<uint16_t*>(wbase + L::prof_bytes(sc.M));
+  load_simp(s_simp, sim, sc);
+  __syncthreads();
+
+  // range = {first list entry, number of entries}, written by the binning
+  // pre-pass (or the overflow counter) on the device.
+  const int n = range[1];
+  list += range[0];
+  const int items = (n + T::NP - 1) / T::NP;
+  const long gw = (long)blockIdx.x * warps + wib;
+  int2* scr = scratch + gw * 2 * rowsCap;
+  while (true) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(queue_head, 1);
+    item = __shfl_sync(FULL, item, 0);
+    if (item >= items) break;
+    constexpr int NP = T::NP;
+    int pid[NP], alen[NP], blen[NP];
+    const uint8_t* a0[NP];
+    const uint8_t* b0[NP];
+#pragma unroll
+    for (int h = 0; h < NP; ++h) {
+      const int k = item * NP + h;
+      pid[h] = (k < n) ? list[k] : -1;
+      PairDesc d = (pid[h] >= 0) ? pairs[pid[h]] : PairDesc{0, 0, 0, 0};
+      alen[h] = d.a_len;
+      blen[h] = d.b_len;
+      a0[h] = codes + d.a_off;
+      b0[h] = codes + d.b_off;
+    }
+    if (blen[0] > rowsCap || (NP == 2 && blen[NP - 1] > rowsCap)) {
+      // The host sizes the scratch for the longest B; report, never trap.
+      if (lane == 0) atomicCAS(&st->error, 0, ERR_SCRATCH);
+      continue;
+    }
+    Best fw[NP], rv[NP];
+    bool ovf[NP];
+    align_pairs<T, K>(sc, s_prof, s_simp, s_bring, a0, b0, alen, blen, scr, rowsCap, fw, rv, ovf);
+    if (lane == 0) {
+#pragma unroll
+      for (int h = 0; h < NP; ++h) {
+        if (pid[h] < 0) continue;
+        if (ovf[h]) {
+          const int slot = atomicAdd(&st->overflow_count, 1);
+          overflow_list[slot] = pid[h];
+          if (rerun_cells)
+            atomicAdd(rerun_cells, (unsigned long long)alen[h] * (unsigned long long)blen[h]);
+          continue;
+        }
+        write_result(sc, fw[h], rv[h], score, arange, brange, pid[h]);
+      }
+    }
+  }
+}
+
+// One-launch-per-batch kernel over the reference wire buffer.
+// Comparison slot g = tile * maxBatches + slot reads Meta[4g..4g+3] =
+// {a_len, a_off, b_len, b_off}, byte offsets into the tile's Seqs region
+// (ipu_batch_affine.cpp:164-167, 881-884), and writes Scores[g],
+// ARanges[g], BRanges[g] of the output buffer (ipu_batch_affine.cpp:208-210,
+// 288).  Warps take slots g = warp, warp + nwarps, ... in slot order.
+template <int K>
+__global__ void __launch_bounds__(128) k_plain(SwConst sc, const int8_t* __restrict__ sim,
+                                               const int* __restrict__ inputs, long seqWordsPerTile,
+                                               long metaOffset, int maxBatches, int totalSlots,
+                                               int2* scratch, long rowsCap, int* results,
+                                               DevStatus* st) {
+  using T = LaneS32;
+  using L = SmemLayout<T, K>;
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int warps = blockDim.x >> 5;
+  const int wib = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  int8_t* s_simp = reinterpret_cast<int8_t*>(smem);
+  uint8_t* wbase = smem + L::simp_bytes(sc.M) + wib * L::warp_bytes(sc.M);
+  uint8_t* s_prof = wbase;
+  uint16_t* s_bring = reinterpret_cast<uint16_t*>(wbase + L::prof_bytes(sc.M));
+  load_simp(s_simp, sim, sc);
+  __syncthreads();
+  const long gw = (long)blockIdx.x * warps + wib;
+  const long nw = (long)gridDim.x * warps;
+  int2* scr = scratch + gw * 2 * rowsCap;
+  const int* meta = inputs + metaOffset;
+  for (long g = gw; g < totalSlots; g += nw) {
+    const long tile = g / maxBatches;
+    const uint8_t* seqs = reinterpret_cast<const uint8_t*>(inputs + tile * seqWordsPerTile);
+    const int alen = meta[4 * g + 0], aoff = meta[4 * g + 1];
+    const int blen = meta[4 * g + 2], boff = meta[4 * g + 3];
+    if (blen > rowsCap) {
+      if (lane == 0) atomicCAS(&st->error, 0, ERR_SCRATCH);
+      continue;
+    }
+    const uint8_t* const a0[1] = {seqs + aoff};
+    const uint8_t* const b0[1] = {seqs + boff};
+    const int al[1] = {alen}, bl[1] = {blen};
+    Best fw[1], rv[1];
+    bool ovf[1];
+    align_pairs<T, K>(sc, s_prof, s_simp, s_bring, a0, b0, al, bl, scr, rowsCap, fw, rv, ovf);
+    if (lane == 0)
+      write_result(sc, fw[0], rv[0], results, results + totalSlots, results + 2L * totalSlots, g);
+  }
+}
+
+// Exact per-thread kernel: one thread per pair, the recurrence written out
+// cell by cell in int32 (codelet_batch_affine.cpp:65-115) with C and F rows
+// in global scratch (2 * maxA int per thread).  Covers every scoring
+// configuration.  Pairs come either from a pair list or from the wire
+// buffer (inputs != nullptr).
+__device__ void exact_pass(const uint8_t* a0, int alen, int da, const uint8_t* b0, int blen, int db,
+                           const int8_t* sim, int M, int gI, int gE, int* C, int* F, Best& out) {
+  int s = 0, bi = 0, bj = 0;
+  for (int j = 0; j < alen; ++j) {
+    C[j] = 0;
+    F[j] = 0;
+  }
+  for (int i = 0; i < blen; ++i) {
+    const int bc = b0[(long)i * db];
+    int e = gI, hl = 0, diag = 0;
+    for (int j = 0; j < alen; ++j) {
+      const int ac = a0[(long)j * da];
+      e = max(hl + gI + gE, e + gE);
+      const int f = max(C[j] + gI + gE, F[j] + gE);
+      F[j] = f;
+      int h = max(diag + (int)sim[ac * M + bc], e);
+      h = max(max(h, f), 0);
+      diag = C[j];
+      C[j] = h;
+      hl = h;
+      if (h > s) {
+        s = h;
+        bi = i;
+        bj = j;
+      }
+    }
+  }
+  out = Best{s, bi, bj};
+}
+
+__global__ void k_exact(SwConst sc, const int8_t* __restrict__ sim, const uint8_t* __restrict__ codes,
+                        const PairDesc* __restrict__ pairs, int n, const int* __restrict__ inputs,
+                        long seqWordsPerTile, long metaOffset, int maxBatches, int* cf_scratch,
+                        long maxA, int* score, int* arange, int* brange) {
+  const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long nt = (long)gridDim.x * blockDim.x;
+  int* C = cf_scratch + tid * 2 * maxA;
+  int* F = C + maxA;
+  for (long p = tid; p < n; p += nt) {
+    const uint8_t *a, *b;
+    int alen, blen;
+    if (inputs) {
+      const long tile = p / maxBatches;
+      const uint8_t* seqs = reinterpret_cast<const uint8_t*>(inputs + tile * seqWordsPerTile);
+      const int* m = inputs + metaOffset + 4 * p;
+      alen = m[0];
+      a = seqs + m[1];
+      blen = m[2];
+      b = seqs + m[3];
+    } else {
+      const PairDesc d = pairs[p];
+      alen = d.a_len;
+      blen = d.b_len;
+      a = codes + d.a_off;
+      b = codes + d.b_off;
+    }
+    Best fw{0, 0, 0}, rv{0, 0, 0};
+    if (alen > 0 && blen > 0 && alen <= maxA) {
+      exact_pass(a, alen, 1, b, blen, 1, sim, sc.M, sc.gI, sc.gE, C, F, fw);
+      if (!sc.forwardOnly)
+        exact_pass(a + fw.j, fw.j + 1, -1, b + fw.i, fw.i + 1, -1, sim, sc.M, sc.gI, sc.gE, C, F, rv);
+    }
+    write_result(sc, fw, rv, score, arange, brange, p);
+  }
+}
+
+// -------------------------------------------------------------------------
+// Cost-binned work list.  Every pair gets a key = class * NBUCKET + bucket,
+// where the class picks the kernel (lane type and columns per lane) and the
+// bucket orders by descending cost |A|*|B| in powers of two; a counting sort
+// over the keys yields the processing order (largest first inside each
+// class, so that the long tail starts early).  Empty pairs get their zero
+// result here and are not listed.
+// -------------------------------------------------------------------------
+constexpr int NBUCKET = 64;
+constexpr int NCLASS_MAX = 8;
+
+struct BinParams {
+  int nclass;
+  int cls_s32;             // class index of the exact-32-bit kernel
+  int s16_max_len;         // min(|A|,|B|) above which s16x2 could overflow
+  int s16_limit;           // scores above this need s32 lanes
+  int k_limit[NCLASS_MAX]; // s16x2 class c takes |A| <= k_limit[c] (last: any)
+  int n_s16_classes;
+  int max_a, max_b;        // stated maxima (violations set ERR_LENGTH)
+  int M;                   // alphabet size of `sim`
+  int force_s32;           // 1: every pair goes to the s32 class
+};
+
+// Best ungapped score along the main diagonal (a lower bound of the local
+// alignment score): pairs that surely pass the s16 limit go straight to
+// s32 lanes instead of giving up half way in s16x2.
+__device__ int diagonal_bound(const uint8_t* a, const uint8_t* b, int n, const int8_t* sim, int M) {
+  int run = 0, best = 0;
+  for (int k = 0; k < n; ++k) {
+    run = max(run + (int)sim[a[k] * M + b[k]], 0);
+    best = max(best, run);
+  }
+  return best;
+}
+
+__device__ __forceinline__ int pair_key(const BinParams& bp, int alen, int blen, bool s32) {
+  int cls;
+  if (bp.force_s32 || s32) {
+    cls = bp.cls_s32;
+  } else {
+    cls = bp.n_s16_classes - 1;
+    for (int c = 0; c < bp.n_s16_classes - 1; ++c)
+      if (alen <= bp.k_limit[c]) {
+        cls = c;
+        break;
+      }
+  }
+  const unsigned long long cost = (unsigned long long)alen * (unsigned long long)blen;
+  const int lg = 63 - __clzll(cost | 1ull);
+  return cls * NBUCKET + (NBUCKET - 1 - lg);
+}
+
+__global__ void k_bin_count(BinParams bp, const uint8_t* __restrict__ codes, const int8_t* __restrict__ sim,
+                            const PairDesc* __restrict__ pairs, int n, int* hist, uint8_t* s32_flag,
+                            unsigned long long* class_cells, DevStatus* st, int* score, int* arange,
+                            int* brange) {
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
+    const PairDesc d = pairs[p];
+    if (d.a_len <= 0 || d.b_len <= 0) {
+      score[p] = 0;
+      arange[p] = 0;
+      brange[p] = 0;
+      continue;
+    }
+    if (d.a_len > bp.max_a || d.b_len > bp.max_b) {
+      atomicCAS(&st->error, 0, ERR_LENGTH);
+      score[p] = 0;
+      arange[p] = 0;
+      brange[p] = 0;
+      continue;
+    }
+    bool s32 = false;
+    if (!bp.force_s32 && min(d.a_len, d.b_len) > bp.s16_max_len)
+      s32 = diagonal_bound(codes + d.a_off, codes + d.b_off, min(d.a_len, d.b_len), sim, bp.M) >
+            bp.s16_limit;
+    s32_flag[p] = s32 ? 1 : 0;
+    const int key = pair_key(bp, d.a_len, d.b_len, s32);
+    atomicAdd(&hist[key], 1);
+    atomicAdd(&class_cells[key / NBUCKET], (unsigned long long)d.a_len * (unsigned long long)d.b_len);
+  }
+}
+
+// Single block: exclusive scan of the histogram into `offs`, and per class
+// the {start, count} range consumed by k_batched.
+__global__ void k_bin_scan(int nkeys, const int* hist, int* offs, int* class_range) {
+  __shared__ int s_sum[1024];
+  const int tid = threadIdx.x;
+  const int per = (nkeys + blockDim.x - 1) / blockDim.x;
+  int local = 0;
+  for (int k = tid * per; k < min(nkeys, (tid + 1) * per); ++k) local += hist[k];
+  s_sum[tid] = local;
+  __syncthreads();
+  for (int off = 1; off < blockDim.x; off <<= 1) {
+    int v = (tid >= off) ? s_sum[tid - off] : 0;
+    __syncthreads();
+    s_sum[tid] += v;
+    __syncthreads();
+  }
+  int run = s_sum[tid] - local;
+  for (int k = tid * per; k < min(nkeys, (tid + 1) * per); ++k) {
+    offs[k] = run;
+    run += hist[k];
+  }
+  __syncthreads();
+  if (tid < nkeys / NBUCKET) {
+    const int c = tid;
+    int cnt = 0;
+    for (int b = 0; b < NBUCKET; ++b) cnt += hist[c * NBUCKET + b];
+    class_range[2 * c] = offs[c * NBUCKET];
+    class_range[2 * c + 1] = cnt;
+  }
+}
+
+__global__ void k_bin_scatter(BinParams bp, const PairDesc* __restrict__ pairs, int n,
+                              const uint8_t* __restrict__ s32_flag, int* offs, int* list) {
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
+    const PairDesc d = pairs[p];
+    if (d.a_len <= 0 || d.b_len <= 0 || d.a_len > bp.max_a || d.b_len > bp.max_b) continue;
+    const int pos = atomicAdd(&offs[pair_key(bp, d.a_len, d.b_len, s32_flag[p] != 0)], 1);
+    list[pos] = (int)p;
+  }
+}
+
+// Validates the Meta section of a device-resident wire buffer: lengths and
+// offsets must stay inside their tile.  info = {maxA, maxB, bad slots}.
+__global__ void k_wire_check(const int* __restrict__ inputs, long metaOffset, long tileBytes,
+                             int totalSlots, int* info, unsigned long long* cells) {
+  for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < totalSlots;
+       g += (long)gridDim.x * blockDim.x) {
+    const int* m = inputs + metaOffset + 4 * g;
+    const int al = m[0], ao = m[1], bl = m[2], bo = m[3];
+    if (al == 0 || bl == 0) continue;
+    if (al < 0 || bl < 0 || ao < 0 || bo < 0 || (long)ao + al > tileBytes || (long)bo + bl > tileBytes) {
+      atomicAdd(&info[2], 1);
+      continue;
+    }
+    atomicMax(&info[0], al);
+    atomicMax(&info[1], bl);
+    atomicAdd(cells, (unsigned long long)al * (unsigned long long)bl);
+  }
+}
+
+// Wire buffer -> pair list: slot g of tile g / maxBatches, offsets made
+// absolute in bytes from the start of the input buffer.
+__global__ void k_wire_to_pairs(const int* __restrict__ inputs, long seqWordsPerTile, long metaOffset,
+                                int maxBatches, int totalSlots, PairDesc* pairs) {
+  for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < totalSlots;
+       g += (long)gridDim.x * blockDim.x) {
+    const int* m = inputs + metaOffset + 4 * g;
+    const long base = (g / maxBatches) * seqWordsPerTile * 4;
+    pairs[g] = PairDesc{base + m[1], base + m[3], m[0], m[2]};
+  }
+}
+
+}  // namespace ipuma_dev

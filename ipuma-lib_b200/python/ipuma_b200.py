@@ -1,0 +1,275 @@
+"""ctypes binding of the C ABI in include/ipuma_b200.h.
+
+Loads the in-tree ``libipuma_b200.so`` (built by ``make -C ipuma-lib_b200``);
+there is no fallback: a missing library or device raises.  Used by the
+tests, ``bench.py`` and ``__graft_entry__``; C and C++ callers link the
+library directly.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG, "libipuma_b200.so")
+
+OK = 0
+ERR_INVALID_ARG = -1
+ERR_CUDA = -2
+ERR_NO_DEVICE = -3
+ERR_TOO_LONG = -4
+ERR_OUT_OF_BUCKETS = -5
+ERR_BAD_SEQUENCE = -6
+ERR_TIMEOUT = -7
+ERR_NO_MEMORY = -8
+ERR_UNKNOWN_JOB = -9
+ERR_DEVICE = -10
+ERR_CLOSED = -11
+
+SIM = {"na": 0, "blosum50": 1, "blosum62": 2, "simple": 3}
+DT = {"na": 0, "aa": 1, "str": 2}
+
+# Every symbol include/ipuma_b200.h declares.
+EXPORTS = [
+    "ipuma_last_error", "ipuma_version", "ipuma_device_count", "ipuma_encode",
+    "ipuma_select_matrix", "ipuma_input_buffer_words", "ipuma_gpu_create", "ipuma_gpu_destroy",
+    "ipuma_gpu_set_option", "ipuma_gpu_run_buffer", "ipuma_gpu_submit_buffer", "ipuma_gpu_poll",
+    "ipuma_gpu_join", "ipuma_gpu_compare", "ipuma_gpu_compare_device", "ipuma_gpu_last_stats",
+    "ipuma_gpu_run_buffer_device", "ipuma_measure_int_peak",
+]
+
+KERNEL_NAMES = {0: "k_batched<s32,K16>", 1: "k_batched<s16x2,K16>", 2: "k_batched<s16x2,K8>",
+                3: "k_batched<s16x2,K4>", 4: "k_batched<s32,K16> rerun", 5: "k_plain<K>",
+                6: "k_exact"}
+
+
+class SwConfig(ctypes.Structure):
+    _fields_ = [("gap_init", ctypes.c_int32), ("gap_extend", ctypes.c_int32),
+                ("match_value", ctypes.c_int32), ("mismatch_value", ctypes.c_int32),
+                ("ambiguity_value", ctypes.c_int32), ("similarity", ctypes.c_int32),
+                ("datatype", ctypes.c_int32)]
+
+
+class AlgoConfig(ctypes.Structure):
+    _fields_ = [("tiles_used", ctypes.c_int32), ("max_ab", ctypes.c_int32),
+                ("max_batches", ctypes.c_int32), ("bufsize", ctypes.c_int32),
+                ("vtype", ctypes.c_int32), ("fill_algo", ctypes.c_int32),
+                ("forward_only", ctypes.c_int32), ("use_remote_buffer", ctypes.c_int32),
+                ("transmission_programs", ctypes.c_int32), ("io_tiles", ctypes.c_int32)]
+
+
+class Pair(ctypes.Structure):
+    _fields_ = [("a_off", ctypes.c_int64), ("b_off", ctypes.c_int64), ("a_len", ctypes.c_int32),
+                ("b_len", ctypes.c_int32)]
+
+
+PAIR_DTYPE = np.dtype([("a_off", "<i8"), ("b_off", "<i8"), ("a_len", "<i4"), ("b_len", "<i4")])
+assert PAIR_DTYPE.itemsize == ctypes.sizeof(Pair) == 24
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("kernel_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
+                ("cells", ctypes.c_int64), ("pairs", ctypes.c_int64),
+                ("s32_pairs", ctypes.c_int64), ("overflow_reruns", ctypes.c_int64),
+                ("launches", ctypes.c_int32), ("used_graph", ctypes.c_int32),
+                ("n_timed", ctypes.c_int32), ("timed_kind", ctypes.c_int32 * 8),
+                ("timed_ms", ctypes.c_double * 8), ("timed_cells", ctypes.c_int64 * 8)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libipuma_b200.so is not built (run __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i32, i64, sz = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_size_t
+        L.ipuma_last_error.restype = ctypes.c_char_p
+        L.ipuma_version.restype = ctypes.c_char_p
+        L.ipuma_device_count.restype = i32
+        L.ipuma_encode.argtypes = [i32, ctypes.c_char_p, sz, vp]
+        L.ipuma_select_matrix.argtypes = [i32, i32, i32, i32, vp, sz, vp, vp]
+        L.ipuma_input_buffer_words.argtypes = [ctypes.POINTER(AlgoConfig)]
+        L.ipuma_input_buffer_words.restype = i64
+        L.ipuma_gpu_create.argtypes = [ctypes.POINTER(SwConfig), ctypes.POINTER(AlgoConfig), i32,
+                                       ctypes.POINTER(vp)]
+        L.ipuma_gpu_destroy.argtypes = [vp]
+        L.ipuma_gpu_destroy.restype = None
+        L.ipuma_gpu_set_option.argtypes = [vp, ctypes.c_char_p, i64]
+        L.ipuma_gpu_run_buffer.argtypes = [vp, vp, sz, vp, sz]
+        L.ipuma_gpu_submit_buffer.argtypes = [vp, vp, sz, vp, sz, ctypes.POINTER(ctypes.c_uint64)]
+        L.ipuma_gpu_poll.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(i32)]
+        L.ipuma_gpu_join.argtypes = [vp, ctypes.c_uint64, i64]
+        L.ipuma_gpu_compare.argtypes = [vp, vp, sz, vp, i32, vp, vp, vp]
+        L.ipuma_gpu_compare_device.argtypes = [vp, vp, sz, vp, i32, i32, i32, vp, vp, vp, vp]
+        L.ipuma_gpu_last_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+        L.ipuma_gpu_run_buffer_device.argtypes = [vp, vp, sz, vp, sz, vp]
+        L.ipuma_measure_int_peak.argtypes = [i32, ctypes.POINTER(ctypes.c_double)]
+        _lib = L
+    return _lib
+
+
+class IpumaError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("ipuma error %d: %s" % (code, msg))
+        self.code = code
+
+
+def _check(rc):
+    if rc != OK:
+        raise IpumaError(rc, lib().ipuma_last_error().decode())
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None and a.size else ctypes.c_void_p(0)
+
+
+def last_error() -> str:
+    return lib().ipuma_last_error().decode()
+
+
+def device_count() -> int:
+    return int(lib().ipuma_device_count())
+
+
+def measure_int_peak(device: int = 0) -> float:
+    """Lane-ops/s of the s16x2 cell-update instruction mix on `device`."""
+    v = ctypes.c_double()
+    _check(lib().ipuma_measure_int_peak(device, ctypes.byref(v)))
+    return v.value
+
+
+def encode(datatype: str, s: str) -> np.ndarray:
+    b = s.encode("latin-1")
+    out = np.zeros(len(b), dtype=np.uint8)
+    _check(lib().ipuma_encode(DT[datatype], b, len(b), _ptr(out)))
+    return out
+
+
+def select_matrix(similarity: str, match=1, mismatch=-1, ambiguity=-1) -> np.ndarray:
+    out = np.zeros(32 * 32, dtype=np.int8)
+    m = ctypes.c_int32()
+    n = ctypes.c_int32()
+    _check(lib().ipuma_select_matrix(SIM[similarity], match, mismatch, ambiguity, _ptr(out),
+                                     out.size, ctypes.byref(m), ctypes.byref(n)))
+    return out[: m.value * n.value].reshape(m.value, n.value).copy()
+
+
+def sw_config(gap_init=0, gap_extend=-1, match=1, mismatch=-1, ambiguity=-1, similarity="na",
+              datatype="na") -> SwConfig:
+    return SwConfig(gap_init, gap_extend, match, mismatch, ambiguity, SIM[similarity], DT[datatype])
+
+
+def algo_config(tiles_used=1, max_ab=300, max_batches=20, bufsize=3000, vtype=0, fill_algo=0,
+                forward_only=False, use_remote_buffer=False, transmission_programs=1,
+                io_tiles=0) -> AlgoConfig:
+    return AlgoConfig(tiles_used, max_ab, max_batches, bufsize, vtype, fill_algo,
+                      int(bool(forward_only)), int(bool(use_remote_buffer)),
+                      transmission_programs, io_tiles)
+
+
+def input_buffer_words(algo: AlgoConfig) -> int:
+    return int(lib().ipuma_input_buffer_words(ctypes.byref(algo)))
+
+
+class Engine:
+    """One engine on one GPU (ipuma_gpu_create / ipuma_gpu_destroy)."""
+
+    def __init__(self, sw: SwConfig, algo: AlgoConfig | None = None, device: int = 0):
+        self.sw = sw
+        self.algo = algo if algo is not None else algo_config()
+        h = ctypes.c_void_p()
+        _check(lib().ipuma_gpu_create(ctypes.byref(self.sw), ctypes.byref(self.algo), device,
+                                      ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().ipuma_gpu_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_option(self, name: str, value: int):
+        _check(lib().ipuma_gpu_set_option(self.h, name.encode(), int(value)))
+
+    def stats(self) -> Stats:
+        st = Stats()
+        _check(lib().ipuma_gpu_last_stats(self.h, ctypes.byref(st)))
+        return st
+
+    def compare(self, codes: np.ndarray, pairs: np.ndarray):
+        """Host buffers in, (score, arange, brange) out, in pair order."""
+        codes = np.ascontiguousarray(codes, dtype=np.uint8)
+        pairs = np.ascontiguousarray(pairs, dtype=PAIR_DTYPE)
+        n = pairs.shape[0]
+        score = np.zeros(n, dtype=np.int32)
+        ar = np.zeros(n, dtype=np.int32)
+        br = np.zeros(n, dtype=np.int32)
+        _check(lib().ipuma_gpu_compare(self.h, _ptr(codes), codes.size, _ptr(pairs), n,
+                                       _ptr(score), _ptr(ar), _ptr(br)))
+        return score, ar, br
+
+    def compare_into(self, codes: np.ndarray, pairs: np.ndarray, score, ar, br):
+        """Like compare() but into caller buffers (e.g. pinned host arrays)."""
+        _check(lib().ipuma_gpu_compare(self.h, _ptr(codes), codes.size, _ptr(pairs),
+                                       pairs.shape[0], _ptr(score), _ptr(ar), _ptr(br)))
+
+    def compare_device(self, d_codes: int, n_codes: int, d_pairs: int, n: int, max_a: int,
+                       max_b: int, d_score: int, d_ar: int, d_br: int, stream: int = 0):
+        """Device pointers (ints) in and out; enqueued on `stream`."""
+        _check(lib().ipuma_gpu_compare_device(self.h, ctypes.c_void_p(d_codes), n_codes,
+                                              ctypes.c_void_p(d_pairs), n, max_a, max_b,
+                                              ctypes.c_void_p(d_score), ctypes.c_void_p(d_ar),
+                                              ctypes.c_void_p(d_br), ctypes.c_void_p(stream)))
+
+    def run_buffer(self, inputs: np.ndarray) -> np.ndarray:
+        inputs = np.ascontiguousarray(inputs, dtype=np.int32)
+        total = self.algo.tiles_used * self.algo.max_batches
+        results = np.zeros(3 * total, dtype=np.int32)
+        _check(lib().ipuma_gpu_run_buffer(self.h, _ptr(inputs), inputs.size, _ptr(results),
+                                          results.size))
+        return results
+
+    def run_buffer_device(self, d_inputs: int, n_inputs: int, d_results: int, n_results: int,
+                          stream: int = 0):
+        _check(lib().ipuma_gpu_run_buffer_device(self.h, ctypes.c_void_p(d_inputs), n_inputs,
+                                                 ctypes.c_void_p(d_results), n_results,
+                                                 ctypes.c_void_p(stream)))
+
+    def submit_buffer(self, inputs: np.ndarray, results: np.ndarray) -> int:
+        job = ctypes.c_uint64()
+        _check(lib().ipuma_gpu_submit_buffer(self.h, _ptr(inputs), inputs.size, _ptr(results),
+                                             results.size, ctypes.byref(job)))
+        return job.value
+
+    def poll(self, job: int) -> bool:
+        done = ctypes.c_int32()
+        _check(lib().ipuma_gpu_poll(self.h, job, ctypes.byref(done)))
+        return bool(done.value)
+
+    def join(self, job: int, timeout_ms: int = -1):
+        _check(lib().ipuma_gpu_join(self.h, job, timeout_ms))
+
+
+def make_pairs(a_off, a_len, b_off, b_len) -> np.ndarray:
+    p = np.zeros(len(a_len), dtype=PAIR_DTYPE)
+    p["a_off"] = a_off
+    p["a_len"] = a_len
+    p["b_off"] = b_off
+    p["b_len"] = b_len
+    return p

@@ -10,7 +10,7 @@ Outputs (committed; nothing at test time reads the reference tree):
 * ``tables.json``  -- NA_CODE / AA_CODE (src/swatlib/encoding.h:26-72) and the
   NA_SUBSTITUTION / BLOSUM50 / BLOSUM62 tables (src/swatlib/similarity.h:17-94),
   parsed from the headers as text.
-* ``known_answers.json`` -- the 18 (score, q/r start/end) answers of
+* ``known_answers.json`` / ``known_answers.txt`` -- the 19 (score, q/r start/end) answers of
   test/simple-test.cpp:25-45 and the 4 M x N scores of test/mn_cmp-test.cpp:29-57,
   parsed as text.
 * ``parity_ref.json`` -- the DNA and protein pairs of test/parity-test.cpp:20-59,
@@ -236,6 +236,17 @@ def main():
     assert len(known["simple"]) == 19, len(known["simple"])
     with open(os.path.join(HERE, "known_answers.json"), "w") as f:
         json.dump(known, f, indent=1)
+    # Plain-text copy for the C++ drop-in tests (tests/cpp): one case per line.
+    with open(os.path.join(HERE, "known_answers.txt"), "w") as f:
+        f.write("# simple: ref query qstart qend rstart rend score\n")
+        for k in known["simple"]:
+            f.write("simple %s %s %d %d %d %d %d\n" % (k["ref"], k["query"], k["qstart"], k["qend"],
+                                                     k["rstart"], k["rend"], k["score"]))
+        f.write("# mn: seq <s> ... / cmp <indexA> <indexB> <score>\n")
+        for sq in known["mn"]["seqs"]:
+            f.write("mnseq %s\n" % sq)
+        for (ia, ib), sc in zip(known["mn"]["comparisons"], known["mn"]["scores"]):
+            f.write("mncmp %d %d %d\n" % (ia, ib, sc))
 
     par = parse_parity(rd("test/parity-test.cpp"))
     assert len(par["dna_queries"]) == 18 and len(par["aa_queries"]) == 4

@@ -1,0 +1,70 @@
+"""CPU tests of the C ABI library: it loads without a GPU, exports every
+function include/ipuma_b200.h declares, and its host helpers (encoders,
+matrices, buffer sizes) match the reference tables in tests/golden/."""
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+import ipuma_b200 as ib
+import oracle
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    text = open(os.path.join(REPO, "include", "ipuma_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(ipuma_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = ib.lib()
+    declared = _declared()
+    assert len(declared) >= 15
+    for name in declared:
+        assert hasattr(L, name), name
+    assert sorted(ib.EXPORTS) == declared
+
+
+def test_version_and_error_strings():
+    assert b"sm_100a" in ib.lib().ipuma_version()
+    with pytest.raises(ib.IpumaError) as ei:
+        ib.select_matrix("simple")
+    assert ei.value.code == ib.ERR_INVALID_ARG
+    assert "simple" in ib.last_error()
+
+
+@pytest.mark.parametrize("sim,args", [("na", (1, -1, -1)), ("na", (2, -3, -5)),
+                                      ("blosum50", (1, -1, -1)), ("blosum62", (1, -1, -1))])
+def test_matrices_match_reference_tables(sim, args):
+    np.testing.assert_array_equal(ib.select_matrix(sim, *args), oracle.select_matrix(sim, *args))
+
+
+def test_encoders_match_reference_tables():
+    t = json.load(open(os.path.join(REPO, "tests", "golden", "tables.json")))
+    for dt, key in (("na", "NA_CODE"), ("aa", "AA_CODE")):
+        for ch, code in t[key].items():
+            if ch == "\\0":
+                continue
+            assert ib.encode(dt, ch)[0] == code
+            assert ib.encode(dt, ch.lower())[0] == code
+    assert ib.encode("aa", "?")[0] == t["AA_CODE"]["\\0"]
+    with pytest.raises(ib.IpumaError) as ei:
+        ib.encode("na", "ACGX")
+    assert ei.value.code == ib.ERR_BAD_SEQUENCE
+
+
+def test_input_buffer_words():
+    a = ib.algo_config(tiles_used=7, max_batches=9, bufsize=4001)
+    assert ib.input_buffer_words(a) == 7 * 1001 + 7 * 9 * 4
+
+
+def test_create_without_device_fails_cleanly():
+    if ib.device_count() > 0:
+        pytest.skip("a GPU is present")
+    with pytest.raises(ib.IpumaError) as ei:
+        ib.Engine(ib.sw_config())
+    assert ei.value.code == ib.ERR_NO_DEVICE
