@@ -122,19 +122,24 @@ typedef struct ipuma_stats {
   /* With option "time_launches" = 1: device time and forward-pass cells of
    * each alignment-kernel launch of the call, in launch order. */
   int32_t n_timed;
-  int32_t timed_kind[8];   /* IPUMA_KERNEL_* */
-  double timed_ms[8];
-  int64_t timed_cells[8];
+  int32_t timed_kind[10];   /* IPUMA_KERNEL_* */
+  double timed_ms[10];
+  int64_t timed_cells[10];
 } ipuma_stats;
 
-/* Kernel kinds reported in ipuma_stats.timed_kind. */
-#define IPUMA_KERNEL_S32_K16 0     /* s32 lanes, 16 columns per lane        */
-#define IPUMA_KERNEL_S16_K16 1     /* s16x2 lanes (2 pairs), 16 columns     */
-#define IPUMA_KERNEL_S16_K8 2
-#define IPUMA_KERNEL_S16_K4 3
-#define IPUMA_KERNEL_S32_RERUN 4   /* s32 rerun of s16x2 give-ups           */
-#define IPUMA_KERNEL_PLAIN 5       /* one-launch-per-batch wire kernel      */
-#define IPUMA_KERNEL_EXACT 6       /* per-thread exact kernel               */
+/* Kernel kinds reported in ipuma_stats.timed_kind.  S16_L<lanes>_K<k>:
+ * s16x2 lanes (two pairs per lane group), <lanes> lanes per group, <k> A
+ * columns per lane. */
+#define IPUMA_KERNEL_S32_K16 0     /* s32 lanes, 32 lanes, 16 columns       */
+#define IPUMA_KERNEL_S16_L16_K4 1
+#define IPUMA_KERNEL_S16_L16_K8 2
+#define IPUMA_KERNEL_S16_L16_K12 3
+#define IPUMA_KERNEL_S16_L16_K16 4
+#define IPUMA_KERNEL_S16_L32_K12 5
+#define IPUMA_KERNEL_S16_L32_K16 6
+#define IPUMA_KERNEL_S32_RERUN 7   /* s32 rerun of s16x2 give-ups           */
+#define IPUMA_KERNEL_PLAIN 8       /* one-launch-per-batch wire kernel      */
+#define IPUMA_KERNEL_EXACT 9       /* per-thread exact kernel               */
 
 typedef struct ipuma_engine ipuma_engine;
 
@@ -164,7 +169,8 @@ void ipuma_gpu_destroy(ipuma_engine* e);
  *   "scheduler"   0 = persistent cost-binned engine (default), 1 = plain
  *                 one-launch-per-batch kernel (wire-buffer API only)
  *   "graphs"      1 = capture and replay CUDA graphs for repeated shapes
- *   "tile_k"      force the columns-per-lane of the wavefront kernels
+ *   "tile_k"      0 = kernel class by |A| (default); 1..6 = every pair
+ *                 through s16x2 class IPUMA_KERNEL_S16_* (value = kind)
  *   "time_launches" 1 = time every alignment-kernel launch (ipuma_stats) */
 int ipuma_gpu_set_option(ipuma_engine* e, const char* name, int64_t value);
 

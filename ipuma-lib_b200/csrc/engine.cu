@@ -78,9 +78,20 @@ struct DevBuf {
   }
 };
 
-// Columns per lane of the s16x2 classes and their |A| limits.
-constexpr int kS16K[3] = {4, 8, 16};
-constexpr int kS32K = 16;
+// Kernel classes of the batched pipeline.  s16x2 classes by |A| (columns
+// per strip = lanes * K), then the s32 class; the rerun reuses the s32
+// kernel.
+struct ClassDef {
+  int lanes, k, kind;
+};
+constexpr int kNumS16 = 6;
+constexpr ClassDef kClasses[kNumS16 + 1] = {
+    {16, 4, IPUMA_KERNEL_S16_L16_K4},   {16, 8, IPUMA_KERNEL_S16_L16_K8},
+    {16, 12, IPUMA_KERNEL_S16_L16_K12}, {16, 16, IPUMA_KERNEL_S16_L16_K16},
+    {32, 12, IPUMA_KERNEL_S16_L32_K12}, {32, 16, IPUMA_KERNEL_S16_L32_K16},
+    {32, 16, IPUMA_KERNEL_S32_K16},
+};
+constexpr int kClsS32 = kNumS16;
 constexpr int kWarpsPerBlock = 4;
 constexpr int kThreads = 32 * kWarpsPerBlock;
 
@@ -112,10 +123,10 @@ struct ipuma_engine {
   int time_launches = 0;
 
   // per-launch timing of the current call (time_launches)
-  cudaEvent_t tev[2 * 8] = {};
+  cudaEvent_t tev[2 * 10] = {};
   int n_timed = 0;
-  int timed_kind[8] = {};
-  int timed_cls[8] = {};
+  int timed_kind[10] = {};
+  int timed_cls[10] = {};
 
   DevBuf d_sim, d_codes, d_pairs, d_list, d_res, d_scratch, d_cf, d_ovf, d_ctl, d_inputs, d_wres, d_flag;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -149,29 +160,33 @@ int occupancy_grid(ipuma_engine* e, K kernel, int smem) {
   return nb * e->nsm;
 }
 
-template <class T, int K>
+template <class T, int K, int LANES>
 int smem_for(const ipuma_engine* e) {
-  return SmemLayout<T, K>::total(e->M, kWarpsPerBlock);
+  return SmemLayout<T, K, LANES>::total(e->M, kWarpsPerBlock);
 }
 
-// Grid of a k_batched<T, K> launch and the warps it runs.
-template <class T, int K>
+// Grid of a k_batched<T, K, LANES> launch.
+template <class T, int K, int LANES>
 int batched_grid(ipuma_engine* e) {
-  return occupancy_grid(e, k_batched<T, K>, smem_for<T, K>(e));
+  return occupancy_grid(e, k_batched<T, K, LANES>, smem_for<T, K, LANES>(e));
 }
 
-int max_batched_warps(ipuma_engine* e) {
+// Lane groups (one scratch slice each) of the widest batched launch.
+int max_batched_groups(ipuma_engine* e) {
   int g = 0;
-  g = std::max(g, batched_grid<LaneS16x2, 4>(e));
-  g = std::max(g, batched_grid<LaneS16x2, 8>(e));
-  g = std::max(g, batched_grid<LaneS16x2, 16>(e));
-  g = std::max(g, batched_grid<LaneS32, 16>(e));
+  g = std::max(g, batched_grid<LaneS16x2, 4, 16>(e) * 2);
+  g = std::max(g, batched_grid<LaneS16x2, 8, 16>(e) * 2);
+  g = std::max(g, batched_grid<LaneS16x2, 12, 16>(e) * 2);
+  g = std::max(g, batched_grid<LaneS16x2, 16, 16>(e) * 2);
+  g = std::max(g, batched_grid<LaneS16x2, 12, 32>(e));
+  g = std::max(g, batched_grid<LaneS16x2, 16, 32>(e));
+  g = std::max(g, batched_grid<LaneS32, 16, 32>(e));
   return g * kWarpsPerBlock;
 }
 
 // Brackets one alignment-kernel launch with events when time_launches is set.
 int timed_begin(ipuma_engine* e, cudaStream_t s, int kind, int cls) {
-  if (!e->time_launches || e->n_timed >= 8) return IPUMA_OK;
+  if (!e->time_launches || e->n_timed >= 10) return IPUMA_OK;
   if (!e->tev[2 * e->n_timed]) {
     CUDA_TRY(cudaEventCreate(&e->tev[2 * e->n_timed]));
     CUDA_TRY(cudaEventCreate(&e->tev[2 * e->n_timed + 1]));
@@ -183,23 +198,23 @@ int timed_begin(ipuma_engine* e, cudaStream_t s, int kind, int cls) {
 }
 
 int timed_end(ipuma_engine* e, cudaStream_t s) {
-  if (!e->time_launches || e->n_timed >= 8) return IPUMA_OK;
+  if (!e->time_launches || e->n_timed >= 10) return IPUMA_OK;
   CUDA_TRY(cudaEventRecord(e->tev[2 * e->n_timed + 1], s));
   e->n_timed++;
   return IPUMA_OK;
 }
 
-template <class T, int K>
+template <class T, int K, int LANES>
 int launch_batched(ipuma_engine* e, cudaStream_t s, const uint8_t* codes, const PairDesc* pairs,
                    const int* list, const int* range, int* head, long rowsCap, int* score,
                    int* arange, int* brange, int kind, int cls) {
-  const int smem = smem_for<T, K>(e);
-  const int grid = batched_grid<T, K>(e);
+  const int smem = smem_for<T, K, LANES>(e);
+  const int grid = batched_grid<T, K, LANES>(e);
   int* ctl = e->d_ctl.as<int>();
   auto* cells = reinterpret_cast<unsigned long long*>(ctl + CTL_CELLS);
   int rc;
   if ((rc = timed_begin(e, s, kind, cls))) return rc;
-  k_batched<T, K><<<grid, kThreads, smem, s>>>(
+  k_batched<T, K, LANES><<<grid, kThreads, smem, s>>>(
       e->sc, e->d_sim.as<int8_t>(), codes, pairs, list, range, head, e->d_scratch.as<int2>(),
       rowsCap, score, arange, brange, e->d_ovf.as<int>(), cells + CELLS_RERUN,
       reinterpret_cast<DevStatus*>(ctl + CTL_STATUS));
@@ -234,22 +249,22 @@ int run_batched(ipuma_engine* e, cudaStream_t s, const uint8_t* codes, const Pai
 
   // Scratch for strip boundaries and the lists.
   const long rowsCap = std::max(1, maxB);
-  const long warps = max_batched_warps(e);
-  if ((rc = e->d_scratch.ensure(sizeof(int2) * 2 * rowsCap * warps, s))) return rc;
+  const long groups = max_batched_groups(e);
+  if ((rc = e->d_scratch.ensure(sizeof(int2) * 2 * rowsCap * groups, s))) return rc;
   if ((rc = e->d_list.ensure(sizeof(int) * (size_t)n + 64, s))) return rc;
   if ((rc = e->d_ovf.ensure(sizeof(int) * (size_t)n + 64, s))) return rc;
 
   BinParams bp{};
-  const int ns16 = 3;
-  bp.n_s16_classes = ns16;
-  bp.cls_s32 = ns16;
-  bp.nclass = ns16 + 1;
+  bp.n_s16_classes = kNumS16;
+  bp.cls_s32 = kClsS32;
+  bp.nclass = kNumS16 + 1;
   bp.s16_max_len = e->s16_max_len;
   bp.force_s32 = e->s16_ok ? 0 : 1;
-  for (int c = 0; c < ns16; ++c) bp.k_limit[c] = 32 * kS16K[c];
+  for (int c = 0; c < kNumS16; ++c) bp.k_limit[c] = kClasses[c].lanes * kClasses[c].k;
   if (e->tile_k > 0) {
-    // Force one s16x2 class: all pairs use the chosen columns per lane.
-    for (int c = 0; c < ns16; ++c) bp.k_limit[c] = (kS16K[c] == e->tile_k) ? (1 << 30) : -1;
+    // Force one s16x2 class: every pair uses the chosen kernel, long A
+    // crossing several strips.
+    for (int c = 0; c < kNumS16; ++c) bp.k_limit[c] = (c == e->tile_k - 1) ? (1 << 30) : -1;
   }
   bp.max_a = maxA;
   bp.max_b = maxB;
@@ -271,29 +286,27 @@ int run_batched(ipuma_engine* e, cudaStream_t s, const uint8_t* codes, const Pai
 
   int* list = e->d_list.as<int>();
   int* heads = ctl + CTL_HEADS;
-  // Long-tail first: the s32 class holds the longest high-scoring pairs.
-  if ((rc = launch_batched<LaneS32, kS32K>(e, s, codes, pairs, list, ctl + CTL_RANGES + 2 * 3,
-                                           heads + 3, rowsCap, score, arange, brange,
-                                           IPUMA_KERNEL_S32_K16, 3)))
+  // Long-tail first: the s32 class holds the longest high-scoring pairs,
+  // then the s16x2 classes from the widest down.
+  const int* R = ctl + CTL_RANGES;
+#define IPUMA_LAUNCH(T, K, L, cls)                                                              \
+  if ((rc = launch_batched<T, K, L>(e, s, codes, pairs, list, R + 2 * (cls), heads + (cls), rowsCap, \
+                                    score, arange, brange, kClasses[cls].kind, cls)))          \
     return rc;
-  if ((rc = launch_batched<LaneS16x2, 16>(e, s, codes, pairs, list, ctl + CTL_RANGES + 2 * 2,
-                                          heads + 2, rowsCap, score, arange, brange,
-                                          IPUMA_KERNEL_S16_K16, 2)))
-    return rc;
-  if ((rc = launch_batched<LaneS16x2, 8>(e, s, codes, pairs, list, ctl + CTL_RANGES + 2 * 1,
-                                         heads + 1, rowsCap, score, arange, brange,
-                                         IPUMA_KERNEL_S16_K8, 1)))
-    return rc;
-  if ((rc = launch_batched<LaneS16x2, 4>(e, s, codes, pairs, list, ctl + CTL_RANGES + 2 * 0,
-                                         heads + 0, rowsCap, score, arange, brange,
-                                         IPUMA_KERNEL_S16_K4, 0)))
-    return rc;
+  IPUMA_LAUNCH(LaneS32, 16, 32, 6)
+  IPUMA_LAUNCH(LaneS16x2, 16, 32, 5)
+  IPUMA_LAUNCH(LaneS16x2, 12, 32, 4)
+  IPUMA_LAUNCH(LaneS16x2, 16, 16, 3)
+  IPUMA_LAUNCH(LaneS16x2, 12, 16, 2)
+  IPUMA_LAUNCH(LaneS16x2, 8, 16, 1)
+  IPUMA_LAUNCH(LaneS16x2, 4, 16, 0)
+#undef IPUMA_LAUNCH
   // Exact 32-bit rerun of the s16x2 pairs whose score may have overflowed.
-  if ((rc = launch_batched<LaneS32, kS32K>(e, s, codes, pairs, e->d_ovf.as<int>(),
-                                           ctl + CTL_STATUS + 1, heads + 4, rowsCap, score,
-                                           arange, brange, IPUMA_KERNEL_S32_RERUN, CELLS_RERUN)))
+  if ((rc = launch_batched<LaneS32, 16, 32>(e, s, codes, pairs, e->d_ovf.as<int>(), ctl + CTL_STATUS + 1,
+                                            heads + 7, rowsCap, score, arange, brange,
+                                            IPUMA_KERNEL_S32_RERUN, CELLS_RERUN)))
     return rc;
-  *launches += 5;
+  *launches += kNumS16 + 2;
   return IPUMA_OK;
 }
 
@@ -342,7 +355,7 @@ int run_plain_wire(ipuma_engine* e, cudaStream_t s, const int* d_inputs, long se
   int* ctl = e->d_ctl.as<int>();
   DevStatus* st = reinterpret_cast<DevStatus*>(ctl + CTL_STATUS);
   const long rowsCap = std::max(1, maxB);
-  const int K = e->tile_k > 0 ? e->tile_k : plain_k_for(e->algo.max_ab);
+  const int K = plain_k_for(e->algo.max_ab);
   auto go = [&](auto kern, int smem) -> int {
     const int grid = occupancy_grid(e, kern, smem);
     const long warps = (long)grid * kWarpsPerBlock;
@@ -355,9 +368,9 @@ int run_plain_wire(ipuma_engine* e, cudaStream_t s, const int* d_inputs, long se
     CUDA_TRY(cudaGetLastError());
     return timed_end(e, s);
   };
-  if (K == 4) rc = go(k_plain<4>, smem_for<LaneS32, 4>(e));
-  else if (K == 8) rc = go(k_plain<8>, smem_for<LaneS32, 8>(e));
-  else rc = go(k_plain<16>, smem_for<LaneS32, 16>(e));
+  if (K == 4) rc = go(k_plain<4>, smem_for<LaneS32, 4, 32>(e));
+  else if (K == 8) rc = go(k_plain<8>, smem_for<LaneS32, 8, 32>(e));
+  else rc = go(k_plain<16>, smem_for<LaneS32, 16, 32>(e));
   *launches += 1;
   return rc;
 }
@@ -515,8 +528,8 @@ int ipuma_gpu_set_option(ipuma_engine* e, const char* name, int64_t value) {
   } else if (k == "time_launches") {
     e->time_launches = value ? 1 : 0;
   } else if (k == "tile_k") {
-    if (value != 0 && value != 4 && value != 8 && value != 16)
-      return fail(IPUMA_ERR_INVALID_ARG, "tile_k must be 0, 4, 8 or 16");
+    if (value < 0 || value > kNumS16)
+      return fail(IPUMA_ERR_INVALID_ARG, "tile_k must be 0 (automatic) or a kernel class 1..%d", kNumS16);
     e->tile_k = (int)value;
   } else {
     return fail(IPUMA_ERR_INVALID_ARG, "unknown option '%s'", name);

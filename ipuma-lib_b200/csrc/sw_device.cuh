@@ -134,29 +134,16 @@ __device__ __forceinline__ bool better(int s1, int i1, int j1, int s2, int i2, i
   return s1 > s2 || (s1 == s2 && (i1 < i2 || (i1 == i2 && j1 < j2)));
 }
 
-__device__ __forceinline__ void warp_best_reduce(int& s, int& i, int& j) {
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    int s2 = __shfl_xor_sync(FULL, s, off);
-    int i2 = __shfl_xor_sync(FULL, i, off);
-    int j2 = __shfl_xor_sync(FULL, j, off);
-    if (better(s2, i2, j2, s, i, j)) {
-      s = s2;
-      i = i2;
-      j = j2;
-    }
-  }
-}
-
 // -------------------------------------------------------------------------
-// Query profile: prof[x * (32K) + col] = sim[A[col]][x] - (gI + gE), int8.
-// Row M (the padding letter) and columns past |A| hold SUB_PAD.
+// Query profile of one group's strip: prof[x * SW + col] =
+// sim[A[col0 + col]][x] - (gI + gE) as int8, SW = LANES * K columns.  Row M
+// (the padding letter) and columns past |A| hold SUB_PAD.
 // -------------------------------------------------------------------------
-template <int K>
+template <int K, int LANES>
 __device__ __forceinline__ void build_profile(uint8_t* prof, const int8_t* s_simp, int M,
                                               const PassSeq& ps, int col0, int lane) {
   // s_simp[a * (M + 1) + x] = clamp(sim[a][x] - gIgE) and SUB_PAD for x == M.
-  constexpr int SW = 32 * K;
+  constexpr int SW = LANES * K;
   int acode[K];
 #pragma unroll
   for (int c = 0; c < K; ++c) {
@@ -202,43 +189,78 @@ __device__ __forceinline__ void load_profile_row(uint32_t (&w)[K / 4], const uin
   }
 }
 
+template <int LANES>
+__device__ __forceinline__ void group_best_reduce(int& s, int& i, int& j) {
+#pragma unroll
+  for (int off = LANES / 2; off > 0; off >>= 1) {
+    int s2 = __shfl_xor_sync(FULL, s, off, LANES);
+    int i2 = __shfl_xor_sync(FULL, i, off, LANES);
+    int j2 = __shfl_xor_sync(FULL, j, off, LANES);
+    if (better(s2, i2, j2, s, i, j)) {
+      s = s2;
+      i = i2;
+      j = j2;
+    }
+  }
+}
+
+// Keep-mask of the running best: all-ones in the halfwords (or the word)
+// where the row maximum `rm` does NOT exceed the best `b`.  For s16x2,
+// rm + ~b = rm - b - 1 is negative exactly there; the halfword signs are
+// replicated with prmt.  (The difference only leaves int16 for cells above
+// the s16 limit, whose pair is then rerun in s32 lanes.)
+__device__ __forceinline__ uint32_t keep_mask(LaneS16x2, uint32_t rm, uint32_t b) {
+  return prmt(LaneS16x2::add(rm, ~b), 0u, 0xBB99u);
+}
+__device__ __forceinline__ uint32_t keep_mask(LaneS32, int rm, int b) {
+  return (uint32_t)((rm + ~b) >> 31);
+}
+
 // -------------------------------------------------------------------------
-// One full pass (forward or reverse) of one warp over NP pairs.
+// One full pass (forward or reverse) of one warp.
+//
+// The warp is split into 32 / LANES groups of LANES lanes; each group aligns
+// its own NP pairs (`ps`, the lane's group) with a wavefront of LANES lanes,
+// K columns per lane.  All groups step in lockstep (the shuffles span the
+// warp) for the warp-wide maximum of rows and strips.
+//
 // Returns false when s16x2 lanes gave up because a running best passed
 // sc.s16Limit (checked every 32 steps, warp-uniformly); the caller reruns
-// both pairs in s32 lanes.
+// the warp's pairs in s32 lanes.
 //
-//   s_prof   : this warp's profile area, NP * (M + 1) * 32K bytes
+//   s_prof   : this group's profile area, NP * (M + 1) * LANES * K bytes
 //   s_simp   : shifted substitution table (see build_profile)
-//   s_bring  : this warp's 64-entry ring of B letters (P low byte, Q high)
-//   scr      : this warp's scratch, 2 * rowsCap int2 (only used when the
+//   s_bring  : this group's 64-entry ring of B letters (P low byte, Q high)
+//   scr      : this group's scratch, 2 * rowsCap int2 (only used when the
 //              pass needs more than one strip)
 //   out      : best cell per pair, in pass coordinates
 // -------------------------------------------------------------------------
-template <class T, int K>
+template <class T, int K, int LANES>
 __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, const int8_t* s_simp,
                                         uint16_t* s_bring, const PassSeq (&ps)[T::NP], int2* scr,
                                         long rowsCap, Best (&out)[T::NP]) {
   using V = typename T::V;
-  constexpr int SW = 32 * K;
+  constexpr int SW = LANES * K;
   constexpr int NP = T::NP;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & (LANES - 1);
   const int M = sc.M;
   const int profStride = (M + 1) * SW;
 
-  int rows = 0, amax = 0;
+  int rowsG = 0, amax = 0;
 #pragma unroll
   for (int h = 0; h < NP; ++h) {
-    rows = max(rows, ps[h].blen);
+    rowsG = max(rowsG, ps[h].blen);
     amax = max(amax, ps[h].alen);
     out[h].s = 0;
     out[h].i = 0;
     out[h].j = 0;
   }
-  const int nstrips = (amax + SW - 1) / SW;
+  const int rowsW = __reduce_max_sync(FULL, rowsG);
+  const int nstrips = (__reduce_max_sync(FULL, amax) + SW - 1) / SW;
   const V vgE = T::splat(sc.gE);
   const V vgIgE = T::splat(sc.gIgE);
   const V vgI = T::splat(sc.gI);
+  const int limG = sc.s16Limit + sc.gIgE;
 
   for (int strip = 0; strip < nstrips; ++strip) {
     const int col0 = strip * SW;
@@ -249,7 +271,8 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
 
     __syncwarp();
 #pragma unroll
-    for (int h = 0; h < NP; ++h) build_profile<K>(s_prof + h * profStride, s_simp, M, ps[h], col0, lane);
+    for (int h = 0; h < NP; ++h)
+      build_profile<K, LANES>(s_prof + h * profStride, s_simp, M, ps[h], col0, lane);
     __threadfence_block();
     __syncwarp();
 
@@ -262,20 +285,20 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
     }
     V outHG = vgIgE, outE = vgI, diagIn = vgIgE;
     V bestG = vgIgE;
-    int brow[NP];
-#pragma unroll
-    for (int h = 0; h < NP; ++h) brow[h] = 0;
+    // Row of each lane's best, one halfword per pair (rows < 65536).
+    uint32_t brow = 0;
 
     // Boundary (HG, E) of the previous strip's last column: lane k of the
-    // chunk registers holds row (chunkBase + k).
+    // group's chunk registers holds row (chunkBase + k).
     int2 chunk = make_int2(0, 0), chunkNext = make_int2(0, 0);
     if (hasIn) {
-      if (lane < rows) chunk = scrIn[lane];
-      if (32 + lane < rows) chunkNext = scrIn[32 + lane];
+      if (lane < rowsG) chunk = scrIn[lane];
+      if (LANES + lane < rowsG) chunkNext = scrIn[LANES + lane];
     }
 
-    // B letters, 32 rows at a time: lane k of `bnext` holds the letters of
-    // row (t + 32 + k) and is parked in the shared ring every 32 steps.
+    // B letters, LANES rows at a time: lane k of `bnext` holds the letters
+    // of row (t + LANES + k) and is parked in the group's ring every LANES
+    // steps.
     auto fetch_letters = [&](int r) -> uint32_t {
       uint32_t v = 0;
 #pragma unroll
@@ -287,33 +310,34 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
     };
     uint32_t bnext = fetch_letters(lane);
 
-    const int nsteps = rows + 31;
+    const int nsteps = rowsW + LANES - 1;
     bool gaveUp = false;
     for (int t = 0; t < nsteps; ++t) {
-      if ((t & 31) == 0) {
+      if ((t & (LANES - 1)) == 0) {
         if constexpr (NP == 2) {
-          // hG of a cell above s16Limit could overflow the next additions.
-          const int lim = sc.s16Limit + sc.gIgE;
-          const bool hi = T::half(bestG, 0) > lim || T::half(bestG, 1) > lim;
-          if (__any_sync(FULL, hi)) {
-            gaveUp = true;
-            break;
+          if ((t & 31) == 0) {
+            // hG of a cell above s16Limit could overflow the next additions.
+            const bool hi = T::half(bestG, 0) > limG || T::half(bestG, 1) > limG;
+            if (__any_sync(FULL, hi)) {
+              gaveUp = true;
+              break;
+            }
           }
         }
         s_bring[(t + lane) & 63] = (uint16_t)bnext;
-        bnext = fetch_letters(t + 32 + lane);
+        bnext = fetch_letters(t + LANES + lane);
         __syncwarp();
-      }
-      V recvHG = T::shfl_up(outHG);
-      V recvE = T::shfl_up(outE);
-      if (hasIn) {
-        if ((t & 31) == 0 && t > 0) {
+        if (hasIn && t > 0) {
           chunk = chunkNext;
-          const int r = t + 32 + lane;
-          chunkNext = (r < rows) ? scrIn[r] : make_int2(0, 0);
+          const int r = t + LANES + lane;
+          chunkNext = (r < rowsG) ? scrIn[r] : make_int2(0, 0);
         }
-        const int bx = __shfl_sync(FULL, chunk.x, t & 31);
-        const int by = __shfl_sync(FULL, chunk.y, t & 31);
+      }
+      V recvHG = __shfl_up_sync(FULL, outHG, 1, LANES);
+      V recvE = __shfl_up_sync(FULL, outE, 1, LANES);
+      if (hasIn) {
+        const int bx = __shfl_sync(FULL, chunk.x, t & (LANES - 1), LANES);
+        const int by = __shfl_sync(FULL, chunk.y, t & (LANES - 1), LANES);
         if (lane == 0) {
           recvHG = (V)bx;
           recvE = (V)by;
@@ -325,7 +349,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
       const V diag0 = diagIn;
       diagIn = recvHG;
       const int i = t - lane;
-      if (i >= 0 && i < rows) {
+      if (i >= 0 && i < rowsG) {
         // Profile words for this row's B letters.
         uint32_t wp[K / 4], wq[K / 4];
         const uint32_t letters = s_bring[i & 63];
@@ -339,7 +363,6 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
         V hl = recvHG;
         V e = recvE;
         V diag = diag0;
-        V rm;
 #pragma unroll
         for (int c = 0; c < K; ++c) {
           V s;
@@ -358,34 +381,29 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
           HG[c] = hg;
           F[c] = f;
           hl = hg;
-          rm = (c == 0) ? hg : T::max2(rm, hg);
         }
+        // Row maximum of the lane, two columns per 3-input max.
+        V rm = HG[0];
+#pragma unroll
+        for (int c = 1; c + 1 < K; c += 2) rm = T::max3(rm, HG[c], HG[c + 1]);
+        if ((K & 1) == 0) rm = T::max2(rm, HG[K - 1]);
         outHG = hl;
         outE = e;
         // Running best of this lane: strict > keeps the first row.
-        const V nb = T::max2(bestG, rm);
-        if (nb != bestG) {
-          uint32_t mask = 0;
+        const uint32_t keep = keep_mask(T{}, rm, bestG);
+        bestG = T::max2(bestG, rm);
+        if (keep != 0xffffffffu) {
+          const uint32_t ipk = (uint32_t)i * 0x00010001u;  // row in both halfwords
+          brow = (brow & keep) | (ipk & ~keep);
 #pragma unroll
-          for (int h = 0; h < NP; ++h) {
-            if (T::half(rm, h) > T::half(bestG, h)) {
-              mask |= (NP == 1) ? 0xffffffffu : (h == 0 ? 0x0000ffffu : 0xffff0000u);
-              brow[h] = i;
-            }
-          }
-#pragma unroll
-          for (int c = 0; c < K; ++c) snap[c] = (V)(((uint32_t)HG[c] & mask) | ((uint32_t)snap[c] & ~mask));
-          bestG = nb;
+          for (int c = 0; c < K; ++c) snap[c] = (V)(((uint32_t)snap[c] & keep) | ((uint32_t)HG[c] & ~keep));
         }
-        if (hasOut && lane == 31) scrOut[i] = make_int2((int)outHG, (int)outE);
+        if (hasOut && lane == LANES - 1) scrOut[i] = make_int2((int)outHG, (int)outE);
       }
     }
 
     if constexpr (NP == 2) {
-      if (!gaveUp) {
-        const int lim = sc.s16Limit + sc.gIgE;
-        gaveUp = __any_sync(FULL, T::half(bestG, 0) > lim || T::half(bestG, 1) > lim);
-      }
+      if (!gaveUp) gaveUp = __any_sync(FULL, T::half(bestG, 0) > limG || T::half(bestG, 1) > limG);
       if (gaveUp) return false;
     }
     // Strip result: first column of the lane's snapshot that holds its best.
@@ -397,14 +415,14 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
 #pragma unroll
       for (int c = K - 1; c >= 0; --c)
         if (T::half(snap[c], h) == bg) jj = c;
-      int ii = brow[h];
+      int ii = (NP == 1) ? (int)(brow & 0xffffu) : (int)((brow >> (16 * h)) & 0xffffu);
       int j = col0 + lane * K + jj;
       if (s <= 0) {
         s = 0;
         ii = 0;
         j = 0;
       }
-      warp_best_reduce(s, ii, j);
+      group_best_reduce<LANES>(s, ii, j);
       if (better(s, ii, j, out[h].s, out[h].i, out[h].j)) {
         out[h].s = s;
         out[h].i = ii;

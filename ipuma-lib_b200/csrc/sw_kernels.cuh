@@ -44,13 +44,16 @@ constexpr int ERR_SCRATCH = 1;  // a pass needed more scratch rows than provided
 constexpr int ERR_LENGTH = 2;   // a pair exceeded the stated maximum lengths
 
 // Shared-memory layout of the wavefront kernels.
-template <class T, int K>
+// Per warp: 32 / LANES groups, each with its profile and B-letter ring.
+template <class T, int K, int LANES>
 struct SmemLayout {
-  static constexpr int SW = 32 * K;
+  static constexpr int SW = LANES * K;
+  static constexpr int GROUPS = 32 / LANES;
   __host__ __device__ static int simp_bytes(int M) { return ((M * (M + 1)) + 15) & ~15; }
   __host__ __device__ static int prof_bytes(int M) { return T::NP * (M + 1) * SW; }
   __host__ __device__ static int ring_bytes() { return 64 * 2; }
-  __host__ __device__ static int warp_bytes(int M) { return prof_bytes(M) + ring_bytes(); }
+  __host__ __device__ static int group_bytes(int M) { return (prof_bytes(M) + ring_bytes() + 15) & ~15; }
+  __host__ __device__ static int warp_bytes(int M) { return GROUPS * group_bytes(M); }
   __host__ __device__ static int total(int M, int warps) { return simp_bytes(M) + warps * warp_bytes(M); }
 };
 
@@ -67,9 +70,10 @@ __device__ __forceinline__ void load_simp(int8_t* s_simp, const int8_t* sim, con
 }
 
 // Forward pass (+ reverse pass unless forwardOnly) for the NP pairs held
-// by one warp.  For s16x2 lanes a pair whose score exceeds sc.s16Limit is
-// flagged in `ovf` and gets no reverse pass (the s32 rerun redoes it).
-template <class T, int K>
+// by one lane group.  For s16x2 lanes a pair whose score exceeds
+// sc.s16Limit (or any pair of a warp that gave up) is flagged in `ovf` and
+// gets no reverse pass (the s32 rerun redoes it).
+template <class T, int K, int LANES>
 __device__ __forceinline__ void align_pairs(const SwConst& sc, uint8_t* s_prof,
                                             const int8_t* s_simp, uint16_t* s_bring,
                                             const uint8_t* const (&a0)[T::NP],
@@ -84,7 +88,7 @@ __device__ __forceinline__ void align_pairs(const SwConst& sc, uint8_t* s_prof,
     const bool empty = alen[h] <= 0 || blen[h] <= 0;
     ps[h] = PassSeq{a0[h], b0[h], empty ? 0 : alen[h], empty ? 0 : blen[h], 1, 1};
   }
-  const bool done = sw_pass<T, K>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, fw);
+  const bool done = sw_pass<T, K, LANES>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, fw);
 #pragma unroll
   for (int h = 0; h < NP; ++h) {
     ovf[h] = (NP == 2) && (!done || fw[h].s > sc.s16Limit);
@@ -100,7 +104,8 @@ __device__ __forceinline__ void align_pairs(const SwConst& sc, uint8_t* s_prof,
       rs[h] = run ? PassSeq{a0[h] + fw[h].j, b0[h] + fw[h].i, fw[h].j + 1, fw[h].i + 1, -1, -1}
                   : PassSeq{a0[h], b0[h], 0, 0, 1, 1};
     }
-    if (any) sw_pass<T, K>(sc, s_prof, s_simp, s_bring, rs, scr, rowsCap, rv);
+    // Uniform across the warp: every group takes part in the shuffles.
+    if (__any_sync(FULL, any)) sw_pass<T, K, LANES>(sc, s_prof, s_simp, s_bring, rs, scr, rowsCap, rv);
   }
 }
 
@@ -115,8 +120,9 @@ __device__ __forceinline__ void write_result(const SwConst& sc, const Best& fw, 
 }
 
 // Persistent batched kernel.  `list` holds pair ids in processing order;
-// item k covers list[NP*k .. NP*k+NP-1] (ids < 0 are padding).
-template <class T, int K>
+// a warp takes items of 32 / LANES * NP consecutive entries (ids < 0 are
+// padding), lane group g aligning entries [g * NP, g * NP + NP).
+template <class T, int K, int LANES>
 __global__ void __launch_bounds__(128) k_batched(SwConst sc, const int8_t* __restrict__ sim,
                                                  const uint8_t* __restrict__ codes,
                                                  const PairDesc* __restrict__ pairs,
@@ -125,15 +131,20 @@ __global__ void __launch_bounds__(128) k_batched(SwConst sc, const int8_t* __res
                                                  int2* scratch, long rowsCap, int* score,
                                                  int* arange, int* brange, int* overflow_list,
                                                  unsigned long long* rerun_cells, DevStatus* st) {
-  using L = SmemLayout<T, K>;
+  using L = SmemLayout<T, K, LANES>;
+  constexpr int NP = T::NP;
+  constexpr int GROUPS = L::GROUPS;
+  constexpr int PER_ITEM = GROUPS * NP;
   extern __shared__ __align__(16) uint8_t smem[];
   const int warps = blockDim.x >> 5;
   const int wib = threadIdx.x >> 5;
-  const int lane = threadIdx.x & 31;
+  const int lane32 = threadIdx.x & 31;
+  const int group = lane32 / LANES;
+  const int glane = lane32 & (LANES - 1);
   int8_t* s_simp = reinterpret_cast<int8_t*>(smem);
-  uint8_t* wbase = smem + L::simp_bytes(sc.M) + wib * L::warp_bytes(sc.M);
-  uint8_t* s_prof = wbase;
-  uint16_t* s_bring = reinterpret_cast<uint16_t*>(wbase + L::prof_bytes(sc.M));
+  uint8_t* gbase = smem + L::simp_bytes(sc.M) + wib * L::warp_bytes(sc.M) + group * L::group_bytes(sc.M);
+  uint8_t* s_prof = gbase;
+  uint16_t* s_bring = reinterpret_cast<uint16_t*>(gbase + L::prof_bytes(sc.M));
   load_simp(s_simp, sim, sc);
   __syncthreads();
 
@@ -141,37 +152,38 @@ __global__ void __launch_bounds__(128) k_batched(SwConst sc, const int8_t* __res
   // pre-pass (or the overflow counter) on the device.
   const int n = range[1];
   list += range[0];
-  const int items = (n + T::NP - 1) / T::NP;
+  const int items = (n + PER_ITEM - 1) / PER_ITEM;
   const long gw = (long)blockIdx.x * warps + wib;
-  int2* scr = scratch + gw * 2 * rowsCap;
+  int2* scr = scratch + (gw * GROUPS + group) * 2 * rowsCap;
   while (true) {
     int item = 0;
-    if (lane == 0) item = atomicAdd(queue_head, 1);
+    if (lane32 == 0) item = atomicAdd(queue_head, 1);
     item = __shfl_sync(FULL, item, 0);
     if (item >= items) break;
-    constexpr int NP = T::NP;
     int pid[NP], alen[NP], blen[NP];
     const uint8_t* a0[NP];
     const uint8_t* b0[NP];
+    bool tooLong = false;
 #pragma unroll
     for (int h = 0; h < NP; ++h) {
-      const int k = item * NP + h;
+      const int k = item * PER_ITEM + group * NP + h;
       pid[h] = (k < n) ? list[k] : -1;
       PairDesc d = (pid[h] >= 0) ? pairs[pid[h]] : PairDesc{0, 0, 0, 0};
       alen[h] = d.a_len;
       blen[h] = d.b_len;
       a0[h] = codes + d.a_off;
       b0[h] = codes + d.b_off;
+      tooLong |= d.b_len > rowsCap;
     }
-    if (blen[0] > rowsCap || (NP == 2 && blen[NP - 1] > rowsCap)) {
+    if (__any_sync(FULL, tooLong)) {
       // The host sizes the scratch for the longest B; report, never trap.
-      if (lane == 0) atomicCAS(&st->error, 0, ERR_SCRATCH);
+      if (lane32 == 0) atomicCAS(&st->error, 0, ERR_SCRATCH);
       continue;
     }
     Best fw[NP], rv[NP];
     bool ovf[NP];
-    align_pairs<T, K>(sc, s_prof, s_simp, s_bring, a0, b0, alen, blen, scr, rowsCap, fw, rv, ovf);
-    if (lane == 0) {
+    align_pairs<T, K, LANES>(sc, s_prof, s_simp, s_bring, a0, b0, alen, blen, scr, rowsCap, fw, rv, ovf);
+    if (glane == 0) {
 #pragma unroll
       for (int h = 0; h < NP; ++h) {
         if (pid[h] < 0) continue;
@@ -201,7 +213,7 @@ __global__ void __launch_bounds__(128) k_plain(SwConst sc, const int8_t* __restr
                                                int2* scratch, long rowsCap, int* results,
                                                DevStatus* st) {
   using T = LaneS32;
-  using L = SmemLayout<T, K>;
+  using L = SmemLayout<T, K, 32>;
   extern __shared__ __align__(16) uint8_t smem[];
   const int warps = blockDim.x >> 5;
   const int wib = threadIdx.x >> 5;
@@ -230,7 +242,7 @@ __global__ void __launch_bounds__(128) k_plain(SwConst sc, const int8_t* __restr
     const int al[1] = {alen}, bl[1] = {blen};
     Best fw[1], rv[1];
     bool ovf[1];
-    align_pairs<T, K>(sc, s_prof, s_simp, s_bring, a0, b0, al, bl, scr, rowsCap, fw, rv, ovf);
+    align_pairs<T, K, 32>(sc, s_prof, s_simp, s_bring, a0, b0, al, bl, scr, rowsCap, fw, rv, ovf);
     if (lane == 0)
       write_result(sc, fw[0], rv[0], results, results + totalSlots, results + 2L * totalSlots, g);
   }
@@ -309,14 +321,24 @@ __global__ void k_exact(SwConst sc, const int8_t* __restrict__ sim, const uint8_
 
 // -------------------------------------------------------------------------
 // Cost-binned work list.  Every pair gets a key = class * NBUCKET + bucket,
-// where the class picks the kernel (lane type and columns per lane) and the
-// bucket orders by descending cost |A|*|B| in powers of two; a counting sort
-// over the keys yields the processing order (largest first inside each
-// class, so that the long tail starts early).  Empty pairs get their zero
-// result here and are not listed.
+// where the class picks the kernel (lane type, lanes per pair, columns per
+// lane: |A| decides it) and the bucket orders by descending |B| on a
+// log-linear scale; a counting sort over the keys yields the processing
+// order: longest first inside each class (the long tail starts early) and
+// neighbours of near-equal rows, which share a warp.  Empty pairs get their
+// zero result here and are not listed.
 // -------------------------------------------------------------------------
-constexpr int NBUCKET = 64;
+constexpr int NBUCKET = 128;
 constexpr int NCLASS_MAX = 8;
+
+// Log-linear bucket of |B| (8 sub-buckets per power of two): pairs that
+// share a bucket differ by at most 1/8 in rows, so the groups of a warp
+// finish their wavefronts together.
+__device__ __forceinline__ int rows_bucket(int b) {
+  if (b < 8) return b;
+  const int lg = 31 - __clz(b);
+  return min(NBUCKET - 1, (lg - 2) * 8 + ((b >> (lg - 3)) & 7));
+}
 
 struct BinParams {
   int nclass;
@@ -354,9 +376,7 @@ __device__ __forceinline__ int pair_key(const BinParams& bp, int alen, int blen,
         break;
       }
   }
-  const unsigned long long cost = (unsigned long long)alen * (unsigned long long)blen;
-  const int lg = 63 - __clzll(cost | 1ull);
-  return cls * NBUCKET + (NBUCKET - 1 - lg);
+  return cls * NBUCKET + (NBUCKET - 1 - rows_bucket(blen));
 }
 
 __global__ void k_bin_count(BinParams bp, const uint8_t* __restrict__ codes, const int8_t* __restrict__ sim,

@@ -40,9 +40,11 @@ EXPORTS = [
     "ipuma_gpu_run_buffer_device", "ipuma_measure_int_peak",
 ]
 
-KERNEL_NAMES = {0: "k_batched<s32,K16>", 1: "k_batched<s16x2,K16>", 2: "k_batched<s16x2,K8>",
-                3: "k_batched<s16x2,K4>", 4: "k_batched<s32,K16> rerun", 5: "k_plain<K>",
-                6: "k_exact"}
+KERNEL_NAMES = {0: "k_batched<s32,L32,K16>", 1: "k_batched<s16x2,L16,K4>",
+                2: "k_batched<s16x2,L16,K8>", 3: "k_batched<s16x2,L16,K12>",
+                4: "k_batched<s16x2,L16,K16>", 5: "k_batched<s16x2,L32,K12>",
+                6: "k_batched<s16x2,L32,K16>", 7: "k_batched<s32,L32,K16> rerun",
+                8: "k_plain<K>", 9: "k_exact"}
 
 
 class SwConfig(ctypes.Structure):
@@ -74,8 +76,8 @@ class Stats(ctypes.Structure):
                 ("cells", ctypes.c_int64), ("pairs", ctypes.c_int64),
                 ("s32_pairs", ctypes.c_int64), ("overflow_reruns", ctypes.c_int64),
                 ("launches", ctypes.c_int32), ("used_graph", ctypes.c_int32),
-                ("n_timed", ctypes.c_int32), ("timed_kind", ctypes.c_int32 * 8),
-                ("timed_ms", ctypes.c_double * 8), ("timed_cells", ctypes.c_int64 * 8)]
+                ("n_timed", ctypes.c_int32), ("timed_kind", ctypes.c_int32 * 10),
+                ("timed_ms", ctypes.c_double * 10), ("timed_cells", ctypes.c_int64 * 10)]
 
 
 _lib = None

@@ -110,13 +110,16 @@ def test_reference_codelet_answers(fixture, forward_only):
         _assert_same(_gpu(case, forward_only), want, case["name"])
 
 
-@pytest.mark.parametrize("tile_k", [4, 8, 16])
+@pytest.mark.parametrize("tile_k", [1, 2, 3, 4, 5, 6])
 def test_random_answers_each_tile_width(tile_k):
-    """Forces every pair through one columns-per-lane variant, so that long
-    pairs cross several strips (global scratch hand-over)."""
+    """Forces every pair through one s16x2 kernel class (16 or 32 lanes per
+    group, 4..16 columns per lane), so that long pairs cross several strips
+    (global scratch hand-over)."""
     for case in json.load(open(os.path.join(GOLD, "random_ref.json")))["cases"]:
         want = (case["ref"]["score"], case["ref"]["arange"], case["ref"]["brange"])
-        _assert_same(_gpu(case, False, tile_k=tile_k), want, "%s k=%d" % (case["name"], tile_k))
+        _assert_same(_gpu(case, False, tile_k=tile_k), want, "%s class=%d" % (case["name"], tile_k))
+        fwd = (case["ref"]["fwd_score"], case["ref"]["fwd_arange"], case["ref"]["fwd_brange"])
+        _assert_same(_gpu(case, True, tile_k=tile_k), fwd, "%s class=%d fwd" % (case["name"], tile_k))
 
 
 # ------------------------------------------------------- workload shapes ---
