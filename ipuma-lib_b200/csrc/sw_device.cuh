@@ -9,10 +9,18 @@
 //   H      = max(Hdiag + sim[a[j]][b[i]], E, F[j], 0)
 //   best   : first strict maximum in (i over B, j over A) row-major order
 //
-// Kernels keep every H in the shifted form HG = H + (gI + gE).  One add per
-// cell then serves both the E update of the next column and the F update of
-// the next row, and the diagonal term becomes HG_diag + sub' with the query
-// profile holding sub' = sim - (gI + gE).
+// Kernels keep H in the reference's frame and E, F shifted by -(gI + gE)
+// (Ê = E - gI - gE, F̂ = F - gI - gE).  Writing Y = max(Hdiag + sim,
+// F, 0), the left neighbour's H + gI + gE = max(Y, E) + gI + gE, and
+// E + gI + gE <= E + gE whenever gI <= 0, so the E recurrence needs Y only:
+//   F̂  = max(F̂ + gE, Hup)                      F̂ = -gI - gE at the start
+//   Y  = max(Hdiag + sim, F̂ + gI + gE, 0)
+//   Ê  = max(Ê + gE', Yleft)                    gE' = max(gE, gI + gE)
+//   H  = max(Y, Ê + gI + gE)                     Ê = -gE at a row start
+// (with gE' the E chain is exact for gI > 0 too).  Every line is one fused
+// DPX add-max (__viaddmax / __viaddmax_relu) except the add F̂ + gI + gE,
+// and only Ê depends on the previous column of the same row, so the
+// row-serial chain is one instruction per cell.
 //
 // Layout of the work: one warp aligns one pair (s32 lanes) or two pairs
 // (s16x2 lanes, pair P in the low and pair Q in the high halfword).  Lane l
@@ -32,6 +40,8 @@
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+
+#include <type_traits>
 
 namespace ipuma_dev {
 
@@ -68,6 +78,8 @@ struct LaneS32 {
   __device__ __forceinline__ static V addmax(V a, V b, V c) { return __viaddmax_s32(a, b, c); }
   // max(a, b, c, 0)
   __device__ __forceinline__ static V max3relu(V a, V b, V c) { return __vimax3_s32_relu(a, b, c); }
+  // max(a + b, c, 0)
+  __device__ __forceinline__ static V addmax_relu(V a, V b, V c) { return __viaddmax_s32_relu(a, b, c); }
   __device__ __forceinline__ static V max2(V a, V b) { return max(a, b); }
   __device__ __forceinline__ static V max3(V a, V b, V c) { return __vimax3_s32(a, b, c); }
   // Substitution value of byte `c` (0..3) of the profile word, sign-extended.
@@ -93,6 +105,7 @@ struct LaneS16x2 {
   }
   __device__ __forceinline__ static V addmax(V a, V b, V c) { return __viaddmax_s16x2(a, b, c); }
   __device__ __forceinline__ static V max3relu(V a, V b, V c) { return __vimax3_s16x2_relu(a, b, c); }
+  __device__ __forceinline__ static V addmax_relu(V a, V b, V c) { return __viaddmax_s16x2_relu(a, b, c); }
   __device__ __forceinline__ static V max2(V a, V b) {
     V d;
     asm("max.s16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
@@ -136,13 +149,13 @@ __device__ __forceinline__ bool better(int s1, int i1, int j1, int s2, int i2, i
 
 // -------------------------------------------------------------------------
 // Query profile of one group's strip: prof[x * SW + col] =
-// sim[A[col0 + col]][x] - (gI + gE) as int8, SW = LANES * K columns.  Row M
-// (the padding letter) and columns past |A| hold SUB_PAD.
+// sim[A[col0 + col]][x] as int8, SW = LANES * K columns.  Row M (the padding
+// letter) and columns past |A| hold SUB_PAD.
 // -------------------------------------------------------------------------
 template <int K, int LANES>
 __device__ __forceinline__ void build_profile(uint8_t* prof, const int8_t* s_simp, int M,
                                               const PassSeq& ps, int col0, int lane) {
-  // s_simp[a * (M + 1) + x] = clamp(sim[a][x] - gIgE) and SUB_PAD for x == M.
+  // s_simp[a * (M + 1) + x] = sim[a][x] and SUB_PAD for x == M.
   constexpr int SW = LANES * K;
   int acode[K];
 #pragma unroll
@@ -222,14 +235,16 @@ __device__ __forceinline__ uint32_t keep_mask(LaneS32, int rm, int b) {
 // The warp is split into 32 / LANES groups of LANES lanes; each group aligns
 // its own NP pairs (`ps`, the lane's group) with a wavefront of LANES lanes,
 // K columns per lane.  All groups step in lockstep (the shuffles span the
-// warp) for the warp-wide maximum of rows and strips.
+// warp) for the warp-wide maximum of rows and strips.  Steps run in blocks
+// of LANES; blocks in which every lane of every group has a row to work on
+// take an unrolled path without per-step activity checks.
 //
 // Returns false when s16x2 lanes gave up because a running best passed
 // sc.s16Limit (checked every 32 steps, warp-uniformly); the caller reruns
 // the warp's pairs in s32 lanes.
 //
 //   s_prof   : this group's profile area, NP * (M + 1) * LANES * K bytes
-//   s_simp   : shifted substitution table (see build_profile)
+//   s_simp   : substitution table with the padding column (build_profile)
 //   s_bring  : this group's 64-entry ring of B letters (P low byte, Q high)
 //   scr      : this group's scratch, 2 * rowsCap int2 (only used when the
 //              pass needs more than one strip)
@@ -256,11 +271,17 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
     out[h].j = 0;
   }
   const int rowsW = __reduce_max_sync(FULL, rowsG);
+  const int rowsMin = __reduce_min_sync(FULL, rowsG);
   const int nstrips = (__reduce_max_sync(FULL, amax) + SW - 1) / SW;
   const V vgE = T::splat(sc.gE);
+  const V vgEp = T::splat(max(sc.gE, sc.gIgE));
   const V vgIgE = T::splat(sc.gIgE);
-  const V vgI = T::splat(sc.gI);
-  const int limG = sc.s16Limit + sc.gIgE;
+  // Ê handed to column 0 (and the initial hand-over value): -gE' makes the
+  // first column's Ê come out as the reference's E = max(gI, H - gI) + gE.
+  const V vE0 = T::splat(-max(sc.gE, sc.gIgE));
+  const V vF0 = T::splat(-sc.gIgE);   // F̂ where F = 0 (pass start)
+  const V vZero = T::splat(0);
+  const int lim = sc.s16Limit;
 
   for (int strip = 0; strip < nstrips; ++strip) {
     const int col0 = strip * SW;
@@ -276,19 +297,19 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
     __threadfence_block();
     __syncwarp();
 
-    V HG[K], F[K], snap[K];
+    V H[K], Fh[K], snap[K];
 #pragma unroll
     for (int c = 0; c < K; ++c) {
-      HG[c] = vgIgE;
-      F[c] = T::splat(0);
-      snap[c] = vgIgE;
+      H[c] = vZero;
+      Fh[c] = vF0;
+      snap[c] = vZero;
     }
-    V outHG = vgIgE, outE = vgI, diagIn = vgIgE;
-    V bestG = vgIgE;
+    V outY = vZero, outE = vE0, diagIn = vZero;
+    V best = vZero;
     // Row of each lane's best, one halfword per pair (rows < 65536).
     uint32_t brow = 0;
 
-    // Boundary (HG, E) of the previous strip's last column: lane k of the
+    // Boundary (Y, Ê) of the previous strip's last column: lane k of the
     // group's chunk registers holds row (chunkBase + k).
     int2 chunk = make_int2(0, 0), chunkNext = make_int2(0, 0);
     if (hasIn) {
@@ -297,7 +318,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
     }
 
     // B letters, LANES rows at a time: lane k of `bnext` holds the letters
-    // of row (t + LANES + k) and is parked in the group's ring every LANES
+    // of row (t0 + LANES + k) and is parked in the group's ring every LANES
     // steps.
     auto fetch_letters = [&](int r) -> uint32_t {
       uint32_t v = 0;
@@ -310,47 +331,27 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
     };
     uint32_t bnext = fetch_letters(lane);
 
-    const int nsteps = rowsW + LANES - 1;
-    bool gaveUp = false;
-    for (int t = 0; t < nsteps; ++t) {
-      if ((t & (LANES - 1)) == 0) {
-        if constexpr (NP == 2) {
-          if ((t & 31) == 0) {
-            // hG of a cell above s16Limit could overflow the next additions.
-            const bool hi = T::half(bestG, 0) > limG || T::half(bestG, 1) > limG;
-            if (__any_sync(FULL, hi)) {
-              gaveUp = true;
-              break;
-            }
-          }
-        }
-        s_bring[(t + lane) & 63] = (uint16_t)bnext;
-        bnext = fetch_letters(t + LANES + lane);
-        __syncwarp();
-        if (hasIn && t > 0) {
-          chunk = chunkNext;
-          const int r = t + LANES + lane;
-          chunkNext = (r < rowsG) ? scrIn[r] : make_int2(0, 0);
-        }
-      }
-      V recvHG = __shfl_up_sync(FULL, outHG, 1, LANES);
+    // One wavefront step: lane works on row t - lane (when CHECK, only if
+    // that row exists for its group).
+    auto step = [&](int t, auto check) {
+      V recvY = __shfl_up_sync(FULL, outY, 1, LANES);
       V recvE = __shfl_up_sync(FULL, outE, 1, LANES);
       if (hasIn) {
         const int bx = __shfl_sync(FULL, chunk.x, t & (LANES - 1), LANES);
         const int by = __shfl_sync(FULL, chunk.y, t & (LANES - 1), LANES);
         if (lane == 0) {
-          recvHG = (V)bx;
+          recvY = (V)bx;
           recvE = (V)by;
         }
       } else if (lane == 0) {
-        recvHG = vgIgE;
-        recvE = vgI;
+        recvY = vZero;
+        recvE = vE0;
       }
+      // H of the left neighbour's last column, the next row's diagonal.
       const V diag0 = diagIn;
-      diagIn = recvHG;
+      diagIn = T::addmax(recvE, vgIgE, recvY);
       const int i = t - lane;
-      if (i >= 0 && i < rowsG) {
-        // Profile words for this row's B letters.
+      if (!decltype(check)::value || (i >= 0 && i < rowsG)) {
         uint32_t wp[K / 4], wq[K / 4];
         const uint32_t letters = s_bring[i & 63];
         load_profile_row<K>(wp, s_prof + (letters & 0xff) * SW + lane * K);
@@ -360,57 +361,93 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
 #pragma unroll
           for (int q = 0; q < K / 4; ++q) wq[q] = 0;
         }
-        V hl = recvHG;
+        // The left neighbour hands over (Y, Ê) of its last column; lane 0
+        // of the first strip starts the row with Y = 0, Ê = -gE.
+        V yl = recvY;
         V e = recvE;
         V diag = diag0;
 #pragma unroll
         for (int c = 0; c < K; ++c) {
-          V s;
+          V sb;
           switch (c & 3) {
-            case 0: s = T::template sub<0>(wp[c >> 2], wq[c >> 2]); break;
-            case 1: s = T::template sub<1>(wp[c >> 2], wq[c >> 2]); break;
-            case 2: s = T::template sub<2>(wp[c >> 2], wq[c >> 2]); break;
-            default: s = T::template sub<3>(wp[c >> 2], wq[c >> 2]); break;
+            case 0: sb = T::template sub<0>(wp[c >> 2], wq[c >> 2]); break;
+            case 1: sb = T::template sub<1>(wp[c >> 2], wq[c >> 2]); break;
+            case 2: sb = T::template sub<2>(wp[c >> 2], wq[c >> 2]); break;
+            default: sb = T::template sub<3>(wp[c >> 2], wq[c >> 2]); break;
           }
-          e = T::addmax(e, vgE, hl);
-          const V f = T::addmax(F[c], vgE, HG[c]);
-          const V tt = T::add(diag, s);
-          const V hv = T::max3relu(tt, e, f);
-          diag = HG[c];
-          const V hg = T::add(hv, vgIgE);
-          HG[c] = hg;
-          F[c] = f;
-          hl = hg;
+          const V f = T::addmax(Fh[c], vgE, H[c]);                   // F̂
+          const V y = T::addmax_relu(diag, sb, T::add(f, vgIgE));    // Y
+          e = T::addmax(e, vgEp, yl);                                // Ê
+          const V hv = T::addmax(e, vgIgE, y);                       // H
+          diag = H[c];
+          H[c] = hv;
+          Fh[c] = f;
+          yl = y;
         }
-        // Row maximum of the lane, two columns per 3-input max.
-        V rm = HG[0];
-#pragma unroll
-        for (int c = 1; c + 1 < K; c += 2) rm = T::max3(rm, HG[c], HG[c + 1]);
-        if ((K & 1) == 0) rm = T::max2(rm, HG[K - 1]);
-        outHG = hl;
+        outY = yl;
         outE = e;
+        // Row maximum of the lane (full-rate 2-input max tree).
+        V m8[(K + 1) / 2];
+#pragma unroll
+        for (int c = 0; c < K / 2; ++c) m8[c] = T::max2(H[2 * c], H[2 * c + 1]);
+        if constexpr (K & 1) m8[K / 2] = H[K - 1];
+#pragma unroll
+        for (int w = 1; w < (K + 1) / 2; w *= 2)
+#pragma unroll
+          for (int c = 0; c + w < (K + 1) / 2; c += 2 * w) m8[c] = T::max2(m8[c], m8[c + w]);
+        const V rm = m8[0];
         // Running best of this lane: strict > keeps the first row.
-        const uint32_t keep = keep_mask(T{}, rm, bestG);
-        bestG = T::max2(bestG, rm);
+        const uint32_t keep = keep_mask(T{}, rm, best);
+        best = T::max2(best, rm);
         if (keep != 0xffffffffu) {
           const uint32_t ipk = (uint32_t)i * 0x00010001u;  // row in both halfwords
           brow = (brow & keep) | (ipk & ~keep);
 #pragma unroll
-          for (int c = 0; c < K; ++c) snap[c] = (V)(((uint32_t)snap[c] & keep) | ((uint32_t)HG[c] & ~keep));
+          for (int c = 0; c < K; ++c) snap[c] = (V)(((uint32_t)snap[c] & keep) | ((uint32_t)H[c] & ~keep));
         }
-        if (hasOut && lane == LANES - 1) scrOut[i] = make_int2((int)outHG, (int)outE);
+        if (hasOut && lane == LANES - 1) scrOut[i] = make_int2((int)outY, (int)outE);
+      }
+    };
+
+    const int nsteps = rowsW + LANES - 1;
+    bool gaveUp = false;
+    for (int t0 = 0; t0 < nsteps; t0 += LANES) {
+      if constexpr (NP == 2) {
+        if ((t0 & 31) == 0) {
+          // A cell above s16Limit could overflow the next additions.
+          const bool hi = T::half(best, 0) > lim || T::half(best, 1) > lim;
+          if (__any_sync(FULL, hi)) {
+            gaveUp = true;
+            break;
+          }
+        }
+      }
+      s_bring[(t0 + lane) & 63] = (uint16_t)bnext;
+      bnext = fetch_letters(t0 + LANES + lane);
+      __syncwarp();
+      if (hasIn && t0 > 0) {
+        chunk = chunkNext;
+        const int r = t0 + LANES + lane;
+        chunkNext = (r < rowsG) ? scrIn[r] : make_int2(0, 0);
+      }
+      if (t0 >= LANES - 1 && t0 + LANES - 1 < rowsMin) {
+#pragma unroll
+        for (int k = 0; k < LANES; ++k) step(t0 + k, std::false_type{});
+      } else {
+#pragma unroll 1
+        for (int k = 0; k < LANES; ++k) step(t0 + k, std::true_type{});
       }
     }
 
     if constexpr (NP == 2) {
-      if (!gaveUp) gaveUp = __any_sync(FULL, T::half(bestG, 0) > limG || T::half(bestG, 1) > limG);
+      if (!gaveUp) gaveUp = __any_sync(FULL, T::half(best, 0) > lim || T::half(best, 1) > lim);
       if (gaveUp) return false;
     }
     // Strip result: first column of the lane's snapshot that holds its best.
 #pragma unroll
     for (int h = 0; h < NP; ++h) {
-      const int bg = T::half(bestG, h);
-      int s = bg - sc.gIgE;
+      const int bg = T::half(best, h);
+      int s = bg;
       int jj = 0;
 #pragma unroll
       for (int c = K - 1; c >= 0; --c)

@@ -57,15 +57,13 @@ struct SmemLayout {
   __host__ __device__ static int total(int M, int warps) { return simp_bytes(M) + warps * warp_bytes(M); }
 };
 
-// Loads the shifted substitution table: simp[a][x] = sim[a][x] - gIgE for
-// x < M, SUB_PAD for x == M.
+// Loads the substitution table with its padding column: simp[a][x] =
+// sim[a][x] for x < M, SUB_PAD for x == M.
 __device__ __forceinline__ void load_simp(int8_t* s_simp, const int8_t* sim, const SwConst& sc) {
   const int M = sc.M;
   for (int k = threadIdx.x; k < M * (M + 1); k += blockDim.x) {
     const int a = k / (M + 1), x = k % (M + 1);
-    int v = (x < M) ? (int)sim[a * M + x] - sc.gIgE : SUB_PAD;
-    v = v < -128 ? -128 : (v > 127 ? 127 : v);
-    s_simp[k] = (int8_t)v;
+    s_simp[k] = (x < M) ? sim[a * M + x] : (int8_t)SUB_PAD;
   }
 }
 
