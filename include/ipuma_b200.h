@@ -213,6 +213,25 @@ int ipuma_gpu_run_buffer_device(ipuma_engine* e, const int32_t* d_inputs, size_t
 
 int ipuma_gpu_last_stats(ipuma_engine* e, ipuma_stats* out);
 
+/* Allocation-free alignment, for callers that cannot call cudaMalloc (for
+ * example code running while its stream is captured into a CUDA graph,
+ * hosts that own all device memory through their own pool, or paths that
+ * cannot afford the synchronisation cudaMalloc/cudaFree imply).  No
+ * counterpart in the reference.  Aligns n pairs on the current device with
+ * exact 32-bit lanes; codes, pairs and the three result arrays are device
+ * memory owned by the caller; results as ipuma_gpu_compare.  Nothing is
+ * allocated: the kernel's strip-boundary scratch is a 16 MiB file-scope
+ * device array that every GPU loading the library holds until exit.
+ * Limits: max_b_len (an upper bound of every b_len, checked on the device)
+ * at most 65535; gap_init + gap_extend < 0 and gap_extend <= 0.  The first
+ * call on a device looks up the array's device address, so make it before
+ * any stream capture.  All calls share the array: calls that overlap on the
+ * GPU race and must be serialised by the caller.  Blocks until the batch is
+ * done; errors through ipuma_last_error(). */
+int ipuma_gpu_compare_noalloc(const ipuma_sw_config* sw, int32_t forward_only, const uint8_t* d_codes,
+                              size_t n_codes, const ipuma_pair* d_pairs, int32_t n, int32_t max_b_len,
+                              int32_t* d_score, int32_t* d_arange, int32_t* d_brange, void* stream);
+
 /* Measures, on `device`, the issue rate of the s16x2 instruction mix of one
  * cell update (3 add, 2 viaddmax, 1 vimax3.relu, 1 max) in lane-ops per
  * second: the peak against which the kernels' roofline fraction is taken. */

@@ -18,6 +18,7 @@
 #include <thread>
 #include <vector>
 
+#include "errors.h"
 #include "ipuma_b200.h"
 #include "sw_kernels.cuh"
 #include "../host/swatlib/encoding.h"
@@ -26,9 +27,10 @@
 using namespace ipuma_dev;
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
 
+namespace ipuma_internal {
 int fail(int code, const char* fmt, ...) {
   char buf[512];
   va_list ap;
@@ -38,6 +40,10 @@ int fail(int code, const char* fmt, ...) {
   g_last_error = buf;
   return code;
 }
+}  // namespace ipuma_internal
+
+namespace {
+using ipuma_internal::fail;
 
 #define CUDA_TRY(expr)                                                                   \
   do {                                                                                   \

@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(128) k_plain(SwConst sc, const int8_t* __restr
 // in global scratch (2 * maxA int per thread).  Covers every scoring
 // configuration.  Pairs come either from a pair list or from the wire
 // buffer (inputs != nullptr).
-__device__ void exact_pass(const uint8_t* a0, int alen, int da, const uint8_t* b0, int blen, int db,
+static __device__ void exact_pass(const uint8_t* a0, int alen, int da, const uint8_t* b0, int blen, int db,
                            const int8_t* sim, int M, int gI, int gE, int* C, int* F, Best& out) {
   int s = 0, bi = 0, bj = 0;
   for (int j = 0; j < alen; ++j) {
@@ -281,7 +281,7 @@ __device__ void exact_pass(const uint8_t* a0, int alen, int da, const uint8_t* b
   out = Best{s, bi, bj};
 }
 
-__global__ void k_exact(SwConst sc, const int8_t* __restrict__ sim, const uint8_t* __restrict__ codes,
+static __global__ void k_exact(SwConst sc, const int8_t* __restrict__ sim, const uint8_t* __restrict__ codes,
                         const PairDesc* __restrict__ pairs, int n, const int* __restrict__ inputs,
                         long seqWordsPerTile, long metaOffset, int maxBatches, int* cf_scratch,
                         long maxA, int* score, int* arange, int* brange) {
@@ -353,7 +353,7 @@ struct BinParams {
 // Best ungapped score along the main diagonal (a lower bound of the local
 // alignment score): pairs that surely pass the s16 limit go straight to
 // s32 lanes instead of giving up half way in s16x2.
-__device__ int diagonal_bound(const uint8_t* a, const uint8_t* b, int n, const int8_t* sim, int M) {
+static __device__ int diagonal_bound(const uint8_t* a, const uint8_t* b, int n, const int8_t* sim, int M) {
   int run = 0, best = 0;
   for (int k = 0; k < n; ++k) {
     run = max(run + (int)sim[a[k] * M + b[k]], 0);
@@ -377,7 +377,7 @@ __device__ __forceinline__ int pair_key(const BinParams& bp, int alen, int blen,
   return cls * NBUCKET + (NBUCKET - 1 - rows_bucket(blen));
 }
 
-__global__ void k_bin_count(BinParams bp, const uint8_t* __restrict__ codes, const int8_t* __restrict__ sim,
+static __global__ void k_bin_count(BinParams bp, const uint8_t* __restrict__ codes, const int8_t* __restrict__ sim,
                             const PairDesc* __restrict__ pairs, int n, int* hist, uint8_t* s32_flag,
                             unsigned long long* class_cells, DevStatus* st, int* score, int* arange,
                             int* brange) {
@@ -409,7 +409,7 @@ __global__ void k_bin_count(BinParams bp, const uint8_t* __restrict__ codes, con
 
 // Single block: exclusive scan of the histogram into `offs`, and per class
 // the {start, count} range consumed by k_batched.
-__global__ void k_bin_scan(int nkeys, const int* hist, int* offs, int* class_range) {
+static __global__ void k_bin_scan(int nkeys, const int* hist, int* offs, int* class_range) {
   __shared__ int s_sum[1024];
   const int tid = threadIdx.x;
   const int per = (nkeys + blockDim.x - 1) / blockDim.x;
@@ -438,7 +438,7 @@ __global__ void k_bin_scan(int nkeys, const int* hist, int* offs, int* class_ran
   }
 }
 
-__global__ void k_bin_scatter(BinParams bp, const PairDesc* __restrict__ pairs, int n,
+static __global__ void k_bin_scatter(BinParams bp, const PairDesc* __restrict__ pairs, int n,
                               const uint8_t* __restrict__ s32_flag, int* offs, int* list) {
   for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
     const PairDesc d = pairs[p];
@@ -450,7 +450,7 @@ __global__ void k_bin_scatter(BinParams bp, const PairDesc* __restrict__ pairs, 
 
 // Validates the Meta section of a device-resident wire buffer: lengths and
 // offsets must stay inside their tile.  info = {maxA, maxB, bad slots}.
-__global__ void k_wire_check(const int* __restrict__ inputs, long metaOffset, long tileBytes,
+static __global__ void k_wire_check(const int* __restrict__ inputs, long metaOffset, long tileBytes,
                              int totalSlots, int* info, unsigned long long* cells) {
   for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < totalSlots;
        g += (long)gridDim.x * blockDim.x) {
@@ -469,7 +469,7 @@ __global__ void k_wire_check(const int* __restrict__ inputs, long metaOffset, lo
 
 // Wire buffer -> pair list: slot g of tile g / maxBatches, offsets made
 // absolute in bytes from the start of the input buffer.
-__global__ void k_wire_to_pairs(const int* __restrict__ inputs, long seqWordsPerTile, long metaOffset,
+static __global__ void k_wire_to_pairs(const int* __restrict__ inputs, long seqWordsPerTile, long metaOffset,
                                 int maxBatches, int totalSlots, PairDesc* pairs) {
   for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < totalSlots;
        g += (long)gridDim.x * blockDim.x) {

@@ -37,7 +37,7 @@ EXPORTS = [
     "ipuma_select_matrix", "ipuma_input_buffer_words", "ipuma_gpu_create", "ipuma_gpu_destroy",
     "ipuma_gpu_set_option", "ipuma_gpu_run_buffer", "ipuma_gpu_submit_buffer", "ipuma_gpu_poll",
     "ipuma_gpu_join", "ipuma_gpu_compare", "ipuma_gpu_compare_device", "ipuma_gpu_last_stats",
-    "ipuma_gpu_run_buffer_device", "ipuma_measure_int_peak",
+    "ipuma_gpu_run_buffer_device", "ipuma_measure_int_peak", "ipuma_gpu_compare_noalloc",
 ]
 
 KERNEL_NAMES = {0: "k_batched<s32,L32,K16>", 1: "k_batched<s16x2,L16,K4>",
@@ -111,6 +111,8 @@ def lib():
         L.ipuma_gpu_last_stats.argtypes = [vp, ctypes.POINTER(Stats)]
         L.ipuma_gpu_run_buffer_device.argtypes = [vp, vp, sz, vp, sz, vp]
         L.ipuma_measure_int_peak.argtypes = [i32, ctypes.POINTER(ctypes.c_double)]
+        L.ipuma_gpu_compare_noalloc.argtypes = [ctypes.POINTER(SwConfig), i32, vp, sz, vp, i32, i32,
+                                                vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -266,6 +268,16 @@ class Engine:
 
     def join(self, job: int, timeout_ms: int = -1):
         _check(lib().ipuma_gpu_join(self.h, job, timeout_ms))
+
+
+def compare_noalloc(sw: SwConfig, forward_only: bool, d_codes: int, n_codes: int, d_pairs: int,
+                    n: int, max_b: int, d_score: int, d_ar: int, d_br: int, stream: int = 0) -> int:
+    """ipuma_gpu_compare_noalloc on device pointers (ints); returns the status."""
+    return lib().ipuma_gpu_compare_noalloc(ctypes.byref(sw), int(bool(forward_only)),
+                                           ctypes.c_void_p(d_codes), n_codes,
+                                           ctypes.c_void_p(d_pairs), n, max_b,
+                                           ctypes.c_void_p(d_score), ctypes.c_void_p(d_ar),
+                                           ctypes.c_void_p(d_br), ctypes.c_void_p(stream))
 
 
 def make_pairs(a_off, a_len, b_off, b_len) -> np.ndarray:
