@@ -282,6 +282,11 @@ def main():
     sw = ib.sw_config(wl.gap_init, wl.gap_extend, wl.match, wl.mismatch, wl.ambiguity,
                       wl.similarity, wl.datatype)
     eng = ib.Engine(sw, ib.algo_config(forward_only=True), device=local)
+    t_tune = time.perf_counter()
+    eng.autotune(os.environ.get("IPUMA_TUNE_CACHE"))
+    t_tune = time.perf_counter() - t_tune
+    tuning = eng.tuning()
+    tuning["seconds"] = t_tune
     pairs_np = ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len)
     d_codes = torch.from_numpy(wl.codes).to(dev)
     d_pairs = torch.from_numpy(pairs_np.view(np.uint8)).to(dev)
@@ -346,6 +351,7 @@ def main():
         algo = ib.algo_config(tiles_used=tiles, max_batches=mb, bufsize=bufsize, max_ab=max_a,
                               forward_only=True)
         peng = ib.Engine(sw, algo, device=local)
+        peng.autotune(os.environ.get("IPUMA_TUNE_CACHE"))
         d_in = torch.from_numpy(inputs).to(dev)
         d_res = torch.zeros(3 * tiles * mb, dtype=torch.int32, device=dev)
         res = {}
@@ -451,6 +457,7 @@ def main():
             "parity": {"checked_pairs": int(chk.size), "mismatching_fields": mism,
                        "against": "oracle (C restatement of SWAffine::compute)"},
             "launch_breakdown_ms": [{"kernel": n, "ms": m, "cells": c} for n, m, c in timed],
+            "autotune": tuning,
         }
         line.update(result)
         print(json.dumps(line))

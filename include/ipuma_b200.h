@@ -171,7 +171,11 @@ void ipuma_gpu_destroy(ipuma_engine* e);
  *   "graphs"      1 = capture and replay CUDA graphs for repeated shapes
  *   "tile_k"      0 = kernel class by |A| (default); 1..6 = every pair
  *                 through s16x2 class IPUMA_KERNEL_S16_* (value = kind)
- *   "time_launches" 1 = time every alignment-kernel launch (ipuma_stats) */
+ *   "time_launches" 1 = time every alignment-kernel launch (ipuma_stats)
+ *   "autotune"    1 = measure the kernel-class rates before the first batch
+ *                 (default), 0 = built-in rates unless ipuma_gpu_autotune
+ *   "long_a"      |A| above which a pair takes the widest s16x2 class
+ *                 (default 1536): long pairs are latency-bound */
 int ipuma_gpu_set_option(ipuma_engine* e, const char* name, int64_t value);
 
 /* Runs one batch in the reference wire format and waits for it.
@@ -212,6 +216,16 @@ int ipuma_gpu_run_buffer_device(ipuma_engine* e, const int32_t* d_inputs, size_t
                                 int32_t* d_results, size_t n_results, void* stream);
 
 int ipuma_gpu_last_stats(ipuma_engine* e, ipuma_stats* out);
+
+/* Autotuner: measures, for this engine's GPU and alphabet, the rates of the
+ * kernel classes that the cost-binned scheduler chooses between (lanes per
+ * group, columns per lane), or loads them from `cache_path` (a file of
+ * tab-separated lines; NULL = the IPUMA_TUNE_CACHE environment variable or
+ * none).  Runs once per process and key; with option "autotune" = 1 (the
+ * default) the first batched call runs it implicitly. */
+int ipuma_gpu_autotune(ipuma_engine* e, const char* cache_path);
+/* Writes the rates in use as JSON text into buf. */
+int ipuma_gpu_tuning(ipuma_engine* e, char* buf, size_t cap);
 
 /* Allocation-free alignment, for callers that cannot call cudaMalloc (for
  * example code running while its stream is captured into a CUDA graph,

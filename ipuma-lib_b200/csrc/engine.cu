@@ -128,6 +128,14 @@ struct ipuma_engine {
   int tile_k = 0;
   int time_launches = 0;
 
+  // autotuned per-class rates of the class choice (BinParams)
+  float slot_ps[NCLASS_MAX] = {};
+  float strip_ps[NCLASS_MAX] = {};
+  bool tuned = false;
+  int autotune = 1;  // tune lazily before the first batched launch
+  int long_a = 1536; // |A| above which pairs take the widest class
+  std::string tune_source = "defaults";
+
   // per-launch timing of the current call (time_launches)
   cudaEvent_t tev[2 * 10] = {};
   int n_timed = 0;
@@ -151,6 +159,7 @@ constexpr int CTL_RANGES = 4;                       // 2 * NCLASS_MAX
 constexpr int CTL_HEADS = CTL_RANGES + 2 * NCLASS_MAX;  // NCLASS_MAX + 1
 constexpr int CTL_INFO = 30;                        // wire check {maxA, maxB, bad} (+1 pad)
 constexpr int CTL_CELLS = 34;                       // 8-byte aligned: NCLASS_MAX + 2 uint64
+static_assert(CTL_HEADS + NCLASS_MAX + 1 <= CTL_INFO, "control block layout");
 constexpr int CTL_HIST = CTL_CELLS + 2 * (NCLASS_MAX + 2);  // NCLASS_MAX * NBUCKET
 constexpr int CTL_OFFS = CTL_HIST + NCLASS_MAX * NBUCKET;
 constexpr int CTL_INTS = CTL_OFFS + NCLASS_MAX * NBUCKET;
@@ -266,12 +275,17 @@ int run_batched(ipuma_engine* e, cudaStream_t s, const uint8_t* codes, const Pai
   bp.nclass = kNumS16 + 1;
   bp.s16_max_len = e->s16_max_len;
   bp.force_s32 = e->s16_ok ? 0 : 1;
-  for (int c = 0; c < kNumS16; ++c) bp.k_limit[c] = kClasses[c].lanes * kClasses[c].k;
-  if (e->tile_k > 0) {
-    // Force one s16x2 class: every pair uses the chosen kernel, long A
-    // crossing several strips.
-    for (int c = 0; c < kNumS16; ++c) bp.k_limit[c] = (c == e->tile_k - 1) ? (1 << 30) : -1;
+  for (int c = 0; c <= kNumS16; ++c) {
+    bp.lanes[c] = kClasses[c].lanes;
+    bp.width[c] = kClasses[c].lanes * kClasses[c].k;
+    bp.slot_ps[c] = e->slot_ps[c];
+    bp.strip_ps[c] = e->strip_ps[c];
   }
+  bp.widest = kNumS16 - 1;
+  bp.long_a = e->long_a;
+  // tile_k > 0 forces one s16x2 class: every pair uses the chosen kernel,
+  // long A crossing several strips.
+  bp.forced_class = e->tile_k > 0 ? e->tile_k - 1 : -1;
   bp.max_a = maxA;
   bp.max_b = maxB;
   bp.M = e->M;
@@ -389,6 +403,205 @@ int validate_algo(const ipuma_algo_config* a) {
   return IPUMA_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Autotuner.  The class choice (pair_key) models a pair's time in kernel
+// class c as strips * ((|B| + lanes) * width * slot_ps[c] + strip_ps[c]).
+// The two rates per class depend on the GPU and on the alphabet (profile
+// size, occupancy), so they are measured: a synthetic batch of related pairs
+// per class at one strip of 1024 rows and at eight strips of 128 rows, every
+// pair forced through that class, gives two equations for the two unknowns.
+// Results are kept per process (by GPU, alphabet and gaps) and optionally in
+// a cache file of "key<TAB>slot_ps...<TAB>strip_ps..." lines.
+// ---------------------------------------------------------------------------
+
+void set_default_rates(ipuma_engine* e) {
+  // Measured on B200 with the nucleic-acid alphabet (uniform related pairs).
+  const float slot[kNumS16] = {0.385f, 0.286f, 0.263f, 0.25f, 0.3125f, 0.3125f};
+  for (int c = 0; c < kNumS16; ++c) {
+    e->slot_ps[c] = slot[c];
+    e->strip_ps[c] = 0.f;
+  }
+  e->tuned = false;
+  e->tune_source = "defaults";
+}
+
+std::mutex g_tune_mu;
+std::map<std::string, std::vector<float>> g_tune_cache;
+
+std::string tune_key(const ipuma_engine* e) {
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, e->device);
+  char buf[512];
+  snprintf(buf, sizeof(buf), "%s|sm%d%d|M=%d|sim=%d|gI=%d|gE=%d|v1", prop.name, prop.major, prop.minor, e->M,
+           e->sw.similarity, e->sw.gap_init, e->sw.gap_extend);
+  for (char* c = buf; *c; ++c)
+    if (*c == '\t' || *c == '\n') *c = ' ';
+  return buf;
+}
+
+void apply_rates(ipuma_engine* e, const std::vector<float>& v, const char* source) {
+  for (int c = 0; c < kNumS16; ++c) {
+    e->slot_ps[c] = v[c];
+    e->strip_ps[c] = v[kNumS16 + c];
+  }
+  e->tuned = true;
+  e->tune_source = source;
+}
+
+bool load_cache_file(const char* path, const std::string& key, std::vector<float>& v) {
+  if (!path || !*path) return false;
+  FILE* f = fopen(path, "r");
+  if (!f) return false;
+  char line[1024];
+  bool found = false;
+  while (fgets(line, sizeof(line), f)) {
+    char* tab = strchr(line, '\t');
+    if (!tab) continue;
+    *tab = 0;
+    if (key != line) continue;
+    std::vector<float> vals;
+    for (char* p = tab + 1; *p;) {
+      char* end = nullptr;
+      const float x = strtof(p, &end);
+      if (end == p) {
+        ++p;
+        continue;
+      }
+      vals.push_back(x);
+      p = end;
+    }
+    if ((int)vals.size() == 2 * kNumS16) {
+      v = vals;
+      found = true;
+    }
+  }
+  fclose(f);
+  return found;
+}
+
+void append_cache_file(const char* path, const std::string& key, const std::vector<float>& v) {
+  if (!path || !*path) return;
+  FILE* f = fopen(path, "a");
+  if (!f) return;
+  fprintf(f, "%s\t", key.c_str());
+  for (int c = 0; c < kNumS16; ++c) fprintf(f, "%s%.6g", c ? "," : "", v[c]);
+  fprintf(f, "\t");
+  for (int c = 0; c < kNumS16; ++c) fprintf(f, "%s%.6g", c ? "," : "", v[kNumS16 + c]);
+  fprintf(f, "\n");
+  fclose(f);
+}
+
+// Device time (ms) of the class-`cls` launch for n synthetic pairs.
+int time_class(ipuma_engine* e, int cls, int n, int alen, int blen, const DevBuf& letters, int nletters,
+               uint32_t seed, float* ms) {
+  cudaStream_t s = e->stream;
+  int rc;
+  const size_t bytes = (size_t)n * (alen + blen);
+  if ((rc = e->d_codes.ensure(bytes, s))) return rc;
+  if ((rc = e->d_pairs.ensure(sizeof(PairDesc) * (size_t)n, s))) return rc;
+  if ((rc = e->d_res.ensure(sizeof(int) * 3 * (size_t)n, s))) return rc;
+  const int gb = (int)std::min<size_t>((bytes + 255) / 256, (size_t)e->nsm * 16);
+  k_synth_pairs<<<gb, 256, 0, s>>>(e->d_codes.as<uint8_t>(), e->d_pairs.as<PairDesc>(), n, alen, blen,
+                                   letters.as<uint8_t>(), nletters, seed);
+  CUDA_TRY(cudaGetLastError());
+  const int savedK = e->tile_k, savedT = e->time_launches;
+  e->tile_k = cls + 1;
+  e->time_launches = 1;
+  int* out = e->d_res.as<int>();
+  *ms = -1.f;
+  for (int rep = 0; rep < 2 && rc == IPUMA_OK; ++rep) {
+    int launches = 0;
+    if ((rc = reset_ctl(e, s))) break;
+    if ((rc = run_batched(e, s, e->d_codes.as<uint8_t>(), e->d_pairs.as<PairDesc>(), n, alen, blen, out, out + n,
+                          out + 2 * n, &launches)))
+      break;
+    if ((rc = check_status(e, s))) break;
+    for (int k = 0; k < e->stats.n_timed; ++k)
+      if (e->timed_cls[k] == cls) *ms = (float)e->stats.timed_ms[k];
+  }
+  e->tile_k = savedK;
+  e->time_launches = savedT;
+  return rc;
+}
+
+int run_autotune(ipuma_engine* e, const char* cache_path) {
+  const std::string key = tune_key(e);
+  std::vector<float> v;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      apply_rates(e, it->second, "process cache");
+      return IPUMA_OK;
+    }
+  }
+  if (load_cache_file(cache_path, key, v)) {
+    apply_rates(e, v, "cache file");
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = v;
+    return IPUMA_OK;
+  }
+  if (!e->fast_ok || !e->s16_ok) return IPUMA_OK;  // nothing to choose between
+  // Letters of the alphabet that real sequences use.
+  std::vector<uint8_t> letters;
+  if (e->sw.datatype == IPUMA_DT_NUCLEIC_ACID) {
+    letters = {1, 2, 3, 4};
+  } else {
+    for (int x = 0; x < std::min(20, e->M); ++x) letters.push_back((uint8_t)x);
+  }
+  DevBuf dl;
+  int rc;
+  if ((rc = dl.ensure(letters.size(), e->stream))) return rc;
+  CUDA_TRY(cudaMemcpy(dl.p, letters.data(), letters.size(), cudaMemcpyHostToDevice));
+  v.assign(2 * kNumS16, 0.f);
+  for (int c = 0; c < kNumS16 && rc == IPUMA_OK; ++c) {
+    const int W = kClasses[c].lanes * kClasses[c].k, L = kClasses[c].lanes;
+    const int perItem = (32 / L) * 2;
+    int grid = 1;
+    switch (c) {
+      case 0: grid = batched_grid<LaneS16x2, 4, 16>(e); break;
+      case 1: grid = batched_grid<LaneS16x2, 8, 16>(e); break;
+      case 2: grid = batched_grid<LaneS16x2, 12, 16>(e); break;
+      case 3: grid = batched_grid<LaneS16x2, 16, 16>(e); break;
+      case 4: grid = batched_grid<LaneS16x2, 12, 32>(e); break;
+      default: grid = batched_grid<LaneS16x2, 16, 32>(e); break;
+    }
+    const int minPairs = grid * kWarpsPerBlock * perItem * 6;
+    const int shapes[2][3] = {{1, 1024, 0}, {8, 128, 0}};
+    double tpp[2] = {0, 0};
+    for (int sh = 0; sh < 2 && rc == IPUMA_OK; ++sh) {
+      const int alen = shapes[sh][0] * W, blen = shapes[sh][1];
+      const int n = std::max(minPairs, (int)std::min(2.0e6, 1.5e9 / ((double)alen * blen)));
+      float ms = -1.f;
+      rc = time_class(e, c, n, alen, blen, dl, (int)letters.size(), 0x5eed0000u + 16 * c + sh, &ms);
+      tpp[sh] = ms > 0 ? ms * 1e9 / n : 0;  // ps per pair
+    }
+    // tpp = strips * ((rows + L) * W * slot + strip)
+    const double a1 = (1024.0 + L) * W, a2 = 8.0 * (128.0 + L) * W;
+    const double b1 = 1.0, b2 = 8.0;
+    const double det = a1 * b2 - a2 * b1;
+    double slot = (tpp[0] * b2 - tpp[1] * b1) / det;
+    double strip = (a1 * tpp[1] - a2 * tpp[0]) / det;
+    if (slot <= 0) slot = tpp[0] / a1;
+    if (strip < 0) strip = 0;
+    v[c] = (float)slot;
+    v[kNumS16 + c] = (float)strip;
+  }
+  dl.release();
+  if (rc) return rc;
+  apply_rates(e, v, "measured");
+  append_cache_file(cache_path, key, v);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache[key] = v;
+  return IPUMA_OK;
+}
+
+int maybe_autotune(ipuma_engine* e) {
+  if (e->tuned || !e->autotune) return IPUMA_OK;
+  const char* path = getenv("IPUMA_TUNE_CACHE");
+  return run_autotune(e, path);
+}
+
 }  // namespace
 
 extern "C" {
@@ -501,6 +714,7 @@ int ipuma_gpu_create(const ipuma_sw_config* sw, const ipuma_algo_config* algo, i
   e->sc.s16Limit = 32767 - std::max(0, e->maxSub);
   e->s16_ok = e->fast_ok;
   e->s16_max_len = e->maxSub > 0 ? (e->sc.s16Limit / e->maxSub) : (1 << 30);
+  set_default_rates(e.get());
   *out = e.release();
   return IPUMA_OK;
 }
@@ -531,6 +745,11 @@ int ipuma_gpu_set_option(ipuma_engine* e, const char* name, int64_t value) {
     e->scheduler = (int)value;
   } else if (k == "graphs") {
     e->graphs = value ? 1 : 0;
+  } else if (k == "long_a") {
+    if (value < 0) return fail(IPUMA_ERR_INVALID_ARG, "long_a must be >= 0");
+    e->long_a = (int)std::min<int64_t>(value, 1 << 30);
+  } else if (k == "autotune") {
+    e->autotune = value ? 1 : 0;
   } else if (k == "time_launches") {
     e->time_launches = value ? 1 : 0;
   } else if (k == "tile_k") {
@@ -540,6 +759,29 @@ int ipuma_gpu_set_option(ipuma_engine* e, const char* name, int64_t value) {
   } else {
     return fail(IPUMA_ERR_INVALID_ARG, "unknown option '%s'", name);
   }
+  return IPUMA_OK;
+}
+
+int ipuma_gpu_autotune(ipuma_engine* e, const char* cache_path) {
+  if (!e) return fail(IPUMA_ERR_INVALID_ARG, "null engine");
+  std::lock_guard<std::mutex> lk(e->mu);
+  CUDA_TRY(cudaSetDevice(e->device));
+  if (!cache_path) cache_path = getenv("IPUMA_TUNE_CACHE");
+  return run_autotune(e, cache_path);
+}
+
+int ipuma_gpu_tuning(ipuma_engine* e, char* buf, size_t cap) {
+  if (!e || !buf || cap == 0) return fail(IPUMA_ERR_INVALID_ARG, "null argument");
+  std::string j = "{\"source\": \"" + e->tune_source + "\", \"classes\": [";
+  char tmp[256];
+  for (int c = 0; c < kNumS16; ++c) {
+    snprintf(tmp, sizeof(tmp), "%s{\"lanes\": %d, \"k\": %d, \"slot_ps\": %.5g, \"strip_ps\": %.5g}", c ? ", " : "",
+             kClasses[c].lanes, kClasses[c].k, e->slot_ps[c], e->strip_ps[c]);
+    j += tmp;
+  }
+  j += "]}";
+  if (j.size() + 1 > cap) return fail(IPUMA_ERR_INVALID_ARG, "buffer too small (%zu bytes needed)", j.size() + 1);
+  memcpy(buf, j.c_str(), j.size() + 1);
   return IPUMA_OK;
 }
 
@@ -561,9 +803,10 @@ int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_c
   std::lock_guard<std::mutex> lk(e->mu);
   CUDA_TRY(cudaSetDevice(e->device));
   cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : e->stream;
+  int rc;
+  if ((rc = maybe_autotune(e))) return rc;
   e->stats = ipuma_stats{};
   int launches = 0;
-  int rc;
   if ((rc = reset_ctl(e, s))) return rc;
   CUDA_TRY(cudaEventRecord(e->ev[1], s));
   rc = run_batched(e, s, d_codes, reinterpret_cast<const PairDesc*>(d_pairs), n, max_a_len,
@@ -604,6 +847,7 @@ int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes, con
   CUDA_TRY(cudaSetDevice(e->device));
   cudaStream_t s = e->stream;
   int rc;
+  if ((rc = maybe_autotune(e))) return rc;
   if ((rc = e->d_codes.ensure(std::max<size_t>(n_codes, 1), s))) return rc;
   if ((rc = e->d_pairs.ensure(sizeof(ipuma_pair) * (size_t)n, s))) return rc;
   if ((rc = e->d_res.ensure(sizeof(int32_t) * 3 * (size_t)n, s))) return rc;
@@ -719,6 +963,7 @@ int ipuma_gpu_run_buffer_device(ipuma_engine* e, const int32_t* d_inputs, size_t
   const ipuma_algo_config& a = e->algo;
   int rc;
   if ((rc = check_wire_sizes(a, n_inputs, n_results))) return rc;
+  if (e->scheduler == 0 && (rc = maybe_autotune(e))) return rc;
   cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : e->stream;
   const long seqWordsPerTile = (a.bufsize + 3) / 4;
   const long metaOffset = (long)a.tiles_used * seqWordsPerTile;
@@ -769,11 +1014,13 @@ int ipuma_gpu_submit_buffer(ipuma_engine* e, const int32_t* inputs, size_t n_inp
   if ((n_inputs && !inputs) || (n_results && !results)) return fail(IPUMA_ERR_INVALID_ARG, "null buffer");
   std::lock_guard<std::mutex> lk(e->mu);
   CUDA_TRY(cudaSetDevice(e->device));
+  int rc;
+  if (e->scheduler == 0 && (rc = maybe_autotune(e))) return rc;
   e->stats = ipuma_stats{};
   int launches = 0;
   int64_t cells = 0;
   CUDA_TRY(cudaEventRecord(e->ev[0], e->stream));
-  int rc = enqueue_buffer(e, inputs, n_inputs, results, n_results, &launches, &cells);
+  rc = enqueue_buffer(e, inputs, n_inputs, results, n_results, &launches, &cells);
   if (rc) return rc;
   Job j;
   CUDA_TRY(cudaEventCreateWithFlags(&j.done, cudaEventDisableTiming));

@@ -326,16 +326,18 @@ static __global__ void k_exact(SwConst sc, const int8_t* __restrict__ sim, const
 // neighbours of near-equal rows, which share a warp.  Empty pairs get their
 // zero result here and are not listed.
 // -------------------------------------------------------------------------
-constexpr int NBUCKET = 128;
+constexpr int NROWB = 256;    // row buckets (16 per power of two)
+constexpr int NSTRIPB = 16;   // strip-count buckets
+constexpr int NBUCKET = NROWB * NSTRIPB;
 constexpr int NCLASS_MAX = 8;
 
-// Log-linear bucket of |B| (8 sub-buckets per power of two): pairs that
-// share a bucket differ by at most 1/8 in rows, so the groups of a warp
+// Log-linear bucket of |B| (16 sub-buckets per power of two): pairs that
+// share a bucket differ by at most 1/16 in rows, so the groups of a warp
 // finish their wavefronts together.
 __device__ __forceinline__ int rows_bucket(int b) {
-  if (b < 8) return b;
+  if (b < 16) return b;
   const int lg = 31 - __clz(b);
-  return min(NBUCKET - 1, (lg - 2) * 8 + ((b >> (lg - 3)) & 7));
+  return min(NROWB - 1, (lg - 3) * 16 + ((b >> (lg - 4)) & 15));
 }
 
 struct BinParams {
@@ -343,7 +345,13 @@ struct BinParams {
   int cls_s32;             // class index of the exact-32-bit kernel
   int s16_max_len;         // min(|A|,|B|) above which s16x2 could overflow
   int s16_limit;           // scores above this need s32 lanes
-  int k_limit[NCLASS_MAX]; // s16x2 class c takes |A| <= k_limit[c] (last: any)
+  int lanes[NCLASS_MAX];   // lanes per group of each class
+  int width[NCLASS_MAX];   // strip width (lanes * K) of each class
+  float slot_ps[NCLASS_MAX];   // time per cell slot of a strip (autotuned)
+  float strip_ps[NCLASS_MAX];  // fixed time per strip (autotuned)
+  int long_a;                  // |A| above which the widest class is used
+  int widest;                  // that class
+  int forced_class;        // >= 0: every s16x2 pair goes to this class
   int n_s16_classes;
   int max_a, max_b;        // stated maxima (violations set ERR_LENGTH)
   int M;                   // alphabet size of `sim`
@@ -362,19 +370,39 @@ static __device__ int diagonal_bound(const uint8_t* a, const uint8_t* b, int n, 
   return best;
 }
 
+// Class of a pair: the kernel with the lowest modelled time
+//   strips * ((|B| + lanes) * width * slot_ps + strip_ps)
+// where strips * width covers |A|, |B| + lanes counts the fill and drain of
+// each strip's wavefront, and slot_ps / strip_ps are the per-class rates
+// the autotuner measured.  Key = class, then strip count (descending), then
+// rows (descending).
 __device__ __forceinline__ int pair_key(const BinParams& bp, int alen, int blen, bool s32) {
   int cls;
   if (bp.force_s32 || s32) {
     cls = bp.cls_s32;
+  } else if (bp.forced_class >= 0) {
+    cls = bp.forced_class;
+  } else if (alen > bp.long_a) {
+    // Very long pairs are few and each keeps one warp busy for long: their
+    // latency, not throughput, sets the end of the launch, and the widest
+    // strips finish a pair in the fewest steps.
+    cls = bp.widest;
   } else {
-    cls = bp.n_s16_classes - 1;
-    for (int c = 0; c < bp.n_s16_classes - 1; ++c)
-      if (alen <= bp.k_limit[c]) {
+    cls = 0;
+    float bestCost = -1.f;
+    for (int c = 0; c < bp.n_s16_classes; ++c) {
+      const int strips = (alen + bp.width[c] - 1) / bp.width[c];
+      const float cost =
+          (float)strips * ((float)(blen + bp.lanes[c]) * (float)bp.width[c] * bp.slot_ps[c] + bp.strip_ps[c]);
+      if (bestCost < 0.f || cost < bestCost) {
+        bestCost = cost;
         cls = c;
-        break;
       }
+    }
   }
-  return cls * NBUCKET + (NBUCKET - 1 - rows_bucket(blen));
+  const int strips = (alen + bp.width[cls] - 1) / bp.width[cls];
+  const int sb = NSTRIPB - 1 - min(strips - 1, NSTRIPB - 1);
+  return cls * NBUCKET + sb * NROWB + (NROWB - 1 - rows_bucket(blen));
 }
 
 static __global__ void k_bin_count(BinParams bp, const uint8_t* __restrict__ codes, const int8_t* __restrict__ sim,
@@ -407,6 +435,10 @@ static __global__ void k_bin_count(BinParams bp, const uint8_t* __restrict__ cod
   }
 }
 
+__device__ __forceinline__ int run_total(const int* hist, const int* offs, int nkeys) {
+  return offs[nkeys - 1] + hist[nkeys - 1];
+}
+
 // Single block: exclusive scan of the histogram into `offs`, and per class
 // the {start, count} range consumed by k_batched.
 static __global__ void k_bin_scan(int nkeys, const int* hist, int* offs, int* class_range) {
@@ -431,10 +463,9 @@ static __global__ void k_bin_scan(int nkeys, const int* hist, int* offs, int* cl
   __syncthreads();
   if (tid < nkeys / NBUCKET) {
     const int c = tid;
-    int cnt = 0;
-    for (int b = 0; b < NBUCKET; ++b) cnt += hist[c * NBUCKET + b];
     class_range[2 * c] = offs[c * NBUCKET];
-    class_range[2 * c + 1] = cnt;
+    class_range[2 * c + 1] = ((c + 1) * NBUCKET < nkeys ? offs[(c + 1) * NBUCKET] : run_total(hist, offs, nkeys)) -
+                             offs[c * NBUCKET];
   }
 }
 
@@ -445,6 +476,36 @@ static __global__ void k_bin_scatter(BinParams bp, const PairDesc* __restrict__ 
     if (d.a_len <= 0 || d.b_len <= 0 || d.a_len > bp.max_a || d.b_len > bp.max_b) continue;
     const int pos = atomicAdd(&offs[pair_key(bp, d.a_len, d.b_len, s32_flag[p] != 0)], 1);
     list[pos] = (int)p;
+  }
+}
+
+// Synthetic calibration batch for the autotuner: n pairs of |A| = alen,
+// |B| = blen; A uniform over `letters`, B = A with 1 in 8 residues
+// substituted, then random letters past |A|.
+static __global__ void k_synth_pairs(uint8_t* codes, PairDesc* pairs, int n, int alen, int blen,
+                                     const uint8_t* __restrict__ letters, int nletters, uint32_t seed) {
+  const long per = (long)alen + blen;
+  for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < (long)n * per;
+       k += (long)gridDim.x * blockDim.x) {
+    const long p = k / per, i = k % per;
+    auto hash = [&](long x) {
+      uint32_t h = (uint32_t)x * 0x9E3779B1u ^ seed;
+      h ^= h >> 15;
+      h *= 0x85EBCA77u;
+      h ^= h >> 13;
+      h *= 0xC2B2AE3Du;
+      return h ^ (h >> 16);
+    };
+    uint8_t v;
+    if (i < alen) {
+      v = letters[hash(p * 131071 + i) % nletters];
+    } else {
+      const long j = i - alen;
+      const uint32_t r = hash(p * 524287 + j + 7);
+      v = (j < alen && (r & 7)) ? letters[hash(p * 131071 + j) % nletters] : letters[(r >> 3) % nletters];
+    }
+    codes[k] = v;
+    if (i == 0) pairs[p] = PairDesc{p * per, p * per + alen, alen, blen};
   }
 }
 

@@ -38,6 +38,7 @@ EXPORTS = [
     "ipuma_gpu_set_option", "ipuma_gpu_run_buffer", "ipuma_gpu_submit_buffer", "ipuma_gpu_poll",
     "ipuma_gpu_join", "ipuma_gpu_compare", "ipuma_gpu_compare_device", "ipuma_gpu_last_stats",
     "ipuma_gpu_run_buffer_device", "ipuma_measure_int_peak", "ipuma_gpu_compare_noalloc",
+    "ipuma_gpu_autotune", "ipuma_gpu_tuning",
 ]
 
 KERNEL_NAMES = {0: "k_batched<s32,L32,K16>", 1: "k_batched<s16x2,L16,K4>",
@@ -111,6 +112,8 @@ def lib():
         L.ipuma_gpu_last_stats.argtypes = [vp, ctypes.POINTER(Stats)]
         L.ipuma_gpu_run_buffer_device.argtypes = [vp, vp, sz, vp, sz, vp]
         L.ipuma_measure_int_peak.argtypes = [i32, ctypes.POINTER(ctypes.c_double)]
+        L.ipuma_gpu_autotune.argtypes = [vp, ctypes.c_char_p]
+        L.ipuma_gpu_tuning.argtypes = [vp, ctypes.c_char_p, sz]
         L.ipuma_gpu_compare_noalloc.argtypes = [ctypes.POINTER(SwConfig), i32, vp, sz, vp, i32, i32,
                                                 vp, vp, vp, vp]
         _lib = L
@@ -210,6 +213,15 @@ class Engine:
 
     def set_option(self, name: str, value: int):
         _check(lib().ipuma_gpu_set_option(self.h, name.encode(), int(value)))
+
+    def autotune(self, cache_path: str | None = None):
+        _check(lib().ipuma_gpu_autotune(self.h, cache_path.encode() if cache_path else None))
+
+    def tuning(self) -> dict:
+        import json
+        buf = ctypes.create_string_buffer(4096)
+        _check(lib().ipuma_gpu_tuning(self.h, buf, 4096))
+        return json.loads(buf.value.decode())
 
     def stats(self) -> Stats:
         st = Stats()
