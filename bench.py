@@ -299,9 +299,12 @@ def main():
                            max_b, d_out[0].data_ptr(), d_out[1].data_ptr(), d_out[2].data_ptr(),
                            stream.cuda_stream)
 
+    # The timed steps replay the captured pipeline (CUDA graph) of this shape.
+    eng.set_option("graphs", 1)
     for _ in range(args.warmup):
         step()
     launches_per_step = eng.stats().launches
+    used_graph = bool(eng.stats().used_graph)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -324,11 +327,13 @@ def main():
     total_cells = wl.cells * ws
     value = total_cells / (ms_step * 1e-3) / 1e9
 
-    # Per-launch timing of one extra step (outside the timed region).
+    # Per-launch timing of one extra step (outside the timed region; events
+    # around each launch, so without the graph).
     eng.set_option("time_launches", 1)
     step()
     st = eng.stats()
     eng.set_option("time_launches", 0)
+    eng.set_option("graphs", 0)
     timed = [(ib.KERNEL_NAMES.get(st.timed_kind[k], str(st.timed_kind[k])), st.timed_ms[k],
               st.timed_cells[k]) for k in range(st.n_timed)]
     dom = max(timed, key=lambda x: x[1]) if timed else None
@@ -447,7 +452,8 @@ def main():
                        "seed": wl.seed, "scoring": "%s match %d mismatch %d gapInit %d gapExtend %d"
                        % (wl.similarity, wl.match, wl.mismatch, wl.gap_init, wl.gap_extend),
                        "l2": "inputs larger than L2 (%.0f MB codes per GPU)" % (wl.codes.nbytes / 1e6),
-                       "engine": "persistent cost-binned (compare_device)"},
+                       "engine": "persistent cost-binned (compare_device)",
+                       "cuda_graph": used_graph},
             "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps,
             "roofline": rl,

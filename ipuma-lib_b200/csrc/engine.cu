@@ -143,6 +143,10 @@ struct ipuma_engine {
   int timed_cls[10] = {};
 
   DevBuf d_sim, d_codes, d_pairs, d_list, d_res, d_scratch, d_cf, d_ovf, d_ctl, d_inputs, d_wres, d_flag;
+  std::map<const void*, std::pair<int, int>> grid_cache;  // kernel -> {smem, grid}
+  // Captured pipelines of compare_device, by shape and buffers (option "graphs").
+  std::map<std::vector<uint64_t>, cudaGraphExec_t> graphs_cache;
+  std::map<cudaGraphExec_t, int> graph_launches;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   ipuma_stats stats{};
   std::mutex mu;
@@ -166,12 +170,19 @@ constexpr int CTL_INTS = CTL_OFFS + NCLASS_MAX * NBUCKET;
 constexpr int CELLS_RERUN = NCLASS_MAX;             // index of the rerun cells
 constexpr int CELLS_WIRE = NCLASS_MAX + 1;          // cells found by the wire check
 
+// Persistent grid of a kernel: resident blocks per SM times SMs.  Computed
+// once per kernel and engine (engine creation warms the cache, so no
+// occupancy query or attribute change happens during a graph capture).
 template <class K>
 int occupancy_grid(ipuma_engine* e, K kernel, int smem) {
+  const void* key = reinterpret_cast<const void*>(kernel);
+  auto it = e->grid_cache.find(key);
+  if (it != e->grid_cache.end() && it->second.first == smem) return it->second.second;
   int nb = 0;
   if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, kThreads, smem);
   if (nb < 1) nb = 1;
+  e->grid_cache[key] = {smem, nb * e->nsm};
   return nb * e->nsm;
 }
 
@@ -235,6 +246,20 @@ int launch_batched(ipuma_engine* e, cudaStream_t s, const uint8_t* codes, const 
       reinterpret_cast<DevStatus*>(ctl + CTL_STATUS));
   CUDA_TRY(cudaGetLastError());
   return timed_end(e, s);
+}
+
+// Grows every buffer run_batched uses for a batch of this shape, so that
+// the pipeline itself allocates nothing (graph capture).
+int reserve_batched(ipuma_engine* e, cudaStream_t s, int n, int maxA, int maxB) {
+  int rc;
+  const long rowsCap = std::max(1, maxB);
+  if ((rc = e->d_ctl.ensure(sizeof(int) * CTL_INTS, s))) return rc;
+  if ((rc = e->d_scratch.ensure(sizeof(int2) * 2 * rowsCap * max_batched_groups(e), s))) return rc;
+  if ((rc = e->d_list.ensure(sizeof(int) * (size_t)n + 64, s))) return rc;
+  if ((rc = e->d_ovf.ensure(sizeof(int) * (size_t)n + 64, s))) return rc;
+  if ((rc = e->d_flag.ensure((size_t)n + 64, s))) return rc;
+  (void)maxA;
+  return IPUMA_OK;
 }
 
 // Runs the persistent cost-binned pipeline over n device-resident pairs.
@@ -715,6 +740,7 @@ int ipuma_gpu_create(const ipuma_sw_config* sw, const ipuma_algo_config* algo, i
   e->s16_ok = e->fast_ok;
   e->s16_max_len = e->maxSub > 0 ? (e->sc.s16Limit / e->maxSub) : (1 << 30);
   set_default_rates(e.get());
+  max_batched_groups(e.get());  // warm the grid cache
   *out = e.release();
   return IPUMA_OK;
 }
@@ -732,6 +758,7 @@ void ipuma_gpu_destroy(ipuma_engine* e) {
     if (ev) cudaEventDestroy(ev);
   for (auto& ev : e->tev)
     if (ev) cudaEventDestroy(ev);
+  for (auto& kv : e->graphs_cache) cudaGraphExecDestroy(kv.second);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
 }
@@ -807,11 +834,52 @@ int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_c
   if ((rc = maybe_autotune(e))) return rc;
   e->stats = ipuma_stats{};
   int launches = 0;
-  if ((rc = reset_ctl(e, s))) return rc;
-  CUDA_TRY(cudaEventRecord(e->ev[1], s));
-  rc = run_batched(e, s, d_codes, reinterpret_cast<const PairDesc*>(d_pairs), n, max_a_len,
-                   max_b_len, d_score, d_arange, d_brange, &launches);
-  if (rc) return rc;
+  if (e->graphs && !e->time_launches && e->fast_ok && n > 0) {
+    // Replay (or capture, then replay) the whole pipeline as one graph.
+    if ((rc = reserve_batched(e, s, n, max_a_len, max_b_len))) return rc;
+    const std::vector<uint64_t> key = {(uint64_t)(uintptr_t)d_codes, (uint64_t)(uintptr_t)d_pairs, (uint64_t)n,
+                                       (uint64_t)max_a_len, (uint64_t)max_b_len, (uint64_t)(uintptr_t)d_score,
+                                       (uint64_t)(uintptr_t)d_arange, (uint64_t)(uintptr_t)d_brange,
+                                       (uint64_t)(uintptr_t)e->d_scratch.p, (uint64_t)e->d_scratch.cap,
+                                       (uint64_t)(uintptr_t)e->d_list.p, (uint64_t)(uintptr_t)e->d_ctl.p,
+                                       (uint64_t)(uintptr_t)e->d_ovf.p, (uint64_t)(uintptr_t)e->d_flag.p,
+                                       (uint64_t)e->tile_k, (uint64_t)e->long_a};
+    auto it = e->graphs_cache.find(key);
+    if (it == e->graphs_cache.end()) {
+      if (e->graphs_cache.size() >= 16) {
+        cudaGraphExecDestroy(e->graphs_cache.begin()->second);
+        e->graphs_cache.erase(e->graphs_cache.begin());
+      }
+      cudaGraph_t g = nullptr;
+      CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      int crc = reset_ctl(e, s);
+      if (!crc)
+        crc = run_batched(e, s, d_codes, reinterpret_cast<const PairDesc*>(d_pairs), n, max_a_len, max_b_len,
+                          d_score, d_arange, d_brange, &launches);
+      cudaError_t ce = cudaStreamEndCapture(s, &g);
+      if (crc) {
+        if (g) cudaGraphDestroy(g);
+        return crc;
+      }
+      if (ce != cudaSuccess) return fail(IPUMA_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+      cudaGraphExec_t ex = nullptr;
+      ce = cudaGraphInstantiate(&ex, g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess) return fail(IPUMA_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(ce));
+      it = e->graphs_cache.emplace(key, ex).first;
+      e->graph_launches[ex] = launches;
+    }
+    launches = e->graph_launches[it->second];
+    CUDA_TRY(cudaEventRecord(e->ev[1], s));
+    CUDA_TRY(cudaGraphLaunch(it->second, s));
+    e->stats.used_graph = 1;
+  } else {
+    if ((rc = reset_ctl(e, s))) return rc;
+    CUDA_TRY(cudaEventRecord(e->ev[1], s));
+    rc = run_batched(e, s, d_codes, reinterpret_cast<const PairDesc*>(d_pairs), n, max_a_len,
+                     max_b_len, d_score, d_arange, d_brange, &launches);
+    if (rc) return rc;
+  }
   CUDA_TRY(cudaEventRecord(e->ev[2], s));
   if ((rc = check_status(e, s))) return rc;
   float ms = 0;

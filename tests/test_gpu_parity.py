@@ -303,3 +303,33 @@ def test_async_jobs_poll_and_join():
     w = oracle.sw_batch(wl.codes, wl.a_off, wl.a_len, wl.b_off, wl.b_len, sim, 0, -1)
     for o in outs:
         _assert_same((o[slot_of], o[total + slot_of], o[2 * total + slot_of]), w, "async")
+
+
+# ------------------------------------------------------------- graphs ---
+
+def test_graph_replay_matches_direct_launches():
+    """Option "graphs": the binning + kernel pipeline is captured once and
+    replayed for repeated shapes; results must equal direct launches."""
+    import torch
+    wl = workloads.protein(n=1500, seed=71)
+    case = _wl_case(wl)
+    dev = torch.device("cuda", 0)
+    d_codes = torch.from_numpy(wl.codes).to(dev)
+    d_pairs = torch.from_numpy(ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len).view(np.uint8)).to(dev)
+    outs = []
+    for graphs in (0, 1, 1):
+        out = torch.full((3, wl.n), -1, dtype=torch.int32, device=dev)
+        with _engine(case, False, graphs=graphs) as e:
+            for _ in range(2 if graphs else 1):
+                e.compare_device(d_codes.data_ptr(), d_codes.numel(), d_pairs.data_ptr(), wl.n,
+                                 int(wl.a_len.max()), int(wl.b_len.max()), out[0].data_ptr(),
+                                 out[1].data_ptr(), out[2].data_ptr())
+                assert e.stats().used_graph == graphs
+        torch.cuda.synchronize()
+        outs.append(out.cpu().numpy())
+    np.testing.assert_array_equal(outs[0], outs[1])
+    np.testing.assert_array_equal(outs[0], outs[2])
+    sim = oracle.select_matrix(wl.similarity)
+    want = oracle.sw_batch(wl.codes, wl.a_off, wl.a_len, wl.b_off, wl.b_len, sim, wl.gap_init,
+                           wl.gap_extend)
+    _assert_same(tuple(outs[1]), want, "graphs")
