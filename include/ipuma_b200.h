@@ -175,7 +175,7 @@ void ipuma_gpu_destroy(ipuma_engine* e);
  *   "autotune"    1 = measure the kernel-class rates before the first batch
  *                 (default), 0 = built-in rates unless ipuma_gpu_autotune
  *   "long_a"      |A| above which a pair takes the widest s16x2 class
- *                 (default 1536): long pairs are latency-bound */
+ *                 (default 3072): long pairs are latency-bound */
 int ipuma_gpu_set_option(ipuma_engine* e, const char* name, int64_t value);
 
 /* Runs one batch in the reference wire format and waits for it.
@@ -245,6 +245,56 @@ int ipuma_gpu_tuning(ipuma_engine* e, char* buf, size_t cap);
 int ipuma_gpu_compare_noalloc(const ipuma_sw_config* sw, int32_t forward_only, const uint8_t* d_codes,
                               size_t n_codes, const ipuma_pair* d_pairs, int32_t n, int32_t max_b_len,
                               int32_t* d_score, int32_t* d_arange, int32_t* d_brange, void* stream);
+
+/* ---- serving loop ------------------------------------------------------- */
+/* Continuous batching of alignment requests on one GPU: requests queue on
+ * the host; `slots` workers (one engine and CUDA stream each) take whatever
+ * is queued for one scoring configuration into a device batch, so requests
+ * that arrive while others run join the next batch and batches of
+ * different slots overlap on the device.  Batches get their device memory
+ * from a pool allocated when the server starts (admission by free HBM: a
+ * batch waits until the pool has room).  No counterpart API in the
+ * reference; it generalises the pipelined use of
+ * async_submit_prepared_remote_compare / blocking_join (ipusw). */
+typedef struct ipuma_server_config {
+  int32_t n_scorings;              /* scoring configurations; requests pick one by index */
+  const ipuma_sw_config* scorings;
+  int32_t forward_only;            /* 1: no reverse pass (start coordinates 0) */
+  int32_t slots;                   /* concurrent device batches; 0 = 4 */
+  int64_t pool_bytes;              /* device pool; 0 = a quarter of the free memory */
+  int32_t max_batch_pairs;         /* pairs per device batch; 0 = 65536 */
+  int32_t device;
+  int32_t one_request_per_batch;   /* 1: no coalescing (each batch = one request or
+                                      part of one), the per-request baseline */
+} ipuma_server_config;
+
+typedef struct ipuma_server_stats {
+  int64_t submitted, completed, queued, batches, pairs, cells;
+  int64_t max_batch_pairs;         /* largest batch formed */
+  int64_t pool_bytes, pool_used, max_pool_used;
+  double busy_ms;                  /* summed slot time with a batch in flight */
+} ipuma_server_stats;
+
+typedef struct ipuma_server ipuma_server;
+
+int ipuma_server_create(const ipuma_server_config* cfg, ipuma_server** out);
+/* Queues one request (the buffers are copied before the call returns).
+ * IPUMA_ERR_CLOSED after ipuma_server_destroy began; IPUMA_ERR_NO_MEMORY
+ * when one of its pairs cannot fit the device pool. */
+int ipuma_server_submit(ipuma_server* s, int32_t kind, const uint8_t* codes, size_t n_codes,
+                        const ipuma_pair* pairs, int32_t n, uint64_t* req);
+int ipuma_server_poll(ipuma_server* s, uint64_t req, int32_t* done);
+/* Waits for a request (timeout_ms < 0: no limit) and copies its results
+ * (in pair order) and its latency from submission to completion.  A
+ * request id is released by a successful or failed wait. */
+int ipuma_server_wait(ipuma_server* s, uint64_t req, int64_t timeout_ms, int32_t* score, int32_t* arange,
+                      int32_t* brange, double* latency_ms);
+int ipuma_server_get_stats(ipuma_server* s, ipuma_server_stats* out);
+/* Stops accepting requests (submit returns IPUMA_ERR_CLOSED); queued and
+ * running work still completes and can be waited for. */
+int ipuma_server_close(ipuma_server* s);
+/* Closes, finishes queued and running work, then releases the server. */
+void ipuma_server_destroy(ipuma_server* s);
 
 /* Measures, on `device`, the issue rate of the s16x2 instruction mix of one
  * cell update (3 add, 2 viaddmax, 1 vimax3.relu, 1 max) in lane-ops per

@@ -133,7 +133,7 @@ struct ipuma_engine {
   float strip_ps[NCLASS_MAX] = {};
   bool tuned = false;
   int autotune = 1;  // tune lazily before the first batched launch
-  int long_a = 1536; // |A| above which pairs take the widest class
+  int long_a = 3072; // |A| above which pairs take the widest class
   std::string tune_source = "defaults";
 
   // per-launch timing of the current call (time_launches)

@@ -1,0 +1,478 @@
+// server.cu -- the serving loop: continuous batching of alignment requests.
+//
+// Requests (host code arrays + pairs, one scoring configuration each) are
+// queued by ipuma_server_submit and returned through ipuma_server_wait.
+// `slots` worker threads, each with its own engine and CUDA stream, take
+// whatever is queued -- the head request's scoring, as many of its pairs
+// and of the following requests' as fit a device batch -- stage it through
+// pinned memory into a region of the server's device pool, run the
+// cost-binned engine on it and scatter the results back per request.  A
+// request that arrives while batches run on other slots joins the next
+// batch a slot forms, so work of different requests overlaps on the
+// device; a large request is split across batches.
+//
+// Admission by free HBM: the device pool (one allocation made when the
+// server starts, sized from the free device memory) is carved per batch by
+// a first-fit allocator; a slot that cannot get the bytes for its batch
+// waits until running batches return theirs.  A request that cannot fit
+// even an empty pool is refused at submission.
+//
+// Failure handling is on the host: a closed server refuses submissions,
+// waits have timeouts, and a failing batch marks its requests failed
+// (their waiters get the error) without stopping the other slots.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "errors.h"
+#include "ipuma_b200.h"
+
+using ipuma_internal::fail;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+  uint64_t id = 0;
+  int kind = 0;
+  std::vector<uint8_t> codes;
+  std::vector<ipuma_pair> pairs;
+  std::vector<int32_t> score, arange, brange;
+  int64_t cells = 0;
+  int next = 0;          // first pair not yet given to a batch
+  int outstanding = 0;   // pairs in batches not yet finished
+  int error = IPUMA_OK;
+  std::string message;
+  bool done = false;
+  Clock::time_point t_submit, t_done;
+};
+
+// Part of a request carried by one batch.
+struct Chunk {
+  std::shared_ptr<Request> req;
+  int first, count;
+};
+
+// First-fit allocator over the device pool (offsets in bytes).
+class Pool {
+ public:
+  explicit Pool(size_t size) : size_(size) { free_[0] = size; }
+  bool alloc(size_t bytes, size_t* off) {
+    bytes = (bytes + 255) & ~size_t(255);
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second >= bytes) {
+        *off = it->first;
+        const size_t rest = it->second - bytes, at = it->first + bytes;
+        free_.erase(it);
+        if (rest) free_[at] = rest;
+        used_ += bytes;
+        return true;
+      }
+    }
+    return false;
+  }
+  void release(size_t off, size_t bytes) {
+    bytes = (bytes + 255) & ~size_t(255);
+    used_ -= bytes;
+    auto it = free_.emplace(off, bytes).first;
+    auto next = std::next(it);
+    if (next != free_.end() && it->first + it->second == next->first) {
+      it->second += next->second;
+      free_.erase(next);
+    }
+    if (it != free_.begin()) {
+      auto prev = std::prev(it);
+      if (prev->first + prev->second == it->first) {
+        prev->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+  size_t size() const { return size_; }
+  size_t used() const { return used_; }
+
+ private:
+  size_t size_, used_ = 0;
+  std::map<size_t, size_t> free_;
+};
+
+size_t batch_bytes(size_t codes, size_t pairs) {
+  auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+  return up(codes) + up(pairs * sizeof(ipuma_pair)) + up(pairs * 3 * sizeof(int32_t));
+}
+
+}  // namespace
+
+struct ipuma_server {
+  ipuma_server_config cfg{};
+  std::vector<ipuma_sw_config> scorings;
+  int device = 0;
+  uint8_t* d_pool = nullptr;
+  std::unique_ptr<Pool> pool;
+  std::mutex mu;
+  std::condition_variable cv_work;  // work queued / pool freed / closing
+  std::condition_variable cv_done;  // a request finished
+  std::deque<std::shared_ptr<Request>> queue;  // requests with pairs not yet batched
+  std::map<uint64_t, std::shared_ptr<Request>> live;
+  uint64_t next_id = 1;
+  bool closing = false;
+  std::vector<std::thread> workers;
+  // statistics
+  int64_t submitted = 0, completed = 0, batches = 0, pairs_done = 0, cells_done = 0;
+  int64_t max_batch_pairs_seen = 0, max_pool_used = 0;
+  double busy_ms = 0;
+};
+
+namespace {
+
+struct SlotState {
+  std::vector<ipuma_engine*> engines;  // one per scoring, created lazily
+  cudaStream_t stream = nullptr;
+  uint8_t* h_codes = nullptr;
+  ipuma_pair* h_pairs = nullptr;
+  int32_t* h_out = nullptr;
+  size_t cap_codes = 0, cap_pairs = 0;
+};
+
+void finish_request(ipuma_server* s, const std::shared_ptr<Request>& r) {
+  r->done = true;
+  r->t_done = Clock::now();
+  s->completed++;
+}
+
+void fail_chunks(ipuma_server* s, std::vector<Chunk>& chunks, int code, const std::string& msg) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  for (auto& c : chunks) {
+    c.req->error = code;
+    c.req->message = msg;
+    c.req->outstanding -= c.count;
+    if (c.req->outstanding == 0 && c.req->next >= (int)c.req->pairs.size()) finish_request(s, c.req);
+  }
+  s->cv_done.notify_all();
+}
+
+void worker_loop(ipuma_server* s, int slot_index) {
+  SlotState st;
+  st.engines.assign(s->scorings.size(), nullptr);
+  cudaSetDevice(s->device);
+  cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking);
+  st.cap_pairs = (size_t)s->cfg.max_batch_pairs;
+  st.cap_codes = st.cap_pairs * 2048;  // grows on demand
+  cudaHostAlloc((void**)&st.h_codes, st.cap_codes, cudaHostAllocDefault);
+  cudaHostAlloc((void**)&st.h_pairs, st.cap_pairs * sizeof(ipuma_pair), cudaHostAllocDefault);
+  cudaHostAlloc((void**)&st.h_out, st.cap_pairs * 3 * sizeof(int32_t), cudaHostAllocDefault);
+  (void)slot_index;
+
+  while (true) {
+    std::vector<Chunk> chunks;
+    size_t codes_bytes = 0, npairs = 0, pool_off = 0, pool_len = 0;
+    int kind = 0;
+    int maxA = 1, maxB = 1;
+    int64_t cells = 0;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_work.wait(lk, [&] { return s->closing || !s->queue.empty(); });
+      if (s->queue.empty()) break;  // closing and drained
+      // Continuous batching: the head request's scoring, then every queued
+      // request of that scoring that still fits this batch.
+      kind = s->queue.front()->kind;
+      for (auto it = s->queue.begin(); it != s->queue.end() && npairs < st.cap_pairs;) {
+        auto& r = *it;
+        if (r->kind != kind) {
+          ++it;
+          continue;
+        }
+        int take = 0;
+        size_t bytes = 0;
+        while (r->next + take < (int)r->pairs.size() && npairs + take < st.cap_pairs) {
+          const ipuma_pair& p = r->pairs[r->next + take];
+          const size_t add = (size_t)p.a_len + (size_t)p.b_len;
+          if (npairs + take > 0 && batch_bytes(codes_bytes + bytes + add, npairs + take + 1) > s->pool->size() / 2)
+            break;
+          bytes += add;
+          ++take;
+        }
+        if (take == 0) break;
+        chunks.push_back({r, r->next, take});
+        r->next += take;
+        r->outstanding += take;
+        npairs += take;
+        codes_bytes += bytes;
+        if (r->next >= (int)r->pairs.size())
+          it = s->queue.erase(it);
+        else
+          break;  // batch full
+        if (s->cfg.one_request_per_batch) break;
+      }
+      // Admission by free device memory: wait for the pool.
+      pool_len = batch_bytes(std::max<size_t>(codes_bytes, 1), npairs);
+      // (A batch never exceeds half the pool and slots holding pool bytes
+      // are running, so this wait ends.)
+      while (!s->pool->alloc(pool_len, &pool_off)) s->cv_work.wait_for(lk, std::chrono::milliseconds(5));
+      s->max_pool_used = std::max<int64_t>(s->max_pool_used, (int64_t)s->pool->used());
+    }
+    // Stage the batch in pinned memory (pair offsets rebased).
+    if (codes_bytes > st.cap_codes) {
+      cudaFreeHost(st.h_codes);
+      st.cap_codes = codes_bytes * 2;
+      cudaHostAlloc((void**)&st.h_codes, st.cap_codes, cudaHostAllocDefault);
+    }
+    size_t pos = 0, k = 0;
+    for (auto& c : chunks) {
+      const Request& r = *c.req;
+      for (int i = 0; i < c.count; ++i, ++k) {
+        const ipuma_pair& p = r.pairs[c.first + i];
+        ipuma_pair q{(int64_t)pos, (int64_t)(pos + p.a_len), p.a_len, p.b_len};
+        std::memcpy(st.h_codes + pos, r.codes.data() + p.a_off, p.a_len);
+        std::memcpy(st.h_codes + pos + p.a_len, r.codes.data() + p.b_off, p.b_len);
+        pos += (size_t)p.a_len + p.b_len;
+        st.h_pairs[k] = q;
+        maxA = std::max(maxA, p.a_len);
+        maxB = std::max(maxB, p.b_len);
+        cells += (int64_t)p.a_len * p.b_len;
+      }
+    }
+    uint8_t* d_codes = s->d_pool + pool_off;
+    size_t o = (std::max<size_t>(codes_bytes, 1) + 255) & ~size_t(255);
+    ipuma_pair* d_pairs = reinterpret_cast<ipuma_pair*>(s->d_pool + pool_off + o);
+    o += (npairs * sizeof(ipuma_pair) + 255) & ~size_t(255);
+    int32_t* d_out = reinterpret_cast<int32_t*>(s->d_pool + pool_off + o);
+    const auto t0 = Clock::now();
+    int rc = IPUMA_OK;
+    std::string msg;
+    if (!st.engines[kind]) {
+      ipuma_algo_config algo{1, 300, 20, 3000, 0, 0, s->cfg.forward_only, 0, 1, 0};
+      rc = ipuma_gpu_create(&s->scorings[kind], &algo, s->device, &st.engines[kind]);
+      if (rc) msg = ipuma_last_error();
+    }
+    if (rc == IPUMA_OK && npairs > 0) {
+      if (cudaMemcpyAsync(d_codes, st.h_codes, codes_bytes, cudaMemcpyHostToDevice, st.stream) != cudaSuccess ||
+          cudaMemcpyAsync(d_pairs, st.h_pairs, npairs * sizeof(ipuma_pair), cudaMemcpyHostToDevice, st.stream) !=
+              cudaSuccess) {
+        rc = IPUMA_ERR_CUDA;
+        msg = "copy to the device failed";
+      }
+    }
+    if (rc == IPUMA_OK && npairs > 0) {
+      rc = ipuma_gpu_compare_device(st.engines[kind], d_codes, codes_bytes, d_pairs, (int32_t)npairs, maxA, maxB,
+                                    d_out, d_out + npairs, d_out + 2 * npairs, st.stream);
+      if (rc) msg = ipuma_last_error();
+    }
+    if (rc == IPUMA_OK && npairs > 0) {
+      if (cudaMemcpyAsync(st.h_out, d_out, npairs * 3 * sizeof(int32_t), cudaMemcpyDeviceToHost, st.stream) !=
+              cudaSuccess ||
+          cudaStreamSynchronize(st.stream) != cudaSuccess) {
+        rc = IPUMA_ERR_CUDA;
+        msg = "copy from the device failed";
+      }
+    }
+    const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->pool->release(pool_off, pool_len);
+      s->busy_ms += ms;
+    }
+    s->cv_work.notify_all();
+    if (rc != IPUMA_OK) {
+      fail_chunks(s, chunks, rc, msg);
+      continue;
+    }
+    // Scatter results back per request.
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      size_t idx = 0;
+      for (auto& c : chunks) {
+        Request& r = *c.req;
+        for (int i = 0; i < c.count; ++i, ++idx) {
+          r.score[c.first + i] = st.h_out[idx];
+          r.arange[c.first + i] = st.h_out[npairs + idx];
+          r.brange[c.first + i] = st.h_out[2 * npairs + idx];
+        }
+        r.outstanding -= c.count;
+        if (r.outstanding == 0 && r.next >= (int)r.pairs.size()) finish_request(s, c.req);
+      }
+      s->batches++;
+      s->pairs_done += (int64_t)npairs;
+      s->cells_done += cells;
+      s->max_batch_pairs_seen = std::max<int64_t>(s->max_batch_pairs_seen, (int64_t)npairs);
+    }
+    s->cv_done.notify_all();
+  }
+  for (auto* e : st.engines)
+    if (e) ipuma_gpu_destroy(e);
+  cudaFreeHost(st.h_codes);
+  cudaFreeHost(st.h_pairs);
+  cudaFreeHost(st.h_out);
+  cudaStreamDestroy(st.stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+int ipuma_server_create(const ipuma_server_config* cfg, ipuma_server** out) {
+  if (!cfg || !out || cfg->n_scorings < 1 || !cfg->scorings) return fail(IPUMA_ERR_INVALID_ARG, "bad server configuration");
+  std::unique_ptr<ipuma_server> s(new ipuma_server());
+  s->cfg = *cfg;
+  s->scorings.assign(cfg->scorings, cfg->scorings + cfg->n_scorings);
+  s->cfg.scorings = nullptr;
+  if (s->cfg.slots <= 0) s->cfg.slots = 4;
+  if (s->cfg.max_batch_pairs <= 0) s->cfg.max_batch_pairs = 65536;
+  s->device = cfg->device;
+  if (cudaSetDevice(s->device) != cudaSuccess) return fail(IPUMA_ERR_NO_DEVICE, "cannot use device %d", s->device);
+  size_t freeB = 0, totalB = 0;
+  if (cudaMemGetInfo(&freeB, &totalB) != cudaSuccess) return fail(IPUMA_ERR_CUDA, "cudaMemGetInfo failed");
+  size_t pool = cfg->pool_bytes > 0 ? (size_t)cfg->pool_bytes : freeB / 4;
+  if (pool > freeB / 2) pool = freeB / 2;
+  if (pool < (1u << 20)) return fail(IPUMA_ERR_NO_MEMORY, "not enough free device memory for the pool");
+  if (cudaMalloc(&s->d_pool, pool) != cudaSuccess) return fail(IPUMA_ERR_NO_MEMORY, "pool allocation failed");
+  s->pool.reset(new Pool(pool));
+  for (int i = 0; i < s->cfg.slots; ++i) s->workers.emplace_back(worker_loop, s.get(), i);
+  *out = s.release();
+  return IPUMA_OK;
+}
+
+int ipuma_server_submit(ipuma_server* s, int32_t kind, const uint8_t* codes, size_t n_codes,
+                        const ipuma_pair* pairs, int32_t n, uint64_t* req) {
+  if (!s || !req || n < 0 || (n > 0 && (!pairs || (!codes && n_codes))))
+    return fail(IPUMA_ERR_INVALID_ARG, "bad submission");
+  if (kind < 0 || kind >= (int)s->scorings.size()) return fail(IPUMA_ERR_INVALID_ARG, "unknown scoring kind %d", kind);
+  auto r = std::make_shared<Request>();
+  r->kind = kind;
+  // Copy only the sequences the pairs use, offsets rebased to the copy.
+  size_t need = 0;
+  for (int i = 0; i < n; ++i) {
+    const ipuma_pair& p = pairs[i];
+    if (p.a_len < 0 || p.b_len < 0 || p.a_len > 65535 || p.b_len > 65535 || p.a_off < 0 || p.b_off < 0 ||
+        (size_t)p.a_off + p.a_len > n_codes || (size_t)p.b_off + p.b_len > n_codes)
+      return fail(IPUMA_ERR_INVALID_ARG, "pair %d lies outside the code array", i);
+    if (batch_bytes((size_t)p.a_len + p.b_len, 1) > s->pool->size() / 2)
+      return fail(IPUMA_ERR_NO_MEMORY, "pair %d does not fit the device pool", i);
+    need += (size_t)p.a_len + p.b_len;
+    r->cells += (int64_t)p.a_len * p.b_len;
+  }
+  r->codes.resize(need);
+  r->pairs.resize(n);
+  size_t pos = 0;
+  for (int i = 0; i < n; ++i) {
+    const ipuma_pair& p = pairs[i];
+    std::memcpy(r->codes.data() + pos, codes + p.a_off, p.a_len);
+    std::memcpy(r->codes.data() + pos + p.a_len, codes + p.b_off, p.b_len);
+    r->pairs[i] = ipuma_pair{(int64_t)pos, (int64_t)(pos + p.a_len), p.a_len, p.b_len};
+    pos += (size_t)p.a_len + p.b_len;
+  }
+  r->score.assign(n, 0);
+  r->arange.assign(n, 0);
+  r->brange.assign(n, 0);
+  r->t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->closing) return fail(IPUMA_ERR_CLOSED, "server is closed");
+    r->id = s->next_id++;
+    s->submitted++;
+    s->live[r->id] = r;
+    if (n == 0) {
+      finish_request(s, r);
+    } else {
+      s->queue.push_back(r);
+    }
+    *req = r->id;
+  }
+  s->cv_work.notify_one();
+  if (n == 0) s->cv_done.notify_all();
+  return IPUMA_OK;
+}
+
+int ipuma_server_poll(ipuma_server* s, uint64_t req, int32_t* done) {
+  if (!s || !done) return fail(IPUMA_ERR_INVALID_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->live.find(req);
+  if (it == s->live.end()) return fail(IPUMA_ERR_UNKNOWN_JOB, "unknown request %llu", (unsigned long long)req);
+  *done = it->second->done ? 1 : 0;
+  return IPUMA_OK;
+}
+
+int ipuma_server_wait(ipuma_server* s, uint64_t req, int64_t timeout_ms, int32_t* score, int32_t* arange,
+                      int32_t* brange, double* latency_ms) {
+  if (!s) return fail(IPUMA_ERR_INVALID_ARG, "null server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->live.find(req);
+  if (it == s->live.end()) return fail(IPUMA_ERR_UNKNOWN_JOB, "unknown request %llu", (unsigned long long)req);
+  std::shared_ptr<Request> r = it->second;
+  auto pred = [&] { return r->done; };
+  if (timeout_ms < 0) {
+    s->cv_done.wait(lk, pred);
+  } else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), pred)) {
+    return fail(IPUMA_ERR_TIMEOUT, "request %llu not finished after %lld ms", (unsigned long long)req,
+                (long long)timeout_ms);
+  }
+  s->live.erase(r->id);
+  if (r->error != IPUMA_OK) return fail(r->error, "request failed: %s", r->message.c_str());
+  const size_t n = r->score.size();
+  if (n) {
+    if (score) std::memcpy(score, r->score.data(), n * sizeof(int32_t));
+    if (arange) std::memcpy(arange, r->arange.data(), n * sizeof(int32_t));
+    if (brange) std::memcpy(brange, r->brange.data(), n * sizeof(int32_t));
+  }
+  if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+  return IPUMA_OK;
+}
+
+int ipuma_server_get_stats(ipuma_server* s, ipuma_server_stats* out) {
+  if (!s || !out) return fail(IPUMA_ERR_INVALID_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  out->submitted = s->submitted;
+  out->completed = s->completed;
+  out->queued = (int64_t)s->queue.size();
+  out->batches = s->batches;
+  out->pairs = s->pairs_done;
+  out->cells = s->cells_done;
+  out->max_batch_pairs = s->max_batch_pairs_seen;
+  out->pool_bytes = (int64_t)s->pool->size();
+  out->pool_used = (int64_t)s->pool->used();
+  out->max_pool_used = s->max_pool_used;
+  out->busy_ms = s->busy_ms;
+  return IPUMA_OK;
+}
+
+int ipuma_server_close(ipuma_server* s) {
+  if (!s) return fail(IPUMA_ERR_INVALID_ARG, "null server");
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->closing = true;
+  }
+  s->cv_work.notify_all();
+  return IPUMA_OK;
+}
+
+void ipuma_server_destroy(ipuma_server* s) {
+  if (!s) return;
+  ipuma_server_close(s);
+  for (auto& t : s->workers) t.join();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (auto& kv : s->live)
+      if (!kv.second->done) {
+        kv.second->error = IPUMA_ERR_CLOSED;
+        kv.second->message = "server closed";
+        kv.second->done = true;
+      }
+  }
+  s->cv_done.notify_all();
+  cudaSetDevice(s->device);
+  if (s->d_pool) cudaFree(s->d_pool);
+  delete s;
+}
+
+}  // extern "C"

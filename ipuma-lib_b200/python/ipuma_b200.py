@@ -38,7 +38,9 @@ EXPORTS = [
     "ipuma_gpu_set_option", "ipuma_gpu_run_buffer", "ipuma_gpu_submit_buffer", "ipuma_gpu_poll",
     "ipuma_gpu_join", "ipuma_gpu_compare", "ipuma_gpu_compare_device", "ipuma_gpu_last_stats",
     "ipuma_gpu_run_buffer_device", "ipuma_measure_int_peak", "ipuma_gpu_compare_noalloc",
-    "ipuma_gpu_autotune", "ipuma_gpu_tuning",
+    "ipuma_gpu_autotune", "ipuma_gpu_tuning", "ipuma_server_create", "ipuma_server_submit",
+    "ipuma_server_poll", "ipuma_server_wait", "ipuma_server_get_stats", "ipuma_server_close",
+    "ipuma_server_destroy",
 ]
 
 KERNEL_NAMES = {0: "k_batched<s32,L32,K16>", 1: "k_batched<s16x2,L16,K4>",
@@ -81,6 +83,20 @@ class Stats(ctypes.Structure):
                 ("timed_ms", ctypes.c_double * 10), ("timed_cells", ctypes.c_int64 * 10)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("n_scorings", ctypes.c_int32), ("scorings", ctypes.POINTER(SwConfig)),
+                ("forward_only", ctypes.c_int32), ("slots", ctypes.c_int32),
+                ("pool_bytes", ctypes.c_int64), ("max_batch_pairs", ctypes.c_int32),
+                ("device", ctypes.c_int32), ("one_request_per_batch", ctypes.c_int32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int64) for k in ("submitted", "completed", "queued", "batches",
+                                               "pairs", "cells", "max_batch_pairs",
+                                               "pool_bytes", "pool_used", "max_pool_used")] + \
+               [("busy_ms", ctypes.c_double)]
+
+
 _lib = None
 
 
@@ -113,6 +129,15 @@ def lib():
         L.ipuma_gpu_run_buffer_device.argtypes = [vp, vp, sz, vp, sz, vp]
         L.ipuma_measure_int_peak.argtypes = [i32, ctypes.POINTER(ctypes.c_double)]
         L.ipuma_gpu_autotune.argtypes = [vp, ctypes.c_char_p]
+        L.ipuma_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
+        L.ipuma_server_submit.argtypes = [vp, i32, vp, sz, vp, i32, ctypes.POINTER(ctypes.c_uint64)]
+        L.ipuma_server_poll.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(i32)]
+        L.ipuma_server_wait.argtypes = [vp, ctypes.c_uint64, i64, vp, vp, vp,
+                                        ctypes.POINTER(ctypes.c_double)]
+        L.ipuma_server_get_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
+        L.ipuma_server_close.argtypes = [vp]
+        L.ipuma_server_destroy.argtypes = [vp]
+        L.ipuma_server_destroy.restype = None
         L.ipuma_gpu_tuning.argtypes = [vp, ctypes.c_char_p, sz]
         L.ipuma_gpu_compare_noalloc.argtypes = [ctypes.POINTER(SwConfig), i32, vp, sz, vp, i32, i32,
                                                 vp, vp, vp, vp]
@@ -290,6 +315,60 @@ def compare_noalloc(sw: SwConfig, forward_only: bool, d_codes: int, n_codes: int
                                            ctypes.c_void_p(d_pairs), n, max_b,
                                            ctypes.c_void_p(d_score), ctypes.c_void_p(d_ar),
                                            ctypes.c_void_p(d_br), ctypes.c_void_p(stream))
+
+
+class Server:
+    """Serving loop (ipuma_server_*): continuous batching of requests."""
+
+    def __init__(self, scorings, forward_only=True, slots=4, pool_bytes=0, max_batch_pairs=0,
+                 device=0, one_request_per_batch=False):
+        self._scorings = (SwConfig * len(scorings))(*scorings)
+        cfg = ServerConfig(len(scorings), self._scorings, int(bool(forward_only)), slots,
+                           pool_bytes, max_batch_pairs, device, int(bool(one_request_per_batch)))
+        h = ctypes.c_void_p()
+        _check(lib().ipuma_server_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+
+    def submit(self, kind: int, codes: np.ndarray, pairs: np.ndarray) -> int:
+        codes = np.ascontiguousarray(codes, dtype=np.uint8)
+        pairs = np.ascontiguousarray(pairs, dtype=PAIR_DTYPE)
+        rid = ctypes.c_uint64()
+        _check(lib().ipuma_server_submit(self.h, kind, _ptr(codes), codes.size, _ptr(pairs),
+                                         pairs.shape[0], ctypes.byref(rid)))
+        return rid.value
+
+    def poll(self, rid: int) -> bool:
+        d = ctypes.c_int32()
+        _check(lib().ipuma_server_poll(self.h, rid, ctypes.byref(d)))
+        return bool(d.value)
+
+    def wait(self, rid: int, n: int, timeout_ms: int = -1):
+        score = np.zeros(n, np.int32)
+        ar = np.zeros(n, np.int32)
+        br = np.zeros(n, np.int32)
+        lat = ctypes.c_double()
+        _check(lib().ipuma_server_wait(self.h, rid, timeout_ms, _ptr(score), _ptr(ar), _ptr(br),
+                                       ctypes.byref(lat)))
+        return score, ar, br, lat.value
+
+    def stats(self) -> ServerStats:
+        st = ServerStats()
+        _check(lib().ipuma_server_get_stats(self.h, ctypes.byref(st)))
+        return st
+
+    def close(self):
+        _check(lib().ipuma_server_close(self.h))
+
+    def destroy(self):
+        if self.h:
+            lib().ipuma_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.destroy()
 
 
 def make_pairs(a_off, a_len, b_off, b_len) -> np.ndarray:
