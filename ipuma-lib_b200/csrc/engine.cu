@@ -170,6 +170,22 @@ constexpr int CTL_INTS = CTL_OFFS + NCLASS_MAX * NBUCKET;
 constexpr int CELLS_RERUN = NCLASS_MAX;             // index of the rerun cells
 constexpr int CELLS_WIRE = NCLASS_MAX + 1;          // cells found by the wire check
 
+// A kernel's dynamic shared memory limit is one process-wide attribute per
+// device, shared by every engine: engines with different alphabets need
+// different sizes and may run concurrently on several threads, so the limit
+// only ever grows (lowering it would break another engine's launches).
+template <class K>
+void raise_smem_limit(int device, K kernel, int smem) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, int> limit;
+  if (smem <= 48 * 1024) return;
+  std::lock_guard<std::mutex> lock(mu);
+  int& cur = limit[{device, reinterpret_cast<const void*>(kernel)}];
+  if (smem > cur && cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) ==
+                        cudaSuccess)
+    cur = smem;
+}
+
 // Persistent grid of a kernel: resident blocks per SM times SMs.  Computed
 // once per kernel and engine (engine creation warms the cache, so no
 // occupancy query or attribute change happens during a graph capture).
@@ -179,7 +195,7 @@ int occupancy_grid(ipuma_engine* e, K kernel, int smem) {
   auto it = e->grid_cache.find(key);
   if (it != e->grid_cache.end() && it->second.first == smem) return it->second.second;
   int nb = 0;
-  if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  raise_smem_limit(e->device, kernel, smem);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, kThreads, smem);
   if (nb < 1) nb = 1;
   e->grid_cache[key] = {smem, nb * e->nsm};
