@@ -49,6 +49,10 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-serving", action="store_true",
+                    help="skip the serving-loop sweep (run at N=1 only)")
+    ap.add_argument("--serving-seconds", type=float, default=2.0,
+                    help="arrival window of each offered-load point")
     return ap.parse_args()
 
 
@@ -208,6 +212,89 @@ def cpu_baseline(wl, seconds, sw):
                 m, wl.n, sub.cells, dt,
                 "reference SWAffine codelet compiled for the host, OpenMP over pair chunks"
                 if use_ref else "oracle restatement (C), OpenMP over pairs")}
+
+
+def device_gcups(ib, torch, wl, dev, stream, local, reps=3):
+    """Batched-engine GCUPS of one workload on device-resident inputs."""
+    sw = ib.sw_config(wl.gap_init, wl.gap_extend, wl.match, wl.mismatch, wl.ambiguity,
+                      wl.similarity, wl.datatype)
+    eng = ib.Engine(sw, ib.algo_config(forward_only=True), device=local)
+    eng.autotune(os.environ.get("IPUMA_TUNE_CACHE"))
+    pairs = ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len)
+    d_codes = torch.from_numpy(wl.codes).to(dev)
+    d_pairs = torch.from_numpy(pairs.view(np.uint8)).to(dev)
+    d_out = torch.zeros(3, wl.n, dtype=torch.int32, device=dev)
+    max_a, max_b = int(wl.a_len.max()), int(wl.b_len.max())
+
+    def go():
+        eng.compare_device(d_codes.data_ptr(), d_codes.numel(), d_pairs.data_ptr(), wl.n, max_a,
+                           max_b, d_out[0].data_ptr(), d_out[1].data_ptr(), d_out[2].data_ptr(),
+                           stream.cuda_stream)
+    go()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        go()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    eng.close()
+    return wl.cells / (ms * 1e-3) / 1e9
+
+
+def serving_section(args, ib, torch, dev, stream, local):
+    """Open-loop Poisson sweep of the serving loop: 50% DNA (1M-pair DNA
+    distribution) / 50% protein (200k-pair protein distribution) requests of
+    1-4096 pairs (log-uniform) at 10-100% of the batched engine's measured
+    peak for that mix, plus 64-pair requests; against one request per
+    device batch (no coalescing)."""
+    import serving
+    import workloads
+    wls = [workloads.dna_batched(n=400_000, seed=2001), workloads.protein(n=100_000, seed=2002)]
+    g = [device_gcups(ib, torch, wl, dev, stream, local) for wl in wls]
+    peak = serving.mix_peak(g, wls)
+    peak64 = peak  # same mix, same engine
+    scorings = [ib.sw_config(wl.gap_init, wl.gap_extend, wl.match, wl.mismatch, wl.ambiguity,
+                             wl.similarity, wl.datatype) for wl in wls]
+
+    def server(one=False):
+        return ib.Server(scorings, slots=4, pool_bytes=4 << 30, device=local,
+                         one_request_per_batch=one)
+
+    dur = args.serving_seconds
+    loads = [0.1, 0.25, 0.5, 0.8, 1.0]
+    keys = ("offered_load", "gcups", "fraction_of_peak", "p50_ms", "p95_ms", "p99_ms", "requests",
+            "failed", "mean_pairs_per_batch")
+
+    def slim(rs):
+        return [{k: r[k] for k in keys} for r in rs]
+
+    t0 = time.perf_counter()
+    res = {
+        "workload": "poisson requests, 50% dna_batched / 50% protein distributions, "
+                    "400k + 100k pair pools, %.1f s arrival window per point" % dur,
+        "device_gcups": {"dna": g[0], "protein": g[1], "mix_peak": peak},
+        "slots": 4,
+        "sizes_1_4096_resident": slim(serving.sweep(server, wls, peak, loads, dur, 1, 4096,
+                                                    resident=True, seed=10)),
+        "sizes_1_4096_staged": slim(serving.sweep(server, wls, peak, loads, dur, 1, 4096,
+                                                  resident=False, seed=20)),
+        "pairs_64_resident": slim(serving.sweep(server, wls, peak64, [0.5, 0.8, 1.0], dur, 64, 64,
+                                                resident=True, seed=30)),
+        "pairs_64_staged": slim(serving.sweep(server, wls, peak64, [0.8], dur, 64, 64,
+                                              resident=False, seed=40)),
+        "per_request_baseline": {
+            "what": "one request per device batch (no coalescing), resident sets, 4 slots",
+            "sizes_1_4096": slim(serving.sweep(lambda: server(True), wls, peak, [0.1, 0.25, 0.5],
+                                               dur, 1, 4096, resident=True, seed=50,
+                                               max_requests=3000)),
+            "pairs_64": slim(serving.sweep(lambda: server(True), wls, peak64, [0.1, 0.8], dur,
+                                           64, 64, resident=True, seed=60, max_requests=6000)),
+        },
+    }
+    res["seconds"] = time.perf_counter() - t0
+    return res
 
 
 def run_reference(args):
@@ -441,6 +528,10 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(wl, args.cpu_seconds, sw)
 
+    srv = None
+    if ws == 1 and not args.no_serving:
+        srv = serving_section(args, ib, torch, dev, stream, local)
+
     if rank == 0:
         line = {
             "metric": "bit-exact GCUPS (forward pass, score + end coordinates)",
@@ -464,6 +555,7 @@ def main():
                        "against": "oracle (C restatement of SWAffine::compute)"},
             "launch_breakdown_ms": [{"kernel": n, "ms": m, "cells": c} for n, m, c in timed],
             "autotune": tuning,
+            "serving": srv,
         }
         line.update(result)
         print(json.dumps(line))

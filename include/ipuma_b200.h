@@ -283,6 +283,15 @@ int ipuma_server_create(const ipuma_server_config* cfg, ipuma_server** out);
  * when one of its pairs cannot fit the device pool. */
 int ipuma_server_submit(ipuma_server* s, int32_t kind, const uint8_t* codes, size_t n_codes,
                         const ipuma_pair* pairs, int32_t n, uint64_t* req);
+/* Uploads a code array once into device memory that the server keeps
+ * until it is destroyed (outside the batch pool; IPUMA_ERR_NO_MEMORY when
+ * the device has no room) and returns its set id. */
+int ipuma_server_add_sequences(ipuma_server* s, const uint8_t* codes, size_t n_codes, int32_t* set_id);
+/* Queues a request whose pairs index a resident set (offsets into the
+ * codes given to ipuma_server_add_sequences): only the pair descriptors
+ * are copied and staged. */
+int ipuma_server_submit_resident(ipuma_server* s, int32_t kind, int32_t set_id, const ipuma_pair* pairs,
+                                 int32_t n, uint64_t* req);
 int ipuma_server_poll(ipuma_server* s, uint64_t req, int32_t* done);
 /* Waits for a request (timeout_ms < 0: no limit) and copies its results
  * (in pair order) and its latency from submission to completion.  A

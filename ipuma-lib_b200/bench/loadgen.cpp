@@ -5,7 +5,9 @@
 // first pair and pair count within that kind's pair array).  `submitters`
 // threads submit request i at its arrival time (Poisson stream from the
 // caller), `waiters` threads wait for the requests and record each one's
-// latency as the server measured it (submission to completion).
+// latency as the server measured it (submission to completion).  With
+// `set_ids` the requests go to ipuma_server_submit_resident (kind k's pairs
+// index resident set set_ids[k]); without, each request carries its codes.
 #include <atomic>
 #include <chrono>
 #include <cstdint>
@@ -17,7 +19,8 @@
 extern "C" int ipuma_loadgen_run(ipuma_server* srv, int32_t n_kinds, const uint8_t* const* codes,
                                  const int64_t* n_codes, const ipuma_pair* const* pairs, int64_t n_req,
                                  const double* arrival_s, const int32_t* kind, const int64_t* first,
-                                 const int32_t* count, int32_t submitters, int32_t waiters, double* latency_ms,
+                                 const int32_t* count, const int32_t* set_ids, int32_t submitters,
+                                 int32_t waiters, double* latency_ms,
                                  int32_t* status, double* wall_s) {
   using Clock = std::chrono::steady_clock;
   if (!srv || n_req < 0 || submitters < 1 || waiters < 1) return IPUMA_ERR_INVALID_ARG;
@@ -34,7 +37,9 @@ extern "C" int ipuma_loadgen_run(ipuma_server* srv, int32_t n_kinds, const uint8
         std::this_thread::sleep_until(when);
         const int k = kind[i];
         uint64_t id = 0;
-        const int rc = ipuma_server_submit(srv, k, codes[k], (size_t)n_codes[k], pairs[k] + first[i], count[i], &id);
+        const int rc =
+            set_ids ? ipuma_server_submit_resident(srv, k, set_ids[k], pairs[k] + first[i], count[i], &id)
+                    : ipuma_server_submit(srv, k, codes[k], (size_t)n_codes[k], pairs[k] + first[i], count[i], &id);
         sub_status[i] = rc;
         ids[i].store(rc == IPUMA_OK ? id : ~uint64_t(0));
       }

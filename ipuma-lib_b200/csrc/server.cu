@@ -3,7 +3,7 @@
 // Requests (host code arrays + pairs, one scoring configuration each) are
 // queued by ipuma_server_submit and returned through ipuma_server_wait.
 // `slots` worker threads, each with its own engine and CUDA stream, take
-// whatever is queued -- the head request's scoring, as many of its pairs
+// whatever is queued -- the oldest request's scoring, as many of its pairs
 // and of the following requests' as fit a device batch -- stage it through
 // pinned memory into a region of the server's device pool, run the
 // cost-binned engine on it and scatter the results back per request.  A
@@ -16,6 +16,15 @@
 // a first-fit allocator; a slot that cannot get the bytes for its batch
 // waits until running batches return theirs.  A request that cannot fit
 // even an empty pool is refused at submission.
+//
+// Resident sequence sets: a caller that aligns against the same sequences
+// again and again uploads them once (ipuma_server_add_sequences); requests
+// then carry only pair descriptors into that set and batches stage nothing
+// but pairs.  A batch holds requests of one scoring and one set.
+//
+// Engines for every slot and scoring are created (and autotuned, one
+// scoring after the other) when the server starts, so no request waits
+// for an engine and no tuning runs beside live batches.
 //
 // Failure handling is on the host: a closed server refuses submissions,
 // waits have timeouts, and a failing batch marks its requests failed
@@ -46,6 +55,7 @@ using Clock = std::chrono::steady_clock;
 struct Request {
   uint64_t id = 0;
   int kind = 0;
+  int set = -1;          // resident sequence set, -1: codes travel with the request
   std::vector<uint8_t> codes;
   std::vector<ipuma_pair> pairs;
   std::vector<int32_t> score, arange, brange;
@@ -114,16 +124,25 @@ size_t batch_bytes(size_t codes, size_t pairs) {
 
 }  // namespace
 
+struct ResidentSet {
+  uint8_t* d_codes = nullptr;
+  size_t n_codes = 0;
+};
+
 struct ipuma_server {
   ipuma_server_config cfg{};
   std::vector<ipuma_sw_config> scorings;
   int device = 0;
   uint8_t* d_pool = nullptr;
   std::unique_ptr<Pool> pool;
+  std::vector<ResidentSet> sets;   // append-only; freed at destroy
+  std::vector<std::vector<ipuma_engine*>> engines;  // [slot][scoring]
   std::mutex mu;
   std::condition_variable cv_work;  // work queued / pool freed / closing
   std::condition_variable cv_done;  // a request finished
-  std::deque<std::shared_ptr<Request>> queue;  // requests with pairs not yet batched
+  // Requests with pairs not yet batched, one FIFO per (scoring, set).
+  std::map<std::pair<int, int>, std::deque<std::shared_ptr<Request>>> queues;
+  int64_t n_queued = 0;
   std::map<uint64_t, std::shared_ptr<Request>> live;
   uint64_t next_id = 1;
   bool closing = false;
@@ -137,7 +156,7 @@ struct ipuma_server {
 namespace {
 
 struct SlotState {
-  std::vector<ipuma_engine*> engines;  // one per scoring, created lazily
+  std::vector<ipuma_engine*> engines;  // one per scoring, owned by the server
   cudaStream_t stream = nullptr;
   uint8_t* h_codes = nullptr;
   ipuma_pair* h_pairs = nullptr;
@@ -164,7 +183,7 @@ void fail_chunks(ipuma_server* s, std::vector<Chunk>& chunks, int code, const st
 
 void worker_loop(ipuma_server* s, int slot_index) {
   SlotState st;
-  st.engines.assign(s->scorings.size(), nullptr);
+  st.engines = s->engines[slot_index];
   cudaSetDevice(s->device);
   cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking);
   st.cap_pairs = (size_t)s->cfg.max_batch_pairs;
@@ -172,32 +191,37 @@ void worker_loop(ipuma_server* s, int slot_index) {
   cudaHostAlloc((void**)&st.h_codes, st.cap_codes, cudaHostAllocDefault);
   cudaHostAlloc((void**)&st.h_pairs, st.cap_pairs * sizeof(ipuma_pair), cudaHostAllocDefault);
   cudaHostAlloc((void**)&st.h_out, st.cap_pairs * 3 * sizeof(int32_t), cudaHostAllocDefault);
-  (void)slot_index;
 
   while (true) {
     std::vector<Chunk> chunks;
     size_t codes_bytes = 0, npairs = 0, pool_off = 0, pool_len = 0;
-    int kind = 0;
+    int kind = 0, set = -1;
+    ResidentSet rs;
     int maxA = 1, maxB = 1;
     int64_t cells = 0;
     {
       std::unique_lock<std::mutex> lk(s->mu);
-      s->cv_work.wait(lk, [&] { return s->closing || !s->queue.empty(); });
-      if (s->queue.empty()) break;  // closing and drained
-      // Continuous batching: the head request's scoring, then every queued
-      // request of that scoring that still fits this batch.
-      kind = s->queue.front()->kind;
-      for (auto it = s->queue.begin(); it != s->queue.end() && npairs < st.cap_pairs;) {
-        auto& r = *it;
-        if (r->kind != kind) {
-          ++it;
-          continue;
-        }
+      s->cv_work.wait(lk, [&] { return s->closing || s->n_queued > 0; });
+      if (s->n_queued == 0) break;  // closing and drained
+      // Continuous batching: the queue (scoring, sequence set) whose head
+      // request is the oldest, then every request of that queue that still
+      // fits this batch.
+      auto qi = s->queues.end();
+      for (auto it = s->queues.begin(); it != s->queues.end(); ++it)
+        if (!it->second.empty() &&
+            (qi == s->queues.end() || it->second.front()->t_submit < qi->second.front()->t_submit))
+          qi = it;
+      kind = qi->first.first;
+      set = qi->first.second;
+      if (set >= 0) rs = s->sets[set];
+      auto& q = qi->second;
+      while (!q.empty() && npairs < st.cap_pairs) {
+        std::shared_ptr<Request> r = q.front();
         int take = 0;
         size_t bytes = 0;
         while (r->next + take < (int)r->pairs.size() && npairs + take < st.cap_pairs) {
           const ipuma_pair& p = r->pairs[r->next + take];
-          const size_t add = (size_t)p.a_len + (size_t)p.b_len;
+          const size_t add = set >= 0 ? 0 : (size_t)p.a_len + (size_t)p.b_len;
           if (npairs + take > 0 && batch_bytes(codes_bytes + bytes + add, npairs + take + 1) > s->pool->size() / 2)
             break;
           bytes += add;
@@ -209,10 +233,9 @@ void worker_loop(ipuma_server* s, int slot_index) {
         r->outstanding += take;
         npairs += take;
         codes_bytes += bytes;
-        if (r->next >= (int)r->pairs.size())
-          it = s->queue.erase(it);
-        else
-          break;  // batch full
+        if (r->next < (int)r->pairs.size()) break;  // batch full
+        q.pop_front();
+        s->n_queued--;
         if (s->cfg.one_request_per_batch) break;
       }
       // Admission by free device memory: wait for the pool.
@@ -222,7 +245,8 @@ void worker_loop(ipuma_server* s, int slot_index) {
       while (!s->pool->alloc(pool_len, &pool_off)) s->cv_work.wait_for(lk, std::chrono::milliseconds(5));
       s->max_pool_used = std::max<int64_t>(s->max_pool_used, (int64_t)s->pool->used());
     }
-    // Stage the batch in pinned memory (pair offsets rebased).
+    // Stage the batch in pinned memory (pair offsets rebased; pairs into a
+    // resident set keep theirs and stage no codes).
     if (codes_bytes > st.cap_codes) {
       cudaFreeHost(st.h_codes);
       st.cap_codes = codes_bytes * 2;
@@ -231,6 +255,17 @@ void worker_loop(ipuma_server* s, int slot_index) {
     size_t pos = 0, k = 0;
     for (auto& c : chunks) {
       const Request& r = *c.req;
+      if (set >= 0) {
+        std::memcpy(st.h_pairs + k, r.pairs.data() + c.first, sizeof(ipuma_pair) * c.count);
+        for (int i = 0; i < c.count; ++i) {
+          const ipuma_pair& p = st.h_pairs[k + i];
+          maxA = std::max(maxA, p.a_len);
+          maxB = std::max(maxB, p.b_len);
+          cells += (int64_t)p.a_len * p.b_len;
+        }
+        k += c.count;
+        continue;
+      }
       for (int i = 0; i < c.count; ++i, ++k) {
         const ipuma_pair& p = r.pairs[c.first + i];
         ipuma_pair q{(int64_t)pos, (int64_t)(pos + p.a_len), p.a_len, p.b_len};
@@ -243,7 +278,8 @@ void worker_loop(ipuma_server* s, int slot_index) {
         cells += (int64_t)p.a_len * p.b_len;
       }
     }
-    uint8_t* d_codes = s->d_pool + pool_off;
+    uint8_t* d_codes = set >= 0 ? rs.d_codes : s->d_pool + pool_off;
+    const size_t n_codes_batch = set >= 0 ? rs.n_codes : codes_bytes;
     size_t o = (std::max<size_t>(codes_bytes, 1) + 255) & ~size_t(255);
     ipuma_pair* d_pairs = reinterpret_cast<ipuma_pair*>(s->d_pool + pool_off + o);
     o += (npairs * sizeof(ipuma_pair) + 255) & ~size_t(255);
@@ -251,13 +287,9 @@ void worker_loop(ipuma_server* s, int slot_index) {
     const auto t0 = Clock::now();
     int rc = IPUMA_OK;
     std::string msg;
-    if (!st.engines[kind]) {
-      ipuma_algo_config algo{1, 300, 20, 3000, 0, 0, s->cfg.forward_only, 0, 1, 0};
-      rc = ipuma_gpu_create(&s->scorings[kind], &algo, s->device, &st.engines[kind]);
-      if (rc) msg = ipuma_last_error();
-    }
     if (rc == IPUMA_OK && npairs > 0) {
-      if (cudaMemcpyAsync(d_codes, st.h_codes, codes_bytes, cudaMemcpyHostToDevice, st.stream) != cudaSuccess ||
+      if ((set < 0 && cudaMemcpyAsync(d_codes, st.h_codes, codes_bytes, cudaMemcpyHostToDevice, st.stream) !=
+                          cudaSuccess) ||
           cudaMemcpyAsync(d_pairs, st.h_pairs, npairs * sizeof(ipuma_pair), cudaMemcpyHostToDevice, st.stream) !=
               cudaSuccess) {
         rc = IPUMA_ERR_CUDA;
@@ -265,7 +297,7 @@ void worker_loop(ipuma_server* s, int slot_index) {
       }
     }
     if (rc == IPUMA_OK && npairs > 0) {
-      rc = ipuma_gpu_compare_device(st.engines[kind], d_codes, codes_bytes, d_pairs, (int32_t)npairs, maxA, maxB,
+      rc = ipuma_gpu_compare_device(st.engines[kind], d_codes, n_codes_batch, d_pairs, (int32_t)npairs, maxA, maxB,
                                     d_out, d_out + npairs, d_out + 2 * npairs, st.stream);
       if (rc) msg = ipuma_last_error();
     }
@@ -309,12 +341,36 @@ void worker_loop(ipuma_server* s, int slot_index) {
     }
     s->cv_done.notify_all();
   }
-  for (auto* e : st.engines)
-    if (e) ipuma_gpu_destroy(e);
   cudaFreeHost(st.h_codes);
   cudaFreeHost(st.h_pairs);
   cudaFreeHost(st.h_out);
   cudaStreamDestroy(st.stream);
+}
+
+// Queues a prepared request (results sized here) and hands out its id.
+int enqueue(ipuma_server* s, const std::shared_ptr<Request>& r, uint64_t* req) {
+  const size_t n = r->pairs.size();
+  r->score.assign(n, 0);
+  r->arange.assign(n, 0);
+  r->brange.assign(n, 0);
+  r->t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->closing) return fail(IPUMA_ERR_CLOSED, "server is closed");
+    r->id = s->next_id++;
+    s->submitted++;
+    s->live[r->id] = r;
+    if (n == 0) {
+      finish_request(s, r);
+    } else {
+      s->queues[{r->kind, r->set}].push_back(r);
+      s->n_queued++;
+    }
+    *req = r->id;
+  }
+  s->cv_work.notify_one();
+  if (n == 0) s->cv_done.notify_all();
+  return IPUMA_OK;
 }
 
 }  // namespace
@@ -338,8 +394,48 @@ int ipuma_server_create(const ipuma_server_config* cfg, ipuma_server** out) {
   if (pool < (1u << 20)) return fail(IPUMA_ERR_NO_MEMORY, "not enough free device memory for the pool");
   if (cudaMalloc(&s->d_pool, pool) != cudaSuccess) return fail(IPUMA_ERR_NO_MEMORY, "pool allocation failed");
   s->pool.reset(new Pool(pool));
+  // Engines for every slot and scoring, tuned here, one after the other.
+  ipuma_algo_config algo{1, 300, 20, 3000, 0, 0, s->cfg.forward_only, 0, 1, 0};
+  s->engines.assign(s->cfg.slots, std::vector<ipuma_engine*>(s->scorings.size(), nullptr));
+  int rc = IPUMA_OK;
+  for (int i = 0; i < s->cfg.slots && rc == IPUMA_OK; ++i)
+    for (size_t k = 0; k < s->scorings.size() && rc == IPUMA_OK; ++k) {
+      rc = ipuma_gpu_create(&s->scorings[k], &algo, s->device, &s->engines[i][k]);
+      if (rc == IPUMA_OK) rc = ipuma_gpu_autotune(s->engines[i][k], nullptr);
+    }
+  if (rc != IPUMA_OK) {
+    const std::string msg = ipuma_last_error();
+    for (auto& row : s->engines)
+      for (auto* e : row)
+        if (e) ipuma_gpu_destroy(e);
+    cudaFree(s->d_pool);
+    return fail(rc, "%s", msg.c_str());
+  }
   for (int i = 0; i < s->cfg.slots; ++i) s->workers.emplace_back(worker_loop, s.get(), i);
   *out = s.release();
+  return IPUMA_OK;
+}
+
+int ipuma_server_add_sequences(ipuma_server* s, const uint8_t* codes, size_t n_codes, int32_t* set_id) {
+  if (!s || !set_id || (!codes && n_codes)) return fail(IPUMA_ERR_INVALID_ARG, "bad sequence set");
+  if (cudaSetDevice(s->device) != cudaSuccess) return fail(IPUMA_ERR_NO_DEVICE, "cannot use device %d", s->device);
+  ResidentSet rs;
+  rs.n_codes = n_codes;
+  if (cudaMalloc(&rs.d_codes, std::max<size_t>(n_codes, 1)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(IPUMA_ERR_NO_MEMORY, "no device memory for a set of %zu bytes", n_codes);
+  }
+  if (n_codes && cudaMemcpy(rs.d_codes, codes, n_codes, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(rs.d_codes);
+    return fail(IPUMA_ERR_CUDA, "copying the sequence set failed");
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->closing) {
+    cudaFree(rs.d_codes);
+    return fail(IPUMA_ERR_CLOSED, "server is closed");
+  }
+  *set_id = (int32_t)s->sets.size();
+  s->sets.push_back(rs);
   return IPUMA_OK;
 }
 
@@ -372,26 +468,31 @@ int ipuma_server_submit(ipuma_server* s, int32_t kind, const uint8_t* codes, siz
     r->pairs[i] = ipuma_pair{(int64_t)pos, (int64_t)(pos + p.a_len), p.a_len, p.b_len};
     pos += (size_t)p.a_len + p.b_len;
   }
-  r->score.assign(n, 0);
-  r->arange.assign(n, 0);
-  r->brange.assign(n, 0);
-  r->t_submit = Clock::now();
+  return enqueue(s, r, req);
+}
+
+int ipuma_server_submit_resident(ipuma_server* s, int32_t kind, int32_t set_id, const ipuma_pair* pairs,
+                                 int32_t n, uint64_t* req) {
+  if (!s || !req || n < 0 || (n > 0 && !pairs)) return fail(IPUMA_ERR_INVALID_ARG, "bad submission");
+  if (kind < 0 || kind >= (int)s->scorings.size()) return fail(IPUMA_ERR_INVALID_ARG, "unknown scoring kind %d", kind);
+  size_t n_codes;
   {
     std::lock_guard<std::mutex> lk(s->mu);
-    if (s->closing) return fail(IPUMA_ERR_CLOSED, "server is closed");
-    r->id = s->next_id++;
-    s->submitted++;
-    s->live[r->id] = r;
-    if (n == 0) {
-      finish_request(s, r);
-    } else {
-      s->queue.push_back(r);
-    }
-    *req = r->id;
+    if (set_id < 0 || set_id >= (int)s->sets.size()) return fail(IPUMA_ERR_INVALID_ARG, "unknown sequence set %d", set_id);
+    n_codes = s->sets[set_id].n_codes;
   }
-  s->cv_work.notify_one();
-  if (n == 0) s->cv_done.notify_all();
-  return IPUMA_OK;
+  auto r = std::make_shared<Request>();
+  r->kind = kind;
+  r->set = set_id;
+  for (int i = 0; i < n; ++i) {
+    const ipuma_pair& p = pairs[i];
+    if (p.a_len < 0 || p.b_len < 0 || p.a_len > 65535 || p.b_len > 65535 || p.a_off < 0 || p.b_off < 0 ||
+        (size_t)p.a_off + p.a_len > n_codes || (size_t)p.b_off + p.b_len > n_codes)
+      return fail(IPUMA_ERR_INVALID_ARG, "pair %d lies outside the sequence set", i);
+    r->cells += (int64_t)p.a_len * p.b_len;
+  }
+  r->pairs.assign(pairs, pairs + n);
+  return enqueue(s, r, req);
 }
 
 int ipuma_server_poll(ipuma_server* s, uint64_t req, int32_t* done) {
@@ -434,7 +535,7 @@ int ipuma_server_get_stats(ipuma_server* s, ipuma_server_stats* out) {
   std::lock_guard<std::mutex> lk(s->mu);
   out->submitted = s->submitted;
   out->completed = s->completed;
-  out->queued = (int64_t)s->queue.size();
+  out->queued = s->n_queued;
   out->batches = s->batches;
   out->pairs = s->pairs_done;
   out->cells = s->cells_done;
@@ -471,6 +572,10 @@ void ipuma_server_destroy(ipuma_server* s) {
   }
   s->cv_done.notify_all();
   cudaSetDevice(s->device);
+  for (auto& row : s->engines)
+    for (auto* e : row)
+      if (e) ipuma_gpu_destroy(e);
+  for (auto& rs : s->sets) cudaFree(rs.d_codes);
   if (s->d_pool) cudaFree(s->d_pool);
   delete s;
 }

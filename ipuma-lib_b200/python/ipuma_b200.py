@@ -40,7 +40,7 @@ EXPORTS = [
     "ipuma_gpu_run_buffer_device", "ipuma_measure_int_peak", "ipuma_gpu_compare_noalloc",
     "ipuma_gpu_autotune", "ipuma_gpu_tuning", "ipuma_server_create", "ipuma_server_submit",
     "ipuma_server_poll", "ipuma_server_wait", "ipuma_server_get_stats", "ipuma_server_close",
-    "ipuma_server_destroy",
+    "ipuma_server_destroy", "ipuma_server_add_sequences", "ipuma_server_submit_resident",
 ]
 
 KERNEL_NAMES = {0: "k_batched<s32,L32,K16>", 1: "k_batched<s16x2,L16,K4>",
@@ -131,6 +131,9 @@ def lib():
         L.ipuma_gpu_autotune.argtypes = [vp, ctypes.c_char_p]
         L.ipuma_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
         L.ipuma_server_submit.argtypes = [vp, i32, vp, sz, vp, i32, ctypes.POINTER(ctypes.c_uint64)]
+        L.ipuma_server_add_sequences.argtypes = [vp, vp, sz, ctypes.POINTER(i32)]
+        L.ipuma_server_submit_resident.argtypes = [vp, i32, i32, vp, i32,
+                                                   ctypes.POINTER(ctypes.c_uint64)]
         L.ipuma_server_poll.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(i32)]
         L.ipuma_server_wait.argtypes = [vp, ctypes.c_uint64, i64, vp, vp, vp,
                                         ctypes.POINTER(ctypes.c_double)]
@@ -335,6 +338,21 @@ class Server:
         rid = ctypes.c_uint64()
         _check(lib().ipuma_server_submit(self.h, kind, _ptr(codes), codes.size, _ptr(pairs),
                                          pairs.shape[0], ctypes.byref(rid)))
+        return rid.value
+
+    def add_sequences(self, codes: np.ndarray) -> int:
+        """Uploads a code array once; returns its resident set id."""
+        codes = np.ascontiguousarray(codes, dtype=np.uint8)
+        sid = ctypes.c_int32()
+        _check(lib().ipuma_server_add_sequences(self.h, _ptr(codes), codes.size, ctypes.byref(sid)))
+        return sid.value
+
+    def submit_resident(self, kind: int, set_id: int, pairs: np.ndarray) -> int:
+        """Queues pairs whose offsets index resident set `set_id`."""
+        pairs = np.ascontiguousarray(pairs, dtype=PAIR_DTYPE)
+        rid = ctypes.c_uint64()
+        _check(lib().ipuma_server_submit_resident(self.h, kind, set_id, _ptr(pairs), pairs.shape[0],
+                                                  ctypes.byref(rid)))
         return rid.value
 
     def poll(self, rid: int) -> bool:

@@ -25,8 +25,8 @@ def loadgen():
         ib.lib()
         L = ctypes.CDLL(LOADGEN)
         vp, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
-        L.ipuma_loadgen_run.argtypes = [vp, i32, vp, vp, vp, i64, vp, vp, vp, vp, i32, i32, vp, vp,
-                                        ctypes.POINTER(ctypes.c_double)]
+        L.ipuma_loadgen_run.argtypes = [vp, i32, vp, vp, vp, i64, vp, vp, vp, vp, vp, i32, i32, vp,
+                                        vp, ctypes.POINTER(ctypes.c_double)]
         L.ipuma_loadgen_run.restype = ctypes.c_int
         _lg = L
     return _lg
@@ -56,8 +56,12 @@ def schedule(workloads, offered_gcups, duration_s, min_pairs=1, max_pairs=4096, 
     return arrival, kind, first, count, rate
 
 
-def run(server, workloads, arrival, kind, first, count, submitters=4, waiters=8):
-    pairs = [ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len) for wl in workloads]
+def run(server, workloads, arrival, kind, first, count, submitters=4, waiters=8, set_ids=None,
+        pairs=None):
+    """Replays the schedule.  With `set_ids` (one resident set per workload,
+    holding that workload's codes) requests carry only pair descriptors."""
+    if pairs is None:
+        pairs = [ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len) for wl in workloads]
     codes = [np.ascontiguousarray(wl.codes) for wl in workloads]
     k = len(workloads)
     codes_p = (ctypes.c_void_p * k)(*[c.ctypes.data for c in codes])
@@ -71,10 +75,12 @@ def run(server, workloads, arrival, kind, first, count, submitters=4, waiters=8)
     kind = np.ascontiguousarray(kind, np.int32)
     first = np.ascontiguousarray(first, np.int64)
     count = np.ascontiguousarray(count, np.int32)
+    sets = None if set_ids is None else np.ascontiguousarray(set_ids, np.int32)
     rc = loadgen().ipuma_loadgen_run(server.h, k, codes_p, ncodes.ctypes.data, pairs_p, n,
                                      arrival.ctypes.data, kind.ctypes.data, first.ctypes.data,
-                                     count.ctypes.data, submitters, waiters, lat.ctypes.data,
-                                     st.ctypes.data, ctypes.byref(wall))
+                                     count.ctypes.data, None if sets is None else sets.ctypes.data,
+                                     submitters, waiters, lat.ctypes.data, st.ctypes.data,
+                                     ctypes.byref(wall))
     if rc != 0:
         raise RuntimeError("loadgen failed: %d" % rc)
     cells = 0
@@ -91,3 +97,38 @@ def run(server, workloads, arrival, kind, first, count, submitters=4, waiters=8)
         "p99_ms": float(np.percentile(lat[ok], 99)) if ok.any() else None,
         "mean_pairs_per_request": float(count.mean()),
     }
+
+
+def mix_peak(device_gcups, workloads, probs=None):
+    """Batched-engine throughput of a request mix: each workload's device
+    GCUPS weighted by its expected share of the mix's cells."""
+    k = len(workloads)
+    probs = np.full(k, 1.0 / k) if probs is None else np.asarray(probs, float)
+    cpp = np.array([wl.cells / wl.n for wl in workloads])
+    share = probs * cpp / float(np.dot(probs, cpp))
+    return 1.0 / float(np.sum(share / np.asarray(device_gcups, float)))
+
+
+def sweep(make_server, workloads, peak_gcups, loads, duration_s, min_pairs, max_pairs,
+          resident=True, seed=0, max_requests=None):
+    """One open-loop run per offered load (fraction of `peak_gcups`) on a
+    fresh server from `make_server()`; returns a list of result dicts."""
+    out = []
+    pairs = [ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len) for wl in workloads]
+    for j, load in enumerate(loads):
+        dur = duration_s
+        arrival, kind, first, count, rate = schedule(workloads, load * peak_gcups, dur, min_pairs,
+                                                     max_pairs, seed=seed + j)
+        if max_requests and arrival.size > max_requests:
+            keep = max_requests
+            arrival, kind, first, count = arrival[:keep], kind[:keep], first[:keep], count[:keep]
+        with make_server() as srv:
+            sets = [srv.add_sequences(wl.codes) for wl in workloads] if resident else None
+            r = run(srv, workloads, arrival, kind, first, count, set_ids=sets, pairs=pairs)
+            st = srv.stats()
+        r.update({"offered_load": load, "offered_gcups": load * peak_gcups,
+                  "requests_per_s": rate, "batches": int(st.batches),
+                  "mean_pairs_per_batch": float(st.pairs) / max(1, int(st.batches)),
+                  "fraction_of_peak": r["gcups"] / peak_gcups})
+        out.append(r)
+    return out

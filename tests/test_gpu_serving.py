@@ -108,9 +108,9 @@ def test_small_pool_admission_and_split_requests():
     wl = workloads.protein(n=4000, seed=84)
     reqs = [(0, 0, 1500), (0, 1500, 1000), (0, 2500, 1500)]
     alone = _alone([wl], reqs, True)
-    # 4 MiB pool: a batch may use half, so big requests are split and batches
-    # wait for each other's memory.
-    with ib.Server(_scorings([wl]), slots=3, pool_bytes=4 << 20) as srv:
+    # 1 MiB pool: a batch may use half (about 700 of these pairs), so every
+    # request is split and the three slots wait for each other's memory.
+    with ib.Server(_scorings([wl]), slots=3, pool_bytes=1 << 20) as srv:
         mixed = _serve(srv, [wl], reqs, threads=3)
         st = srv.stats()
     assert st.batches > len(reqs)
@@ -119,6 +119,37 @@ def test_small_pool_admission_and_split_requests():
         np.testing.assert_array_equal(sa, sm)
         np.testing.assert_array_equal(aa, am)
         np.testing.assert_array_equal(ba, bm)
+
+
+@pytest.mark.parametrize("forward_only", [True, False])
+def test_resident_sets_match_staged_requests(forward_only):
+    """Requests into resident sequence sets, mixed with requests that carry
+    their codes, give the same results as each request alone."""
+    wls = [workloads.dna_batched(n=5000, seed=91), workloads.protein(n=2500, seed=92)]
+    reqs = _requests(wls, 48, seed=93)
+    alone = _alone(wls, reqs, forward_only)
+    pairs = [ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len) for wl in wls]
+    with ib.Server(_scorings(wls), forward_only=forward_only, slots=3,
+                   max_batch_pairs=1500) as srv:
+        sets = [srv.add_sequences(wl.codes) for wl in wls]
+        ids = []
+        for i, (k, first, cnt) in enumerate(reqs):
+            if i % 3 == 2:
+                codes, p = _request_data(wls[k], first, cnt)
+                ids.append(srv.submit(k, codes, p))
+            else:
+                ids.append(srv.submit_resident(k, sets[k], pairs[k][first:first + cnt]))
+        got = [srv.wait(rid, cnt) for rid, (_, _, cnt) in zip(ids, reqs)]
+        with pytest.raises(ib.IpumaError):
+            srv.submit_resident(0, 7, pairs[0][:1])  # unknown set
+        bad = pairs[0][:1].copy()
+        bad["a_off"] = wls[0].codes.size
+        with pytest.raises(ib.IpumaError):
+            srv.submit_resident(0, sets[0], bad)  # outside the set
+    for i, ((sa, aa, ba), (sm, am, bm, _)) in enumerate(zip(alone, got)):
+        np.testing.assert_array_equal(sa, sm, err_msg="request %d score" % i)
+        np.testing.assert_array_equal(aa, am, err_msg="request %d arange" % i)
+        np.testing.assert_array_equal(ba, bm, err_msg="request %d brange" % i)
 
 
 def test_oversize_pair_is_refused():
@@ -162,13 +193,15 @@ def test_wait_timeout_then_success():
         assert ei.value.code == ib.ERR_UNKNOWN_JOB
 
 
-def test_open_loop_load_generator():
+@pytest.mark.parametrize("resident", [False, True])
+def test_open_loop_load_generator(resident):
     """The C++ load generator replays a Poisson stream; every request
     completes and latencies are recorded."""
     wls = [workloads.dna_batched(n=20000, seed=87), workloads.protein(n=10000, seed=88)]
     arrival, kind, first, count, rate = serving.schedule(wls, offered_gcups=200, duration_s=1.0,
                                                          max_pairs=512, seed=89)
     with ib.Server(_scorings(wls), slots=4) as srv:
-        res = serving.run(srv, wls, arrival, kind, first, count)
+        sets = [srv.add_sequences(wl.codes) for wl in wls] if resident else None
+        res = serving.run(srv, wls, arrival, kind, first, count, set_ids=sets)
     assert res["failed"] == 0 and res["requests"] == arrival.size
     assert res["p99_ms"] >= res["p50_ms"] > 0
