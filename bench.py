@@ -63,6 +63,16 @@ def dist_env():
     return ws, rank, local
 
 
+def max_over_ranks(dist, x, device):
+    """Largest value of `x` over all ranks (identity without a process group)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def make_workload(name, pairs, seed_offset=0):
     import workloads
     fn = workloads.CONFIGS[name]
@@ -272,7 +282,7 @@ def serving_section(args, ib, torch, dev, stream, local):
 
     t0 = time.perf_counter()
     res = {
-        "workload": "poisson requests, 50% dna_batched / 50% protein distributions, "
+        "workload": "poisson requests, 50%% dna_batched / 50%% protein distributions, "
                     "400k + 100k pair pools, %.1f s arrival window per point" % dur,
         "device_gcups": {"dna": g[0], "protein": g[1], "mix_peak": peak},
         "slots": 4,
@@ -405,11 +415,7 @@ def main():
     ev1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(dist, ev0.elapsed_time(ev1), dev)
     ms_step = ms / args.steps
     total_cells = wl.cells * ws
     value = total_cells / (ms_step * 1e-3) / 1e9
@@ -494,11 +500,7 @@ def main():
         t0 = time.perf_counter()
         for _ in range(reps):
             eng.compare_into(codes_np, pairs_view, out_np[0], out_np[1], out_np[2])
-        wall = (time.perf_counter() - t0) / reps
-        if dist:
-            t = torch.tensor([wall], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            wall = float(t.item())
+        wall = max_over_ranks(dist, (time.perf_counter() - t0) / reps, dev)
         e2e_same = bool(np.array_equal(out_np, got))
         e2e = {"value": total_cells / wall / 1e9, "unit": "GCUPS",
                "h2d_bytes_per_step": int(wl.codes.nbytes + pairs_np.nbytes),

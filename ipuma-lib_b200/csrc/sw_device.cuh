@@ -43,6 +43,11 @@
 
 #include <type_traits>
 
+// Steps per unrolled check-free block (0 or >= LANES: the whole block).
+#ifndef IPUMA_STEP_UNROLL
+#define IPUMA_STEP_UNROLL 0
+#endif
+
 namespace ipuma_dev {
 
 constexpr unsigned FULL = 0xffffffffu;
@@ -282,6 +287,9 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
   const V vF0 = T::splat(-sc.gIgE);   // F̂ where F = 0 (pass start)
   const V vZero = T::splat(0);
   const int lim = sc.s16Limit;
+  // Steps unrolled in a check-free block: the block's code has to stay in
+  // the instruction cache next to the checked path.
+  constexpr int kStepUnroll = (IPUMA_STEP_UNROLL > 0 && IPUMA_STEP_UNROLL < LANES) ? IPUMA_STEP_UNROLL : LANES;
 
   for (int strip = 0; strip < nstrips; ++strip) {
     const int col0 = strip * SW;
@@ -431,7 +439,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
         chunkNext = (r < rowsG) ? scrIn[r] : make_int2(0, 0);
       }
       if (t0 >= LANES - 1 && t0 + LANES - 1 < rowsMin) {
-#pragma unroll
+#pragma unroll kStepUnroll
         for (int k = 0; k < LANES; ++k) step(t0 + k, std::false_type{});
       } else {
 #pragma unroll 1
