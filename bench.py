@@ -264,7 +264,6 @@ def serving_section(args, ib, torch, dev, stream, local):
     wls = [workloads.dna_batched(n=400_000, seed=2001), workloads.protein(n=100_000, seed=2002)]
     g = [device_gcups(ib, torch, wl, dev, stream, local) for wl in wls]
     peak = serving.mix_peak(g, wls)
-    peak64 = peak  # same mix, same engine
     scorings = [ib.sw_config(wl.gap_init, wl.gap_extend, wl.match, wl.mismatch, wl.ambiguity,
                              wl.similarity, wl.datatype) for wl in wls]
 
@@ -286,23 +285,25 @@ def serving_section(args, ib, torch, dev, stream, local):
                     "400k + 100k pair pools, %.1f s arrival window per point" % dur,
         "device_gcups": {"dna": g[0], "protein": g[1], "mix_peak": peak},
         "slots": 4,
-        "sizes_1_4096_resident": slim(serving.sweep(server, wls, peak, loads, dur, 1, 4096,
-                                                    resident=True, seed=10)),
-        "sizes_1_4096_staged": slim(serving.sweep(server, wls, peak, loads, dur, 1, 4096,
-                                                  resident=False, seed=20)),
-        "pairs_64_resident": slim(serving.sweep(server, wls, peak64, [0.5, 0.8, 1.0], dur, 64, 64,
-                                                resident=True, seed=30)),
-        "pairs_64_staged": slim(serving.sweep(server, wls, peak64, [0.8], dur, 64, 64,
-                                              resident=False, seed=40)),
-        "per_request_baseline": {
-            "what": "one request per device batch (no coalescing), resident sets, 4 slots",
-            "sizes_1_4096": slim(serving.sweep(lambda: server(True), wls, peak, [0.1, 0.25, 0.5],
-                                               dur, 1, 4096, resident=True, seed=50,
-                                               max_requests=3000)),
-            "pairs_64": slim(serving.sweep(lambda: server(True), wls, peak64, [0.1, 0.8], dur,
-                                           64, 64, resident=True, seed=60, max_requests=6000)),
-        },
     }
+    with server() as srv:
+        sets = [srv.add_sequences(wl.codes) for wl in wls]
+        res["sizes_1_4096_resident"] = slim(serving.sweep(srv, wls, peak, loads, dur, 1, 4096,
+                                                          set_ids=sets, seed=10))
+        res["pairs_64_resident"] = slim(serving.sweep(srv, wls, peak, [0.5, 0.8, 1.0], dur, 64, 64,
+                                                      set_ids=sets, seed=30))
+        res["sizes_1_4096_staged"] = slim(serving.sweep(srv, wls, peak, loads, dur, 1, 4096,
+                                                        seed=20))
+        res["pairs_64_staged"] = slim(serving.sweep(srv, wls, peak, [0.8], dur, 64, 64, seed=40))
+    with server(True) as srv:
+        sets = [srv.add_sequences(wl.codes) for wl in wls]
+        res["per_request_baseline"] = {
+            "what": "one request per device batch (no coalescing), resident sets, 4 slots",
+            "sizes_1_4096": slim(serving.sweep(srv, wls, peak, [0.1, 0.25, 0.5], dur, 1, 4096,
+                                               set_ids=sets, seed=50, max_requests=3000)),
+            "pairs_64": slim(serving.sweep(srv, wls, peak, [0.1, 0.8], dur, 64, 64, set_ids=sets,
+                                           seed=60, max_requests=6000)),
+        }
     res["seconds"] = time.perf_counter() - t0
     return res
 

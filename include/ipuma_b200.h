@@ -208,6 +208,12 @@ int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_c
                              int32_t max_b_len, int32_t* d_score, int32_t* d_arange,
                              int32_t* d_brange, void* stream);
 
+/* Grows every device buffer that ipuma_gpu_compare_device needs for up to
+ * n pairs with |A| <= max_a_len and |B| <= max_b_len, so that such calls
+ * allocate (and synchronise the device) no more -- for serving loops and
+ * before a stream capture.  No counterpart in the reference. */
+int ipuma_gpu_reserve(ipuma_engine* e, int32_t n, int32_t max_a_len, int32_t max_b_len);
+
 /* Wire-buffer batch with inputs and results already in device memory,
  * enqueued on `stream` (NULL = the engine's stream); the call returns once
  * the batch has finished.  Sizes as for ipuma_gpu_run_buffer; the Meta
@@ -266,6 +272,9 @@ typedef struct ipuma_server_config {
   int32_t device;
   int32_t one_request_per_batch;   /* 1: no coalescing (each batch = one request or
                                       part of one), the per-request baseline */
+  int64_t max_batch_cells;         /* cells per device batch (latency bound); 0 = 2e9 */
+  int32_t reserve_b_len;           /* |B| the engines' buffers are sized for at start;
+                                      0 = 2048 (longer pairs grow them on demand) */
 } ipuma_server_config;
 
 typedef struct ipuma_server_stats {

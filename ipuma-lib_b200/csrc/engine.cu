@@ -63,7 +63,9 @@ struct DevBuf {
       p = nullptr;
       cap = 0;
     }
-    size_t want = std::max<size_t>(bytes, 256);
+    // Geometric growth: a stream of slowly growing batches reallocates
+    // (and synchronises the device in cudaFree) only a few times.
+    size_t want = std::max<size_t>({bytes, (size_t)256, cap + cap / 2});
     want = (want + (1u << 20) - 1) & ~(size_t)((1u << 20) - 1);
     cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
@@ -831,6 +833,18 @@ int ipuma_gpu_tuning(ipuma_engine* e, char* buf, size_t cap) {
 int ipuma_gpu_last_stats(ipuma_engine* e, ipuma_stats* out) {
   if (!e || !out) return fail(IPUMA_ERR_INVALID_ARG, "null argument");
   *out = e->stats;
+  return IPUMA_OK;
+}
+
+int ipuma_gpu_reserve(ipuma_engine* e, int32_t n, int32_t max_a_len, int32_t max_b_len) {
+  if (!e) return fail(IPUMA_ERR_INVALID_ARG, "null engine");
+  if (n < 0 || max_a_len < 0 || max_b_len < 0 || max_a_len > 65535 || max_b_len > 65535)
+    return fail(IPUMA_ERR_INVALID_ARG, "bad reservation (%d pairs, %d x %d)", n, max_a_len, max_b_len);
+  std::lock_guard<std::mutex> lk(e->mu);
+  CUDA_TRY(cudaSetDevice(e->device));
+  int rc;
+  if ((rc = reserve_batched(e, e->stream, n, max_a_len, max_b_len))) return rc;
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
   return IPUMA_OK;
 }
 

@@ -9,7 +9,19 @@
 // cost-binned engine on it and scatter the results back per request.  A
 // request that arrives while batches run on other slots joins the next
 // batch a slot forms, so work of different requests overlaps on the
-// device; a large request is split across batches.
+// device; a large request is split across batches.  A batch holds at most
+// max_batch_pairs pairs and (beyond its first pair) max_batch_cells cells,
+// which bounds how long a request waits behind one batch.
+//
+// Resident sequence sets: a caller that aligns against the same sequences
+// again and again uploads them once (ipuma_server_add_sequences); requests
+// then carry only pair descriptors into that set and batches stage nothing
+// but pairs.  A batch holds requests of one scoring and one set.
+//
+// Engines for every slot and scoring are created, autotuned (one scoring
+// after the other) and given device buffers for reserve_b_len rows when
+// the server starts, so no request waits for an engine, a tuning run or an
+// allocation that synchronises the device.
 //
 // Admission by free HBM: the device pool (one allocation made when the
 // server starts, sized from the free device memory) is carved per batch by
@@ -17,14 +29,10 @@
 // waits until running batches return theirs.  A request that cannot fit
 // even an empty pool is refused at submission.
 //
-// Resident sequence sets: a caller that aligns against the same sequences
-// again and again uploads them once (ipuma_server_add_sequences); requests
-// then carry only pair descriptors into that set and batches stage nothing
-// but pairs.  A batch holds requests of one scoring and one set.
-//
-// Engines for every slot and scoring are created (and autotuned, one
-// scoring after the other) when the server starts, so no request waits
-// for an engine and no tuning runs beside live batches.
+// Locking: one mutex guards the queues and the pool; requests in flight
+// live in 64 shards (id % 64), each with its own mutex and condition
+// variable, and count their unfinished pairs in an atomic, so completing
+// one request wakes only the waiters of its shard.
 //
 // Failure handling is on the host: a closed server refuses submissions,
 // waits have timeouts, and a failing batch marks its requests failed
@@ -32,6 +40,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -41,6 +50,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "errors.h"
@@ -60,11 +70,11 @@ struct Request {
   std::vector<ipuma_pair> pairs;
   std::vector<int32_t> score, arange, brange;
   int64_t cells = 0;
-  int next = 0;          // first pair not yet given to a batch
-  int outstanding = 0;   // pairs in batches not yet finished
-  int error = IPUMA_OK;
-  std::string message;
-  bool done = false;
+  int next = 0;                   // first pair not yet given to a batch (queue mutex)
+  std::atomic<int> remaining{0};  // pairs not yet finished
+  std::atomic<int> error{IPUMA_OK};
+  std::string message;            // shard mutex
+  bool done = false;              // shard mutex
   Clock::time_point t_submit, t_done;
 };
 
@@ -122,35 +132,48 @@ size_t batch_bytes(size_t codes, size_t pairs) {
   return up(codes) + up(pairs * sizeof(ipuma_pair)) + up(pairs * 3 * sizeof(int32_t));
 }
 
-}  // namespace
-
 struct ResidentSet {
   uint8_t* d_codes = nullptr;
   size_t n_codes = 0;
 };
+
+constexpr int kShards = 64;
+
+struct Shard {
+  std::mutex mu;
+  std::condition_variable cv;
+  std::unordered_map<uint64_t, std::shared_ptr<Request>> live;
+};
+
+}  // namespace
 
 struct ipuma_server {
   ipuma_server_config cfg{};
   std::vector<ipuma_sw_config> scorings;
   int device = 0;
   uint8_t* d_pool = nullptr;
-  std::unique_ptr<Pool> pool;
-  std::vector<ResidentSet> sets;   // append-only; freed at destroy
+  size_t pool_size = 0;
   std::vector<std::vector<ipuma_engine*>> engines;  // [slot][scoring]
+  // Queue state, under `mu`.
   std::mutex mu;
   std::condition_variable cv_work;  // work queued / pool freed / closing
-  std::condition_variable cv_done;  // a request finished
+  std::unique_ptr<Pool> pool;
+  std::vector<ResidentSet> sets;    // append-only; freed at destroy
   // Requests with pairs not yet batched, one FIFO per (scoring, set).
   std::map<std::pair<int, int>, std::deque<std::shared_ptr<Request>>> queues;
   int64_t n_queued = 0;
-  std::map<uint64_t, std::shared_ptr<Request>> live;
-  uint64_t next_id = 1;
   bool closing = false;
   std::vector<std::thread> workers;
-  // statistics
-  int64_t submitted = 0, completed = 0, batches = 0, pairs_done = 0, cells_done = 0;
+  // Requests in flight, by id.
+  Shard shards[kShards];
+  std::atomic<uint64_t> next_id{1};
+  // Statistics (under `mu` unless atomic).
+  std::atomic<int64_t> submitted{0}, completed{0};
+  int64_t batches = 0, pairs_done = 0, cells_done = 0;
   int64_t max_batch_pairs_seen = 0, max_pool_used = 0;
   double busy_ms = 0;
+
+  Shard& shard(uint64_t id) { return shards[id % kShards]; }
 };
 
 namespace {
@@ -164,21 +187,30 @@ struct SlotState {
   size_t cap_codes = 0, cap_pairs = 0;
 };
 
-void finish_request(ipuma_server* s, const std::shared_ptr<Request>& r) {
-  r->done = true;
-  r->t_done = Clock::now();
-  s->completed++;
+// Marks `count` pairs of a request finished; the last ones complete it.
+void finish_pairs(ipuma_server* s, const std::shared_ptr<Request>& r, int count) {
+  if (r->remaining.fetch_sub(count, std::memory_order_acq_rel) != count) return;
+  Shard& sh = s->shard(r->id);
+  {
+    std::lock_guard<std::mutex> lk(sh.mu);
+    r->done = true;
+    r->t_done = Clock::now();
+  }
+  s->completed.fetch_add(1, std::memory_order_relaxed);
+  sh.cv.notify_all();
 }
 
 void fail_chunks(ipuma_server* s, std::vector<Chunk>& chunks, int code, const std::string& msg) {
-  std::lock_guard<std::mutex> lk(s->mu);
   for (auto& c : chunks) {
-    c.req->error = code;
-    c.req->message = msg;
-    c.req->outstanding -= c.count;
-    if (c.req->outstanding == 0 && c.req->next >= (int)c.req->pairs.size()) finish_request(s, c.req);
+    {
+      std::lock_guard<std::mutex> lk(s->shard(c.req->id).mu);
+      if (c.req->error.load() == IPUMA_OK) {
+        c.req->error.store(code);
+        c.req->message = msg;
+      }
+    }
+    finish_pairs(s, c.req, c.count);
   }
-  s->cv_done.notify_all();
 }
 
 void worker_loop(ipuma_server* s, int slot_index) {
@@ -191,6 +223,7 @@ void worker_loop(ipuma_server* s, int slot_index) {
   cudaHostAlloc((void**)&st.h_codes, st.cap_codes, cudaHostAllocDefault);
   cudaHostAlloc((void**)&st.h_pairs, st.cap_pairs * sizeof(ipuma_pair), cudaHostAllocDefault);
   cudaHostAlloc((void**)&st.h_out, st.cap_pairs * 3 * sizeof(int32_t), cudaHostAllocDefault);
+  const int64_t cell_cap = s->cfg.max_batch_cells;
 
   while (true) {
     std::vector<Chunk> chunks;
@@ -215,24 +248,28 @@ void worker_loop(ipuma_server* s, int slot_index) {
       set = qi->first.second;
       if (set >= 0) rs = s->sets[set];
       auto& q = qi->second;
-      while (!q.empty() && npairs < st.cap_pairs) {
+      while (!q.empty()) {
         std::shared_ptr<Request> r = q.front();
         int take = 0;
         size_t bytes = 0;
         while (r->next + take < (int)r->pairs.size() && npairs + take < st.cap_pairs) {
           const ipuma_pair& p = r->pairs[r->next + take];
           const size_t add = set >= 0 ? 0 : (size_t)p.a_len + (size_t)p.b_len;
-          if (npairs + take > 0 && batch_bytes(codes_bytes + bytes + add, npairs + take + 1) > s->pool->size() / 2)
+          const int64_t c = (int64_t)p.a_len * p.b_len;
+          if (npairs + take > 0 &&
+              (batch_bytes(codes_bytes + bytes + add, npairs + take + 1) > s->pool_size / 2 ||
+               cells + c > cell_cap))
             break;
           bytes += add;
+          cells += c;
           ++take;
         }
-        if (take == 0) break;
-        chunks.push_back({r, r->next, take});
-        r->next += take;
-        r->outstanding += take;
-        npairs += take;
-        codes_bytes += bytes;
+        if (take > 0) {
+          chunks.push_back({r, r->next, take});
+          r->next += take;
+          npairs += take;
+          codes_bytes += bytes;
+        }
         if (r->next < (int)r->pairs.size()) break;  // batch full
         q.pop_front();
         s->n_queued--;
@@ -261,7 +298,6 @@ void worker_loop(ipuma_server* s, int slot_index) {
           const ipuma_pair& p = st.h_pairs[k + i];
           maxA = std::max(maxA, p.a_len);
           maxB = std::max(maxB, p.b_len);
-          cells += (int64_t)p.a_len * p.b_len;
         }
         k += c.count;
         continue;
@@ -275,7 +311,6 @@ void worker_loop(ipuma_server* s, int slot_index) {
         st.h_pairs[k] = q;
         maxA = std::max(maxA, p.a_len);
         maxB = std::max(maxB, p.b_len);
-        cells += (int64_t)p.a_len * p.b_len;
       }
     }
     uint8_t* d_codes = set >= 0 ? rs.d_codes : s->d_pool + pool_off;
@@ -287,7 +322,7 @@ void worker_loop(ipuma_server* s, int slot_index) {
     const auto t0 = Clock::now();
     int rc = IPUMA_OK;
     std::string msg;
-    if (rc == IPUMA_OK && npairs > 0) {
+    if (npairs > 0) {
       if ((set < 0 && cudaMemcpyAsync(d_codes, st.h_codes, codes_bytes, cudaMemcpyHostToDevice, st.stream) !=
                           cudaSuccess) ||
           cudaMemcpyAsync(d_pairs, st.h_pairs, npairs * sizeof(ipuma_pair), cudaMemcpyHostToDevice, st.stream) !=
@@ -314,32 +349,29 @@ void worker_loop(ipuma_server* s, int slot_index) {
       std::lock_guard<std::mutex> lk(s->mu);
       s->pool->release(pool_off, pool_len);
       s->busy_ms += ms;
+      if (rc == IPUMA_OK) {
+        s->batches++;
+        s->pairs_done += (int64_t)npairs;
+        s->cells_done += cells;
+        s->max_batch_pairs_seen = std::max<int64_t>(s->max_batch_pairs_seen, (int64_t)npairs);
+      }
     }
     s->cv_work.notify_all();
     if (rc != IPUMA_OK) {
       fail_chunks(s, chunks, rc, msg);
       continue;
     }
-    // Scatter results back per request.
-    {
-      std::lock_guard<std::mutex> lk(s->mu);
-      size_t idx = 0;
-      for (auto& c : chunks) {
-        Request& r = *c.req;
-        for (int i = 0; i < c.count; ++i, ++idx) {
-          r.score[c.first + i] = st.h_out[idx];
-          r.arange[c.first + i] = st.h_out[npairs + idx];
-          r.brange[c.first + i] = st.h_out[2 * npairs + idx];
-        }
-        r.outstanding -= c.count;
-        if (r.outstanding == 0 && r.next >= (int)r.pairs.size()) finish_request(s, c.req);
-      }
-      s->batches++;
-      s->pairs_done += (int64_t)npairs;
-      s->cells_done += cells;
-      s->max_batch_pairs_seen = std::max<int64_t>(s->max_batch_pairs_seen, (int64_t)npairs);
+    // Scatter results back per request (each chunk's range belongs to this
+    // batch alone; finish_pairs publishes them under the shard mutex).
+    size_t idx = 0;
+    for (auto& c : chunks) {
+      Request& r = *c.req;
+      std::memcpy(r.score.data() + c.first, st.h_out + idx, sizeof(int32_t) * c.count);
+      std::memcpy(r.arange.data() + c.first, st.h_out + npairs + idx, sizeof(int32_t) * c.count);
+      std::memcpy(r.brange.data() + c.first, st.h_out + 2 * npairs + idx, sizeof(int32_t) * c.count);
+      idx += c.count;
+      finish_pairs(s, c.req, c.count);
     }
-    s->cv_done.notify_all();
   }
   cudaFreeHost(st.h_codes);
   cudaFreeHost(st.h_pairs);
@@ -353,24 +385,46 @@ int enqueue(ipuma_server* s, const std::shared_ptr<Request>& r, uint64_t* req) {
   r->score.assign(n, 0);
   r->arange.assign(n, 0);
   r->brange.assign(n, 0);
+  r->remaining.store((int)n);
   r->t_submit = Clock::now();
+  r->id = s->next_id.fetch_add(1);
+  // Registered before it is queued, so a worker may finish it at once.
+  Shard& sh = s->shard(r->id);
+  {
+    std::lock_guard<std::mutex> lk(sh.mu);
+    if (n == 0) {
+      r->done = true;
+      r->t_done = r->t_submit;
+    }
+    sh.live[r->id] = r;
+  }
+  bool closed = false;
   {
     std::lock_guard<std::mutex> lk(s->mu);
-    if (s->closing) return fail(IPUMA_ERR_CLOSED, "server is closed");
-    r->id = s->next_id++;
-    s->submitted++;
-    s->live[r->id] = r;
-    if (n == 0) {
-      finish_request(s, r);
-    } else {
+    if (s->closing) {
+      closed = true;
+    } else if (n > 0) {
       s->queues[{r->kind, r->set}].push_back(r);
       s->n_queued++;
     }
-    *req = r->id;
   }
-  s->cv_work.notify_one();
-  if (n == 0) s->cv_done.notify_all();
+  if (closed) {
+    std::lock_guard<std::mutex> lk(sh.mu);
+    sh.live.erase(r->id);
+    return fail(IPUMA_ERR_CLOSED, "server is closed");
+  }
+  s->submitted.fetch_add(1, std::memory_order_relaxed);
+  if (n == 0)
+    s->completed.fetch_add(1, std::memory_order_relaxed);
+  else
+    s->cv_work.notify_one();
+  *req = r->id;
   return IPUMA_OK;
+}
+
+bool pair_ok(const ipuma_pair& p, size_t n_codes) {
+  return p.a_len >= 0 && p.b_len >= 0 && p.a_len <= 65535 && p.b_len <= 65535 && p.a_off >= 0 && p.b_off >= 0 &&
+         (size_t)p.a_off + p.a_len <= n_codes && (size_t)p.b_off + p.b_len <= n_codes;
 }
 
 }  // namespace
@@ -385,6 +439,9 @@ int ipuma_server_create(const ipuma_server_config* cfg, ipuma_server** out) {
   s->cfg.scorings = nullptr;
   if (s->cfg.slots <= 0) s->cfg.slots = 4;
   if (s->cfg.max_batch_pairs <= 0) s->cfg.max_batch_pairs = 65536;
+  if (s->cfg.max_batch_cells <= 0) s->cfg.max_batch_cells = 2000000000LL;
+  if (s->cfg.reserve_b_len <= 0) s->cfg.reserve_b_len = 2048;
+  s->cfg.reserve_b_len = std::min(s->cfg.reserve_b_len, 65535);
   s->device = cfg->device;
   if (cudaSetDevice(s->device) != cudaSuccess) return fail(IPUMA_ERR_NO_DEVICE, "cannot use device %d", s->device);
   size_t freeB = 0, totalB = 0;
@@ -394,7 +451,9 @@ int ipuma_server_create(const ipuma_server_config* cfg, ipuma_server** out) {
   if (pool < (1u << 20)) return fail(IPUMA_ERR_NO_MEMORY, "not enough free device memory for the pool");
   if (cudaMalloc(&s->d_pool, pool) != cudaSuccess) return fail(IPUMA_ERR_NO_MEMORY, "pool allocation failed");
   s->pool.reset(new Pool(pool));
-  // Engines for every slot and scoring, tuned here, one after the other.
+  s->pool_size = pool;
+  // Engines for every slot and scoring: tuned and given their buffers here,
+  // one after the other.
   ipuma_algo_config algo{1, 300, 20, 3000, 0, 0, s->cfg.forward_only, 0, 1, 0};
   s->engines.assign(s->cfg.slots, std::vector<ipuma_engine*>(s->scorings.size(), nullptr));
   int rc = IPUMA_OK;
@@ -402,6 +461,8 @@ int ipuma_server_create(const ipuma_server_config* cfg, ipuma_server** out) {
     for (size_t k = 0; k < s->scorings.size() && rc == IPUMA_OK; ++k) {
       rc = ipuma_gpu_create(&s->scorings[k], &algo, s->device, &s->engines[i][k]);
       if (rc == IPUMA_OK) rc = ipuma_gpu_autotune(s->engines[i][k], nullptr);
+      if (rc == IPUMA_OK)
+        rc = ipuma_gpu_reserve(s->engines[i][k], s->cfg.max_batch_pairs, s->cfg.reserve_b_len, s->cfg.reserve_b_len);
     }
   if (rc != IPUMA_OK) {
     const std::string msg = ipuma_last_error();
@@ -450,10 +511,8 @@ int ipuma_server_submit(ipuma_server* s, int32_t kind, const uint8_t* codes, siz
   size_t need = 0;
   for (int i = 0; i < n; ++i) {
     const ipuma_pair& p = pairs[i];
-    if (p.a_len < 0 || p.b_len < 0 || p.a_len > 65535 || p.b_len > 65535 || p.a_off < 0 || p.b_off < 0 ||
-        (size_t)p.a_off + p.a_len > n_codes || (size_t)p.b_off + p.b_len > n_codes)
-      return fail(IPUMA_ERR_INVALID_ARG, "pair %d lies outside the code array", i);
-    if (batch_bytes((size_t)p.a_len + p.b_len, 1) > s->pool->size() / 2)
+    if (!pair_ok(p, n_codes)) return fail(IPUMA_ERR_INVALID_ARG, "pair %d lies outside the code array", i);
+    if (batch_bytes((size_t)p.a_len + p.b_len, 1) > s->pool_size / 2)
       return fail(IPUMA_ERR_NO_MEMORY, "pair %d does not fit the device pool", i);
     need += (size_t)p.a_len + p.b_len;
     r->cells += (int64_t)p.a_len * p.b_len;
@@ -486,9 +545,7 @@ int ipuma_server_submit_resident(ipuma_server* s, int32_t kind, int32_t set_id, 
   r->set = set_id;
   for (int i = 0; i < n; ++i) {
     const ipuma_pair& p = pairs[i];
-    if (p.a_len < 0 || p.b_len < 0 || p.a_len > 65535 || p.b_len > 65535 || p.a_off < 0 || p.b_off < 0 ||
-        (size_t)p.a_off + p.a_len > n_codes || (size_t)p.b_off + p.b_len > n_codes)
-      return fail(IPUMA_ERR_INVALID_ARG, "pair %d lies outside the sequence set", i);
+    if (!pair_ok(p, n_codes)) return fail(IPUMA_ERR_INVALID_ARG, "pair %d lies outside the sequence set", i);
     r->cells += (int64_t)p.a_len * p.b_len;
   }
   r->pairs.assign(pairs, pairs + n);
@@ -497,9 +554,10 @@ int ipuma_server_submit_resident(ipuma_server* s, int32_t kind, int32_t set_id, 
 
 int ipuma_server_poll(ipuma_server* s, uint64_t req, int32_t* done) {
   if (!s || !done) return fail(IPUMA_ERR_INVALID_ARG, "null argument");
-  std::lock_guard<std::mutex> lk(s->mu);
-  auto it = s->live.find(req);
-  if (it == s->live.end()) return fail(IPUMA_ERR_UNKNOWN_JOB, "unknown request %llu", (unsigned long long)req);
+  Shard& sh = s->shard(req);
+  std::lock_guard<std::mutex> lk(sh.mu);
+  auto it = sh.live.find(req);
+  if (it == sh.live.end()) return fail(IPUMA_ERR_UNKNOWN_JOB, "unknown request %llu", (unsigned long long)req);
   *done = it->second->done ? 1 : 0;
   return IPUMA_OK;
 }
@@ -507,19 +565,23 @@ int ipuma_server_poll(ipuma_server* s, uint64_t req, int32_t* done) {
 int ipuma_server_wait(ipuma_server* s, uint64_t req, int64_t timeout_ms, int32_t* score, int32_t* arange,
                       int32_t* brange, double* latency_ms) {
   if (!s) return fail(IPUMA_ERR_INVALID_ARG, "null server");
-  std::unique_lock<std::mutex> lk(s->mu);
-  auto it = s->live.find(req);
-  if (it == s->live.end()) return fail(IPUMA_ERR_UNKNOWN_JOB, "unknown request %llu", (unsigned long long)req);
-  std::shared_ptr<Request> r = it->second;
-  auto pred = [&] { return r->done; };
-  if (timeout_ms < 0) {
-    s->cv_done.wait(lk, pred);
-  } else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), pred)) {
-    return fail(IPUMA_ERR_TIMEOUT, "request %llu not finished after %lld ms", (unsigned long long)req,
-                (long long)timeout_ms);
+  Shard& sh = s->shard(req);
+  std::shared_ptr<Request> r;
+  {
+    std::unique_lock<std::mutex> lk(sh.mu);
+    auto it = sh.live.find(req);
+    if (it == sh.live.end()) return fail(IPUMA_ERR_UNKNOWN_JOB, "unknown request %llu", (unsigned long long)req);
+    r = it->second;
+    auto pred = [&] { return r->done; };
+    if (timeout_ms < 0) {
+      sh.cv.wait(lk, pred);
+    } else if (!sh.cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), pred)) {
+      return fail(IPUMA_ERR_TIMEOUT, "request %llu not finished after %lld ms", (unsigned long long)req,
+                  (long long)timeout_ms);
+    }
+    sh.live.erase(r->id);
+    if (r->error.load() != IPUMA_OK) return fail(r->error.load(), "request failed: %s", r->message.c_str());
   }
-  s->live.erase(r->id);
-  if (r->error != IPUMA_OK) return fail(r->error, "request failed: %s", r->message.c_str());
   const size_t n = r->score.size();
   if (n) {
     if (score) std::memcpy(score, r->score.data(), n * sizeof(int32_t));
@@ -533,8 +595,8 @@ int ipuma_server_wait(ipuma_server* s, uint64_t req, int64_t timeout_ms, int32_t
 int ipuma_server_get_stats(ipuma_server* s, ipuma_server_stats* out) {
   if (!s || !out) return fail(IPUMA_ERR_INVALID_ARG, "null argument");
   std::lock_guard<std::mutex> lk(s->mu);
-  out->submitted = s->submitted;
-  out->completed = s->completed;
+  out->submitted = s->submitted.load();
+  out->completed = s->completed.load();
   out->queued = s->n_queued;
   out->batches = s->batches;
   out->pairs = s->pairs_done;
@@ -561,16 +623,18 @@ void ipuma_server_destroy(ipuma_server* s) {
   if (!s) return;
   ipuma_server_close(s);
   for (auto& t : s->workers) t.join();
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    for (auto& kv : s->live)
-      if (!kv.second->done) {
-        kv.second->error = IPUMA_ERR_CLOSED;
-        kv.second->message = "server closed";
-        kv.second->done = true;
-      }
+  for (auto& sh : s->shards) {
+    {
+      std::lock_guard<std::mutex> lk(sh.mu);
+      for (auto& kv : sh.live)
+        if (!kv.second->done) {
+          kv.second->error.store(IPUMA_ERR_CLOSED);
+          kv.second->message = "server closed";
+          kv.second->done = true;
+        }
+    }
+    sh.cv.notify_all();
   }
-  s->cv_done.notify_all();
   cudaSetDevice(s->device);
   for (auto& row : s->engines)
     for (auto* e : row)

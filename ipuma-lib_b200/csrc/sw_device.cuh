@@ -43,7 +43,8 @@
 
 #include <type_traits>
 
-// Steps per unrolled check-free block (0 or >= LANES: the whole block).
+// Steps per unrolled check-free block (0: by K, as measured; >= LANES:
+// the whole block).
 #ifndef IPUMA_STEP_UNROLL
 #define IPUMA_STEP_UNROLL 0
 #endif
@@ -289,7 +290,10 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
   const int lim = sc.s16Limit;
   // Steps unrolled in a check-free block: the block's code has to stay in
   // the instruction cache next to the checked path.
-  constexpr int kStepUnroll = (IPUMA_STEP_UNROLL > 0 && IPUMA_STEP_UNROLL < LANES) ? IPUMA_STEP_UNROLL : LANES;
+  // (Measured on B200: 8 steps for K <= 12, 4 for K = 16; the full LANES
+  // steps stalled on instruction fetch.)
+  constexpr int kStepUnroll = IPUMA_STEP_UNROLL > 0 ? (IPUMA_STEP_UNROLL < LANES ? IPUMA_STEP_UNROLL : LANES)
+                                                   : (K >= 16 ? 4 : 8);
 
   for (int strip = 0; strip < nstrips; ++strip) {
     const int col0 = strip * SW;

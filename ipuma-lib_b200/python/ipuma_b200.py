@@ -41,6 +41,7 @@ EXPORTS = [
     "ipuma_gpu_autotune", "ipuma_gpu_tuning", "ipuma_server_create", "ipuma_server_submit",
     "ipuma_server_poll", "ipuma_server_wait", "ipuma_server_get_stats", "ipuma_server_close",
     "ipuma_server_destroy", "ipuma_server_add_sequences", "ipuma_server_submit_resident",
+    "ipuma_gpu_reserve",
 ]
 
 KERNEL_NAMES = {0: "k_batched<s32,L32,K16>", 1: "k_batched<s16x2,L16,K4>",
@@ -87,7 +88,8 @@ class ServerConfig(ctypes.Structure):
     _fields_ = [("n_scorings", ctypes.c_int32), ("scorings", ctypes.POINTER(SwConfig)),
                 ("forward_only", ctypes.c_int32), ("slots", ctypes.c_int32),
                 ("pool_bytes", ctypes.c_int64), ("max_batch_pairs", ctypes.c_int32),
-                ("device", ctypes.c_int32), ("one_request_per_batch", ctypes.c_int32)]
+                ("device", ctypes.c_int32), ("one_request_per_batch", ctypes.c_int32),
+                ("max_batch_cells", ctypes.c_int64), ("reserve_b_len", ctypes.c_int32)]
 
 
 class ServerStats(ctypes.Structure):
@@ -129,6 +131,7 @@ def lib():
         L.ipuma_gpu_run_buffer_device.argtypes = [vp, vp, sz, vp, sz, vp]
         L.ipuma_measure_int_peak.argtypes = [i32, ctypes.POINTER(ctypes.c_double)]
         L.ipuma_gpu_autotune.argtypes = [vp, ctypes.c_char_p]
+        L.ipuma_gpu_reserve.argtypes = [vp, i32, i32, i32]
         L.ipuma_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
         L.ipuma_server_submit.argtypes = [vp, i32, vp, sz, vp, i32, ctypes.POINTER(ctypes.c_uint64)]
         L.ipuma_server_add_sequences.argtypes = [vp, vp, sz, ctypes.POINTER(i32)]
@@ -245,6 +248,10 @@ class Engine:
     def autotune(self, cache_path: str | None = None):
         _check(lib().ipuma_gpu_autotune(self.h, cache_path.encode() if cache_path else None))
 
+    def reserve(self, n: int, max_a_len: int, max_b_len: int):
+        """Grows the device buffers for compare_device calls up to this size."""
+        _check(lib().ipuma_gpu_reserve(self.h, n, max_a_len, max_b_len))
+
     def tuning(self) -> dict:
         import json
         buf = ctypes.create_string_buffer(4096)
@@ -324,10 +331,11 @@ class Server:
     """Serving loop (ipuma_server_*): continuous batching of requests."""
 
     def __init__(self, scorings, forward_only=True, slots=4, pool_bytes=0, max_batch_pairs=0,
-                 device=0, one_request_per_batch=False):
+                 device=0, one_request_per_batch=False, max_batch_cells=0, reserve_b_len=0):
         self._scorings = (SwConfig * len(scorings))(*scorings)
         cfg = ServerConfig(len(scorings), self._scorings, int(bool(forward_only)), slots,
-                           pool_bytes, max_batch_pairs, device, int(bool(one_request_per_batch)))
+                           pool_bytes, max_batch_pairs, device, int(bool(one_request_per_batch)),
+                           max_batch_cells, reserve_b_len)
         h = ctypes.c_void_p()
         _check(lib().ipuma_server_create(ctypes.byref(cfg), ctypes.byref(h)))
         self.h = h

@@ -109,26 +109,31 @@ def mix_peak(device_gcups, workloads, probs=None):
     return 1.0 / float(np.sum(share / np.asarray(device_gcups, float)))
 
 
-def sweep(make_server, workloads, peak_gcups, loads, duration_s, min_pairs, max_pairs,
-          resident=True, seed=0, max_requests=None):
-    """One open-loop run per offered load (fraction of `peak_gcups`) on a
-    fresh server from `make_server()`; returns a list of result dicts."""
-    out = []
+def sweep(server, workloads, peak_gcups, loads, duration_s, min_pairs, max_pairs, set_ids=None,
+          seed=0, max_requests=None, warmup_s=0.3):
+    """One open-loop run per offered load (fraction of `peak_gcups`) on
+    `server`, after a short warm-up run at half load; `set_ids` (resident
+    sets holding each workload's codes) sends pair descriptors only.
+    Returns a list of result dicts."""
     pairs = [ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len) for wl in workloads]
+    if warmup_s > 0:
+        arrival, kind, first, count, _ = schedule(workloads, 0.5 * peak_gcups, warmup_s, min_pairs,
+                                                  max_pairs, seed=seed + 999)
+        run(server, workloads, arrival, kind, first, count, set_ids=set_ids, pairs=pairs)
+    out = []
     for j, load in enumerate(loads):
-        dur = duration_s
-        arrival, kind, first, count, rate = schedule(workloads, load * peak_gcups, dur, min_pairs,
-                                                     max_pairs, seed=seed + j)
+        arrival, kind, first, count, rate = schedule(workloads, load * peak_gcups, duration_s,
+                                                     min_pairs, max_pairs, seed=seed + j)
         if max_requests and arrival.size > max_requests:
             keep = max_requests
             arrival, kind, first, count = arrival[:keep], kind[:keep], first[:keep], count[:keep]
-        with make_server() as srv:
-            sets = [srv.add_sequences(wl.codes) for wl in workloads] if resident else None
-            r = run(srv, workloads, arrival, kind, first, count, set_ids=sets, pairs=pairs)
-            st = srv.stats()
+        b0 = server.stats()
+        r = run(server, workloads, arrival, kind, first, count, set_ids=set_ids, pairs=pairs)
+        b1 = server.stats()
+        nb = int(b1.batches - b0.batches)
         r.update({"offered_load": load, "offered_gcups": load * peak_gcups,
-                  "requests_per_s": rate, "batches": int(st.batches),
-                  "mean_pairs_per_batch": float(st.pairs) / max(1, int(st.batches)),
+                  "requests_per_s": rate, "batches": nb,
+                  "mean_pairs_per_batch": float(b1.pairs - b0.pairs) / max(1, nb),
                   "fraction_of_peak": r["gcups"] / peak_gcups})
         out.append(r)
     return out
