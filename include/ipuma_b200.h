@@ -125,6 +125,9 @@ typedef struct ipuma_stats {
   int32_t timed_kind[10];   /* IPUMA_KERNEL_* */
   double timed_ms[10];
   int64_t timed_cells[10];
+  /* ipuma_gpu_compare: chunks the batch was split into for upload/compute
+   * overlap (1 = one upload, then the kernels). */
+  int32_t chunks;
 } ipuma_stats;
 
 /* Kernel kinds reported in ipuma_stats.timed_kind.  S16_L<lanes>_K<k>:
@@ -175,7 +178,11 @@ void ipuma_gpu_destroy(ipuma_engine* e);
  *   "autotune"    1 = measure the kernel-class rates before the first batch
  *                 (default), 0 = built-in rates unless ipuma_gpu_autotune
  *   "long_a"      |A| above which a pair takes the widest s16x2 class
- *                 (default 3072): long pairs are latency-bound */
+ *                 (default 3072): long pairs are latency-bound
+ *   "chunks"      ipuma_gpu_compare only: 0 = split large batches into up
+ *                 to 8 chunks whose uploads overlap the alignment of the
+ *                 previous chunks (default), 1 = upload everything first,
+ *                 n = exactly n chunks (at most 8) */
 int ipuma_gpu_set_option(ipuma_engine* e, const char* name, int64_t value);
 
 /* Runs one batch in the reference wire format and waits for it.
@@ -196,7 +203,11 @@ int ipuma_gpu_poll(ipuma_engine* e, uint64_t job, int32_t* done);
 /* Waits for a job (bounded by timeout_ms; < 0 waits without limit). */
 int ipuma_gpu_join(ipuma_engine* e, uint64_t job, int64_t timeout_ms);
 
-/* Aligns n pairs from host memory; results in input order. */
+/* Aligns n pairs from host memory; results in input order.  Large batches
+ * are split into chunks of consecutive pairs: each chunk uploads the byte
+ * ranges of `codes` its pairs read (the span of its A offsets and the span
+ * of its B offsets) while earlier chunks compute, so the copy overlaps the
+ * kernels when sequences are stored in pair order. */
 int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes,
                       const ipuma_pair* pairs, int32_t n, int32_t* score, int32_t* arange,
                       int32_t* brange);

@@ -101,6 +101,10 @@ constexpr ClassDef kClasses[kNumS16 + 1] = {
 };
 constexpr int kClsS32 = kNumS16;
 constexpr int kWarpsPerBlock = 4;
+// Chunked upload/compute overlap of ipuma_gpu_compare.
+constexpr int kMaxChunks = 8;
+constexpr int kChunkMinPairs = 65536;         // automatic chunks hold at least this many pairs
+constexpr size_t kChunkMinBytes = 32u << 20;  // and the batch uploads at least this much
 constexpr int kThreads = 32 * kWarpsPerBlock;
 
 struct Job {
@@ -145,6 +149,13 @@ struct ipuma_engine {
   int timed_cls[10] = {};
 
   DevBuf d_sim, d_codes, d_pairs, d_list, d_res, d_scratch, d_cf, d_ovf, d_ctl, d_inputs, d_wres, d_flag;
+  // Second buffer set and streams of the chunked host-to-host path
+  // (ipuma_gpu_compare): chunks alternate between `stream` and `stream2`
+  // while `copy_stream` uploads the next chunks.
+  DevBuf x_list, x_scratch, x_ovf, x_flag;
+  cudaStream_t stream2 = nullptr, copy_stream = nullptr;
+  cudaEvent_t cev[2 * kMaxChunks + 2] = {};
+  int chunks = 0;  // option "chunks": 0 automatic, 1 off, n fixed
   std::map<const void*, std::pair<int, int>> grid_cache;  // kernel -> {smem, grid}
   // Captured pipelines of compare_device, by shape and buffers (option "graphs").
   std::map<std::vector<uint64_t>, cudaGraphExec_t> graphs_cache;
@@ -228,6 +239,22 @@ int max_batched_groups(ipuma_engine* e) {
   return g * kWarpsPerBlock;
 }
 
+// Device buffers of one run of the batched pipeline: the control block and
+// the per-run work lists and strip scratch.  Two runs may execute at once
+// (on two streams) only with disjoint sets.
+struct RunBufs {
+  int* ctl;  // CTL_INTS ints, cleared before the run
+  DevBuf* scratch;
+  DevBuf* list;
+  DevBuf* ovf;
+  DevBuf* flag;
+};
+
+// The engine's default set (control block at the start of d_ctl).
+RunBufs main_bufs(ipuma_engine* e) {
+  return RunBufs{e->d_ctl.as<int>(), &e->d_scratch, &e->d_list, &e->d_ovf, &e->d_flag};
+}
+
 // Brackets one alignment-kernel launch with events when time_launches is set.
 int timed_begin(ipuma_engine* e, cudaStream_t s, int kind, int cls) {
   if (!e->time_launches || e->n_timed >= 10) return IPUMA_OK;
@@ -249,18 +276,18 @@ int timed_end(ipuma_engine* e, cudaStream_t s) {
 }
 
 template <class T, int K, int LANES>
-int launch_batched(ipuma_engine* e, cudaStream_t s, const uint8_t* codes, const PairDesc* pairs,
-                   const int* list, const int* range, int* head, long rowsCap, int* score,
-                   int* arange, int* brange, int kind, int cls) {
+int launch_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_t* codes,
+                   const PairDesc* pairs, const int* list, const int* range, int* head, long rowsCap,
+                   int* score, int* arange, int* brange, int kind, int cls) {
   const int smem = smem_for<T, K, LANES>(e);
   const int grid = batched_grid<T, K, LANES>(e);
-  int* ctl = e->d_ctl.as<int>();
+  int* ctl = rb.ctl;
   auto* cells = reinterpret_cast<unsigned long long*>(ctl + CTL_CELLS);
   int rc;
   if ((rc = timed_begin(e, s, kind, cls))) return rc;
   k_batched<T, K, LANES><<<grid, kThreads, smem, s>>>(
-      e->sc, e->d_sim.as<int8_t>(), codes, pairs, list, range, head, e->d_scratch.as<int2>(),
-      rowsCap, score, arange, brange, e->d_ovf.as<int>(), cells + CELLS_RERUN,
+      e->sc, e->d_sim.as<int8_t>(), codes, pairs, list, range, head, rb.scratch->as<int2>(),
+      rowsCap, score, arange, brange, rb.ovf->as<int>(), cells + CELLS_RERUN,
       reinterpret_cast<DevStatus*>(ctl + CTL_STATUS));
   CUDA_TRY(cudaGetLastError());
   return timed_end(e, s);
@@ -268,25 +295,31 @@ int launch_batched(ipuma_engine* e, cudaStream_t s, const uint8_t* codes, const 
 
 // Grows every buffer run_batched uses for a batch of this shape, so that
 // the pipeline itself allocates nothing (graph capture).
-int reserve_batched(ipuma_engine* e, cudaStream_t s, int n, int maxA, int maxB) {
+int reserve_bufs(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, int n, int maxB) {
   int rc;
   const long rowsCap = std::max(1, maxB);
-  if ((rc = e->d_ctl.ensure(sizeof(int) * CTL_INTS, s))) return rc;
-  if ((rc = e->d_scratch.ensure(sizeof(int2) * 2 * rowsCap * max_batched_groups(e), s))) return rc;
-  if ((rc = e->d_list.ensure(sizeof(int) * (size_t)n + 64, s))) return rc;
-  if ((rc = e->d_ovf.ensure(sizeof(int) * (size_t)n + 64, s))) return rc;
-  if ((rc = e->d_flag.ensure((size_t)n + 64, s))) return rc;
-  (void)maxA;
+  if ((rc = rb.scratch->ensure(sizeof(int2) * 2 * rowsCap * max_batched_groups(e), s))) return rc;
+  if ((rc = rb.list->ensure(sizeof(int) * (size_t)n + 64, s))) return rc;
+  if ((rc = rb.ovf->ensure(sizeof(int) * (size_t)n + 64, s))) return rc;
+  if ((rc = rb.flag->ensure((size_t)n + 64, s))) return rc;
   return IPUMA_OK;
+}
+
+int reserve_batched(ipuma_engine* e, cudaStream_t s, int n, int maxA, int maxB) {
+  int rc;
+  if ((rc = e->d_ctl.ensure(sizeof(int) * CTL_INTS, s))) return rc;
+  (void)maxA;
+  return reserve_bufs(e, main_bufs(e), s, n, maxB);
 }
 
 // Runs the persistent cost-binned pipeline over n device-resident pairs.
 // Results land at score[p], arange[p], brange[p].
-int run_batched(ipuma_engine* e, cudaStream_t s, const uint8_t* codes, const PairDesc* pairs, int n,
-                int maxA, int maxB, int* score, int* arange, int* brange, int* launches) {
+int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_t* codes,
+                const PairDesc* pairs, int n, int maxA, int maxB, int* score, int* arange, int* brange,
+                int* launches) {
   int rc;
   if (n <= 0) return IPUMA_OK;
-  int* ctl = e->d_ctl.as<int>();
+  int* ctl = rb.ctl;
   DevStatus* st = reinterpret_cast<DevStatus*>(ctl + CTL_STATUS);
 
   if (!e->fast_ok) {
@@ -308,9 +341,9 @@ int run_batched(ipuma_engine* e, cudaStream_t s, const uint8_t* codes, const Pai
   // Scratch for strip boundaries and the lists.
   const long rowsCap = std::max(1, maxB);
   const long groups = max_batched_groups(e);
-  if ((rc = e->d_scratch.ensure(sizeof(int2) * 2 * rowsCap * groups, s))) return rc;
-  if ((rc = e->d_list.ensure(sizeof(int) * (size_t)n + 64, s))) return rc;
-  if ((rc = e->d_ovf.ensure(sizeof(int) * (size_t)n + 64, s))) return rc;
+  if ((rc = rb.scratch->ensure(sizeof(int2) * 2 * rowsCap * groups, s))) return rc;
+  if ((rc = rb.list->ensure(sizeof(int) * (size_t)n + 64, s))) return rc;
+  if ((rc = rb.ovf->ensure(sizeof(int) * (size_t)n + 64, s))) return rc;
 
   BinParams bp{};
   bp.n_s16_classes = kNumS16;
@@ -333,27 +366,27 @@ int run_batched(ipuma_engine* e, cudaStream_t s, const uint8_t* codes, const Pai
   bp.max_b = maxB;
   bp.M = e->M;
   bp.s16_limit = e->sc.s16Limit;
-  if ((rc = e->d_flag.ensure((size_t)n + 64, s))) return rc;
+  if ((rc = rb.flag->ensure((size_t)n + 64, s))) return rc;
   const int nkeys = bp.nclass * NBUCKET;
   const int tb = 256;
   const int gb = std::min<int>((n + tb - 1) / tb, e->nsm * 8);
   k_bin_count<<<gb, tb, 0, s>>>(bp, codes, e->d_sim.as<int8_t>(), pairs, n, ctl + CTL_HIST,
-                                e->d_flag.as<uint8_t>(),
+                                rb.flag->as<uint8_t>(),
                                 reinterpret_cast<unsigned long long*>(ctl + CTL_CELLS), st, score,
                                 arange, brange);
   k_bin_scan<<<1, 1024, 0, s>>>(nkeys, ctl + CTL_HIST, ctl + CTL_OFFS, ctl + CTL_RANGES);
-  k_bin_scatter<<<gb, tb, 0, s>>>(bp, pairs, n, e->d_flag.as<uint8_t>(), ctl + CTL_OFFS,
-                                  e->d_list.as<int>());
+  k_bin_scatter<<<gb, tb, 0, s>>>(bp, pairs, n, rb.flag->as<uint8_t>(), ctl + CTL_OFFS,
+                                  rb.list->as<int>());
   CUDA_TRY(cudaGetLastError());
   *launches += 3;
 
-  int* list = e->d_list.as<int>();
+  int* list = rb.list->as<int>();
   int* heads = ctl + CTL_HEADS;
   // Long-tail first: the s32 class holds the longest high-scoring pairs,
   // then the s16x2 classes from the widest down.
   const int* R = ctl + CTL_RANGES;
 #define IPUMA_LAUNCH(T, K, L, cls)                                                              \
-  if ((rc = launch_batched<T, K, L>(e, s, codes, pairs, list, R + 2 * (cls), heads + (cls), rowsCap, \
+  if ((rc = launch_batched<T, K, L>(e, rb, s, codes, pairs, list, R + 2 * (cls), heads + (cls), rowsCap, \
                                     score, arange, brange, kClasses[cls].kind, cls)))          \
     return rc;
   IPUMA_LAUNCH(LaneS32, 16, 32, 6)
@@ -365,7 +398,7 @@ int run_batched(ipuma_engine* e, cudaStream_t s, const uint8_t* codes, const Pai
   IPUMA_LAUNCH(LaneS16x2, 4, 16, 0)
 #undef IPUMA_LAUNCH
   // Exact 32-bit rerun of the s16x2 pairs whose score may have overflowed.
-  if ((rc = launch_batched<LaneS32, 16, 32>(e, s, codes, pairs, e->d_ovf.as<int>(), ctl + CTL_STATUS + 1,
+  if ((rc = launch_batched<LaneS32, 16, 32>(e, rb, s, codes, pairs, rb.ovf->as<int>(), ctl + CTL_STATUS + 1,
                                             heads + 7, rowsCap, score, arange, brange,
                                             IPUMA_KERNEL_S32_RERUN, CELLS_RERUN)))
     return rc;
@@ -382,12 +415,26 @@ int reset_ctl(ipuma_engine* e, cudaStream_t s) {
   return IPUMA_OK;
 }
 
-int check_status(ipuma_engine* e, cudaStream_t s) {
+// Waits for the stream and reads the status of the call's runs: `nblk`
+// consecutive control blocks at the start of d_ctl (one per run; errors,
+// overflow reruns and per-class cells are summed).
+int check_status(ipuma_engine* e, cudaStream_t s, int nblk = 1) {
   DevStatus st{};
   unsigned long long cells[NCLASS_MAX + 2] = {};
-  CUDA_TRY(cudaMemcpyAsync(&st, e->d_ctl.as<int>() + CTL_STATUS, sizeof(st), cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaMemcpyAsync(cells, e->d_ctl.as<int>() + CTL_CELLS, sizeof(cells), cudaMemcpyDeviceToHost, s));
+  DevStatus stk[kMaxChunks];
+  unsigned long long cellsk[kMaxChunks][NCLASS_MAX + 2];
+  nblk = std::max(1, std::min(nblk, kMaxChunks));
+  for (int k = 0; k < nblk; ++k) {
+    const int* ctl = e->d_ctl.as<int>() + (size_t)k * CTL_INTS;
+    CUDA_TRY(cudaMemcpyAsync(&stk[k], ctl + CTL_STATUS, sizeof(DevStatus), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(cellsk[k], ctl + CTL_CELLS, sizeof(cellsk[k]), cudaMemcpyDeviceToHost, s));
+  }
   CUDA_TRY(cudaStreamSynchronize(s));
+  for (int k = 0; k < nblk; ++k) {
+    if (!st.error) st.error = stk[k].error;
+    st.overflow_count += stk[k].overflow_count;
+    for (int c = 0; c < NCLASS_MAX + 2; ++c) cells[c] += cellsk[k][c];
+  }
   e->stats.overflow_reruns = st.overflow_count;
   e->stats.n_timed = e->n_timed;
   for (int k = 0; k < e->n_timed; ++k) {
@@ -555,7 +602,7 @@ int time_class(ipuma_engine* e, int cls, int n, int alen, int blen, const DevBuf
   for (int rep = 0; rep < 2 && rc == IPUMA_OK; ++rep) {
     int launches = 0;
     if ((rc = reset_ctl(e, s))) break;
-    if ((rc = run_batched(e, s, e->d_codes.as<uint8_t>(), e->d_pairs.as<PairDesc>(), n, alen, blen, out, out + n,
+    if ((rc = run_batched(e, main_bufs(e), s, e->d_codes.as<uint8_t>(), e->d_pairs.as<PairDesc>(), n, alen, blen, out, out + n,
                           out + 2 * n, &launches)))
       break;
     if ((rc = check_status(e, s))) break;
@@ -643,6 +690,54 @@ int maybe_autotune(ipuma_engine* e) {
   if (e->tuned || !e->autotune) return IPUMA_OK;
   const char* path = getenv("IPUMA_TUNE_CACHE");
   return run_autotune(e, path);
+}
+
+// Byte ranges of the code array one chunk of pairs reads: its A range and
+// its B range (empty pairs read nothing).
+struct ChunkSpan {
+  size_t lo[2] = {SIZE_MAX, SIZE_MAX};
+  size_t hi[2] = {0, 0};
+};
+
+// Adds [lo, hi) to the sorted disjoint list `have` and appends the parts
+// that were missing to `todo`.
+void take_range(std::vector<std::pair<size_t, size_t>>& have, size_t lo, size_t hi,
+                std::vector<std::pair<size_t, size_t>>& todo) {
+  if (lo >= hi) return;
+  size_t cur = lo;
+  for (const auto& r : have) {
+    if (r.second <= cur) continue;
+    if (r.first >= hi) break;
+    if (r.first > cur) todo.emplace_back(cur, r.first);
+    cur = std::max(cur, r.second);
+    if (cur >= hi) break;
+  }
+  if (cur < hi) todo.emplace_back(cur, hi);
+  have.emplace_back(lo, hi);
+  std::sort(have.begin(), have.end());
+  std::vector<std::pair<size_t, size_t>> merged;
+  for (const auto& r : have) {
+    if (!merged.empty() && r.first <= merged.back().second)
+      merged.back().second = std::max(merged.back().second, r.second);
+    else
+      merged.push_back(r);
+  }
+  have.swap(merged);
+}
+
+int chunk_count(const ipuma_engine* e, int32_t n, size_t n_codes) {
+  if (e->chunks > 0) return std::min<int>(std::min(e->chunks, kMaxChunks), std::max(1, n));
+  if (n < 2 * kChunkMinPairs || n_codes < kChunkMinBytes) return 1;
+  return std::min(kMaxChunks, n / kChunkMinPairs);
+}
+
+bool is_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
 }
 
 }  // namespace
@@ -769,9 +864,16 @@ void ipuma_gpu_destroy(ipuma_engine* e) {
   if (e->stream) cudaStreamSynchronize(e->stream);
   for (auto& kv : e->jobs)
     if (kv.second.done) cudaEventDestroy(kv.second.done);
+  if (e->stream2) cudaStreamSynchronize(e->stream2);
+  if (e->copy_stream) cudaStreamSynchronize(e->copy_stream);
   for (auto* b : {&e->d_sim, &e->d_codes, &e->d_pairs, &e->d_list, &e->d_res, &e->d_scratch, &e->d_cf,
-                  &e->d_ovf, &e->d_ctl, &e->d_inputs, &e->d_wres, &e->d_flag})
+                  &e->d_ovf, &e->d_ctl, &e->d_inputs, &e->d_wres, &e->d_flag, &e->x_list, &e->x_scratch,
+                  &e->x_ovf, &e->x_flag})
     b->release();
+  for (auto& ev : e->cev)
+    if (ev) cudaEventDestroy(ev);
+  if (e->stream2) cudaStreamDestroy(e->stream2);
+  if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
   for (auto& ev : e->ev)
     if (ev) cudaEventDestroy(ev);
   for (auto& ev : e->tev)
@@ -797,6 +899,10 @@ int ipuma_gpu_set_option(ipuma_engine* e, const char* name, int64_t value) {
     e->autotune = value ? 1 : 0;
   } else if (k == "time_launches") {
     e->time_launches = value ? 1 : 0;
+  } else if (k == "chunks") {
+    if (value < 0 || value > kMaxChunks)
+      return fail(IPUMA_ERR_INVALID_ARG, "chunks must be 0 (automatic) .. %d", kMaxChunks);
+    e->chunks = (int)value;
   } else if (k == "tile_k") {
     if (value < 0 || value > kNumS16)
       return fail(IPUMA_ERR_INVALID_ARG, "tile_k must be 0 (automatic) or a kernel class 1..%d", kNumS16);
@@ -884,7 +990,7 @@ int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_c
       CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       int crc = reset_ctl(e, s);
       if (!crc)
-        crc = run_batched(e, s, d_codes, reinterpret_cast<const PairDesc*>(d_pairs), n, max_a_len, max_b_len,
+        crc = run_batched(e, main_bufs(e), s, d_codes, reinterpret_cast<const PairDesc*>(d_pairs), n, max_a_len, max_b_len,
                           d_score, d_arange, d_brange, &launches);
       cudaError_t ce = cudaStreamEndCapture(s, &g);
       if (crc) {
@@ -906,7 +1012,7 @@ int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_c
   } else {
     if ((rc = reset_ctl(e, s))) return rc;
     CUDA_TRY(cudaEventRecord(e->ev[1], s));
-    rc = run_batched(e, s, d_codes, reinterpret_cast<const PairDesc*>(d_pairs), n, max_a_len,
+    rc = run_batched(e, main_bufs(e), s, d_codes, reinterpret_cast<const PairDesc*>(d_pairs), n, max_a_len,
                      max_b_len, d_score, d_arange, d_brange, &launches);
     if (rc) return rc;
   }
@@ -927,21 +1033,34 @@ int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes, con
   if (n < 0) return fail(IPUMA_ERR_INVALID_ARG, "negative pair count");
   if (n == 0) return IPUMA_OK;
   if (!codes || !pairs || !score || !arange || !brange) return fail(IPUMA_ERR_INVALID_ARG, "null buffer");
-  // Host-side bounds check of every pair (the kernels trust the descriptors).
+  std::lock_guard<std::mutex> lk(e->mu);
+  const int nch = e->time_launches ? 1 : chunk_count(e, n, n_codes);
+  // Host-side bounds check of every pair (the kernels trust the
+  // descriptors), with the code ranges each chunk of pairs reads.
   int maxA = 0, maxB = 0;
   int64_t cells = 0;
-  for (int32_t p = 0; p < n; ++p) {
-    const ipuma_pair& d = pairs[p];
-    if (d.a_len < 0 || d.b_len < 0 || d.a_off < 0 || d.b_off < 0 ||
-        (size_t)d.a_off + (size_t)d.a_len > n_codes || (size_t)d.b_off + (size_t)d.b_len > n_codes)
-      return fail(IPUMA_ERR_INVALID_ARG, "pair %d lies outside the code array", p);
-    maxA = std::max(maxA, d.a_len);
-    maxB = std::max(maxB, d.b_len);
-    cells += (int64_t)d.a_len * d.b_len;
+  ChunkSpan span[kMaxChunks];
+  int32_t cbeg[kMaxChunks + 1];
+  for (int k = 0; k <= nch; ++k) cbeg[k] = (int32_t)((int64_t)n * k / nch);
+  for (int k = 0; k < nch; ++k) {
+    ChunkSpan& sp = span[k];
+    for (int32_t p = cbeg[k]; p < cbeg[k + 1]; ++p) {
+      const ipuma_pair& d = pairs[p];
+      if (d.a_len < 0 || d.b_len < 0 || d.a_off < 0 || d.b_off < 0 ||
+          (size_t)d.a_off + (size_t)d.a_len > n_codes || (size_t)d.b_off + (size_t)d.b_len > n_codes)
+        return fail(IPUMA_ERR_INVALID_ARG, "pair %d lies outside the code array", p);
+      maxA = std::max(maxA, d.a_len);
+      maxB = std::max(maxB, d.b_len);
+      cells += (int64_t)d.a_len * d.b_len;
+      if (d.a_len == 0 || d.b_len == 0) continue;
+      sp.lo[0] = std::min(sp.lo[0], (size_t)d.a_off);
+      sp.hi[0] = std::max(sp.hi[0], (size_t)d.a_off + (size_t)d.a_len);
+      sp.lo[1] = std::min(sp.lo[1], (size_t)d.b_off);
+      sp.hi[1] = std::max(sp.hi[1], (size_t)d.b_off + (size_t)d.b_len);
+    }
   }
   if (maxA > 65535 || maxB > 65535)
     return fail(IPUMA_ERR_TOO_LONG, "sequence longer than 65535 (ranges are uint16)");
-  std::lock_guard<std::mutex> lk(e->mu);
   CUDA_TRY(cudaSetDevice(e->device));
   cudaStream_t s = e->stream;
   int rc;
@@ -951,23 +1070,85 @@ int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes, con
   if ((rc = e->d_res.ensure(sizeof(int32_t) * 3 * (size_t)n, s))) return rc;
   e->stats = ipuma_stats{};
   int launches = 0;
-  if ((rc = reset_ctl(e, s))) return rc;
-  CUDA_TRY(cudaEventRecord(e->ev[0], s));
-  CUDA_TRY(cudaMemcpyAsync(e->d_codes.p, codes, n_codes, cudaMemcpyHostToDevice, s));
-  CUDA_TRY(cudaMemcpyAsync(e->d_pairs.p, pairs, sizeof(ipuma_pair) * (size_t)n, cudaMemcpyHostToDevice, s));
   int32_t* d_score = e->d_res.as<int32_t>();
   int32_t* d_ar = d_score + n;
   int32_t* d_br = d_ar + n;
-  CUDA_TRY(cudaEventRecord(e->ev[1], s));
-  rc = run_batched(e, s, e->d_codes.as<uint8_t>(), e->d_pairs.as<PairDesc>(), n, maxA, maxB, d_score,
-                   d_ar, d_br, &launches);
-  if (rc) return rc;
-  CUDA_TRY(cudaEventRecord(e->ev[2], s));
-  CUDA_TRY(cudaMemcpyAsync(score, d_score, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaMemcpyAsync(arange, d_ar, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaMemcpyAsync(brange, d_br, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaEventRecord(e->ev[3], s));
-  if ((rc = check_status(e, s))) return rc;
+  if (nch == 1) {
+    if ((rc = reset_ctl(e, s))) return rc;
+    CUDA_TRY(cudaEventRecord(e->ev[0], s));
+    CUDA_TRY(cudaMemcpyAsync(e->d_codes.p, codes, n_codes, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(e->d_pairs.p, pairs, sizeof(ipuma_pair) * (size_t)n, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaEventRecord(e->ev[1], s));
+    rc = run_batched(e, main_bufs(e), s, e->d_codes.as<uint8_t>(), e->d_pairs.as<PairDesc>(), n, maxA, maxB,
+                     d_score, d_ar, d_br, &launches);
+    if (rc) return rc;
+    CUDA_TRY(cudaEventRecord(e->ev[2], s));
+    CUDA_TRY(cudaMemcpyAsync(score, d_score, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(arange, d_ar, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(brange, d_br, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaEventRecord(e->ev[3], s));
+    if ((rc = check_status(e, s))) return rc;
+  } else {
+    // Chunked: chunk k's code ranges and descriptors go up on copy_stream
+    // while earlier chunks run; runs alternate between two streams with
+    // their own buffer sets, so one chunk's launches fill the tail of the
+    // previous one's.  Results come back per chunk when the host buffers
+    // are pinned (pageable copies would block the issuing thread), else
+    // once at the end.
+    if (!e->stream2) CUDA_TRY(cudaStreamCreateWithFlags(&e->stream2, cudaStreamNonBlocking));
+    if (!e->copy_stream) CUDA_TRY(cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking));
+    for (auto& ev : e->cev)
+      if (!ev) CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    int nmax = 0;
+    for (int k = 0; k < nch; ++k) nmax = std::max(nmax, cbeg[k + 1] - cbeg[k]);
+    const RunBufs rb1{nullptr, &e->x_scratch, &e->x_list, &e->x_ovf, &e->x_flag};
+    if ((rc = e->d_ctl.ensure(sizeof(int) * CTL_INTS * (size_t)nch, s))) return rc;
+    if ((rc = reserve_bufs(e, main_bufs(e), s, nmax, maxB))) return rc;
+    if ((rc = reserve_bufs(e, rb1, s, nmax, maxB))) return rc;
+    const bool pinned_out = is_pinned(score) && is_pinned(arange) && is_pinned(brange);
+    cudaStream_t run_s[2] = {s, e->stream2};
+    CUDA_TRY(cudaEventRecord(e->ev[0], s));
+    CUDA_TRY(cudaMemsetAsync(e->d_ctl.p, 0, sizeof(int) * CTL_INTS * (size_t)nch, s));
+    e->n_timed = 0;
+    CUDA_TRY(cudaEventRecord(e->ev[1], s));
+    CUDA_TRY(cudaStreamWaitEvent(e->stream2, e->ev[1], 0));
+    CUDA_TRY(cudaStreamWaitEvent(e->copy_stream, e->ev[1], 0));
+    std::vector<std::pair<size_t, size_t>> have, todo;
+    for (int k = 0; k < nch; ++k) {
+      const int32_t off = cbeg[k], nk = cbeg[k + 1] - cbeg[k];
+      todo.clear();
+      for (int r = 0; r < 2; ++r)
+        if (span[k].lo[r] < span[k].hi[r]) take_range(have, span[k].lo[r], span[k].hi[r], todo);
+      for (const auto& r : todo)
+        CUDA_TRY(cudaMemcpyAsync(e->d_codes.as<uint8_t>() + r.first, codes + r.first, r.second - r.first,
+                                 cudaMemcpyHostToDevice, e->copy_stream));
+      CUDA_TRY(cudaMemcpyAsync(e->d_pairs.as<ipuma_pair>() + off, pairs + off, sizeof(ipuma_pair) * (size_t)nk,
+                               cudaMemcpyHostToDevice, e->copy_stream));
+      CUDA_TRY(cudaEventRecord(e->cev[k], e->copy_stream));
+      cudaStream_t rs = run_s[k & 1];
+      CUDA_TRY(cudaStreamWaitEvent(rs, e->cev[k], 0));
+      RunBufs rb = (k & 1) ? rb1 : main_bufs(e);
+      rb.ctl = e->d_ctl.as<int>() + (size_t)k * CTL_INTS;
+      if ((rc = run_batched(e, rb, rs, e->d_codes.as<uint8_t>(), e->d_pairs.as<PairDesc>() + off, nk, maxA, maxB,
+                            d_score + off, d_ar + off, d_br + off, &launches)))
+        return rc;
+      if (pinned_out) {
+        CUDA_TRY(cudaMemcpyAsync(score + off, d_score + off, sizeof(int32_t) * nk, cudaMemcpyDeviceToHost, rs));
+        CUDA_TRY(cudaMemcpyAsync(arange + off, d_ar + off, sizeof(int32_t) * nk, cudaMemcpyDeviceToHost, rs));
+        CUDA_TRY(cudaMemcpyAsync(brange + off, d_br + off, sizeof(int32_t) * nk, cudaMemcpyDeviceToHost, rs));
+      }
+    }
+    CUDA_TRY(cudaEventRecord(e->cev[kMaxChunks], e->stream2));
+    CUDA_TRY(cudaStreamWaitEvent(s, e->cev[kMaxChunks], 0));
+    CUDA_TRY(cudaEventRecord(e->ev[2], s));
+    if (!pinned_out) {
+      CUDA_TRY(cudaMemcpyAsync(score, d_score, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+      CUDA_TRY(cudaMemcpyAsync(arange, d_ar, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+      CUDA_TRY(cudaMemcpyAsync(brange, d_br, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+    }
+    CUDA_TRY(cudaEventRecord(e->ev[3], s));
+    if ((rc = check_status(e, s, nch))) return rc;
+  }
   float kms = 0, tms = 0;
   cudaEventElapsedTime(&kms, e->ev[1], e->ev[2]);
   cudaEventElapsedTime(&tms, e->ev[0], e->ev[3]);
@@ -976,6 +1157,7 @@ int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes, con
   e->stats.cells = cells;
   e->stats.pairs = n;
   e->stats.launches = launches;
+  e->stats.chunks = nch;
   return IPUMA_OK;
 }
 
@@ -999,7 +1181,7 @@ static int launch_wire(ipuma_engine* e, cudaStream_t s, const int* d_in, int* d_
                                      e->d_pairs.as<PairDesc>());
   CUDA_TRY(cudaGetLastError());
   *launches += 1;
-  return run_batched(e, s, reinterpret_cast<const uint8_t*>(d_in), e->d_pairs.as<PairDesc>(),
+  return run_batched(e, main_bufs(e), s, reinterpret_cast<const uint8_t*>(d_in), e->d_pairs.as<PairDesc>(),
                      (int)totalSlots, maxA, maxB, d_res, d_res + totalSlots, d_res + 2 * totalSlots, launches);
 }
 

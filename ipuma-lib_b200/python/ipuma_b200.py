@@ -81,7 +81,8 @@ class Stats(ctypes.Structure):
                 ("s32_pairs", ctypes.c_int64), ("overflow_reruns", ctypes.c_int64),
                 ("launches", ctypes.c_int32), ("used_graph", ctypes.c_int32),
                 ("n_timed", ctypes.c_int32), ("timed_kind", ctypes.c_int32 * 10),
-                ("timed_ms", ctypes.c_double * 10), ("timed_cells", ctypes.c_int64 * 10)]
+                ("timed_ms", ctypes.c_double * 10), ("timed_cells", ctypes.c_int64 * 10),
+                ("chunks", ctypes.c_int32)]
 
 
 class ServerConfig(ctypes.Structure):
