@@ -143,6 +143,7 @@ typedef struct ipuma_stats {
 #define IPUMA_KERNEL_S32_RERUN 7   /* s32 rerun of s16x2 give-ups           */
 #define IPUMA_KERNEL_PLAIN 8       /* one-launch-per-batch wire kernel      */
 #define IPUMA_KERNEL_EXACT 9       /* per-thread exact kernel               */
+#define IPUMA_KERNEL_S16_T_K16 10  /* s16x2, one thread per two pairs, 16-column strips */
 
 typedef struct ipuma_engine ipuma_engine;
 
@@ -173,7 +174,16 @@ void ipuma_gpu_destroy(ipuma_engine* e);
  *                 one-launch-per-batch kernel (wire-buffer API only)
  *   "graphs"      1 = capture and replay CUDA graphs for repeated shapes
  *   "tile_k"      0 = kernel class by |A| (default); 1..6 = every pair
- *                 through s16x2 class IPUMA_KERNEL_S16_* (value = kind)
+ *                 through s16x2 class IPUMA_KERNEL_S16_* (value = kind),
+ *                 7 = every pair through IPUMA_KERNEL_S16_T_K16
+ *   "concurrent"  2 = class launches alternate between two streams, so
+ *                 each starts on the SMs the previous one frees (default);
+ *                 1 = all classes at once, each on a share of the SMs
+ *                 proportional to its modelled work; 0 = one launch after
+ *                 the other (always the case with time_launches)
+ *   "thread_class" 1 = the per-thread class IPUMA_KERNEL_S16_T_K16 may be
+ *                 chosen for pairs that are small relative to the batch,
+ *                 0 = never (default) unless tile_k forces it
  *   "time_launches" 1 = time every alignment-kernel launch (ipuma_stats)
  *   "autotune"    1 = measure the kernel-class rates before the first batch
  *                 (default), 0 = built-in rates unless ipuma_gpu_autotune

@@ -21,6 +21,7 @@
 #include "errors.h"
 #include "ipuma_b200.h"
 #include "sw_kernels.cuh"
+#include "sw_thread.cuh"
 #include "../host/swatlib/encoding.h"
 #include "../host/swatlib/similarity.h"
 
@@ -89,17 +90,31 @@ struct DevBuf {
 // Kernel classes of the batched pipeline.  s16x2 classes by |A| (columns
 // per strip = lanes * K), then the s32 class; the rerun reuses the s32
 // kernel.
+// lanes = lanes per pair group (0: the per-thread class, no wavefront),
+// k = columns per lane, width = columns per strip.
 struct ClassDef {
-  int lanes, k, kind;
+  int lanes, k, kind, width;
 };
-constexpr int kNumS16 = 6;
+constexpr int kNumS16 = 7;
 constexpr ClassDef kClasses[kNumS16 + 1] = {
-    {16, 4, IPUMA_KERNEL_S16_L16_K4},   {16, 8, IPUMA_KERNEL_S16_L16_K8},
-    {16, 12, IPUMA_KERNEL_S16_L16_K12}, {16, 16, IPUMA_KERNEL_S16_L16_K16},
-    {32, 12, IPUMA_KERNEL_S16_L32_K12}, {32, 16, IPUMA_KERNEL_S16_L32_K16},
-    {32, 16, IPUMA_KERNEL_S32_K16},
+    {16, 4, IPUMA_KERNEL_S16_L16_K4, 64},    {16, 8, IPUMA_KERNEL_S16_L16_K8, 128},
+    {16, 12, IPUMA_KERNEL_S16_L16_K12, 192}, {16, 16, IPUMA_KERNEL_S16_L16_K16, 256},
+    {32, 12, IPUMA_KERNEL_S16_L32_K12, 384}, {32, 16, IPUMA_KERNEL_S16_L32_K16, 512},
+    {0, 16, IPUMA_KERNEL_S16_T_K16, 16},     {32, 16, IPUMA_KERNEL_S32_K16, 512},
 };
+constexpr int kClsWidest = 5;  // widest wavefront class (very long |A|)
+constexpr int kClsThread = 6;  // per-thread class k_thread<16>
 constexpr int kClsS32 = kNumS16;
+// Per-thread class: rows it accepts (its boundary scratch is rows x threads)
+// and the share of the batch's time one of its pairs may take.
+constexpr int kThrMaxRows = 2048;
+constexpr float kThrLatencyShare = 0.5f;
+// Latency bound of every class (BinParams::lat_share): an item may take at
+// most this share of the batch's modelled time (cells x fastest slot time
+// / packing efficiency), for batches of at least 1 ms.
+constexpr float kLatencyShare = 0.25f;
+constexpr float kPackingEfficiency = 0.85f;
+constexpr float kLatencyMinBatchPs = 1.0e9f;
 constexpr int kWarpsPerBlock = 4;
 // Chunked upload/compute overlap of ipuma_gpu_compare.
 constexpr int kMaxChunks = 8;
@@ -133,6 +148,10 @@ struct ipuma_engine {
   int graphs = 0;
   int tile_k = 0;
   int time_launches = 0;
+  // option "thread_class": the per-thread class may be chosen.  Off by
+  // default: on the benchmark batches its divergence between pairs of
+  // different lengths made it slower than the wavefront classes.
+  int thread_class = 0;
 
   // autotuned per-class rates of the class choice (BinParams)
   float slot_ps[NCLASS_MAX] = {};
@@ -153,6 +172,12 @@ struct ipuma_engine {
   // (ipuma_gpu_compare): chunks alternate between `stream` and `stream2`
   // while `copy_stream` uploads the next chunks.
   DevBuf x_list, x_scratch, x_ovf, x_flag;
+  // One stream per kernel class: the class launches of a batch run
+  // concurrently, each on its share of the SMs (option "concurrent").
+  cudaStream_t cls_stream[NCLASS_MAX] = {};
+  cudaEvent_t fork_ev = nullptr;
+  cudaEvent_t join_ev[NCLASS_MAX] = {};
+  int concurrent = 2;
   cudaStream_t stream2 = nullptr, copy_stream = nullptr;
   cudaEvent_t cev[2 * kMaxChunks + 2] = {};
   int chunks = 0;  // option "chunks": 0 automatic, 1 off, n fixed
@@ -175,13 +200,18 @@ constexpr int CTL_STATUS = 0;                       // DevStatus (4 ints)
 constexpr int CTL_RANGES = 4;                       // 2 * NCLASS_MAX
 constexpr int CTL_HEADS = CTL_RANGES + 2 * NCLASS_MAX;  // NCLASS_MAX + 1
 constexpr int CTL_INFO = 30;                        // wire check {maxA, maxB, bad} (+1 pad)
-constexpr int CTL_CELLS = 34;                       // 8-byte aligned: NCLASS_MAX + 2 uint64
+constexpr int CTL_CELLS = 34;                       // 8-byte aligned: NCELLS uint64
 static_assert(CTL_HEADS + NCLASS_MAX + 1 <= CTL_INFO, "control block layout");
-constexpr int CTL_HIST = CTL_CELLS + 2 * (NCLASS_MAX + 2);  // NCLASS_MAX * NBUCKET
+constexpr int NCELLS = NCLASS_MAX + 3;              // per class, rerun, wire check, batch total
+constexpr int CTL_COST = CTL_CELLS + 2 * NCELLS;    // modelled cost per class (uint64, ps)
+constexpr int CTL_ALLOT = CTL_COST + 2 * NCLASS_MAX;  // ClassAllot per class + rerun (4 ints each)
+static_assert(CTL_COST % 2 == 0 && CTL_ALLOT % 2 == 0, "8-byte aligned control block fields");
+constexpr int CTL_HIST = CTL_ALLOT + 4 * (NCLASS_MAX + 1);  // NCLASS_MAX * NBUCKET
 constexpr int CTL_OFFS = CTL_HIST + NCLASS_MAX * NBUCKET;
 constexpr int CTL_INTS = CTL_OFFS + NCLASS_MAX * NBUCKET;
 constexpr int CELLS_RERUN = NCLASS_MAX;             // index of the rerun cells
 constexpr int CELLS_WIRE = NCLASS_MAX + 1;          // cells found by the wire check
+constexpr int CELLS_TOTAL = NCLASS_MAX + 2;         // cells of the batch (k_bin_total)
 
 // A kernel's dynamic shared memory limit is one process-wide attribute per
 // device, shared by every engine: engines with different alphabets need
@@ -224,6 +254,17 @@ int smem_for(const ipuma_engine* e) {
 template <class T, int K, int LANES>
 int batched_grid(ipuma_engine* e) {
   return occupancy_grid(e, k_batched<T, K, LANES>, smem_for<T, K, LANES>(e));
+}
+
+template <int K>
+int thread_smem(const ipuma_engine* e) {
+  return ThreadSmem<K>::total(e->M, kWarpsPerBlock);
+}
+
+// Threads of a k_thread<K> launch (one boundary column each).
+template <int K>
+long thread_threads(ipuma_engine* e) {
+  return (long)occupancy_grid(e, k_thread<K>, thread_smem<K>(e)) * kThreads;
 }
 
 // Lane groups (one scratch slice each) of the widest batched launch.
@@ -275,10 +316,12 @@ int timed_end(ipuma_engine* e, cudaStream_t s) {
   return IPUMA_OK;
 }
 
+// allot_idx = entry of the control block's ClassAllot table (the class, or
+// NCLASS_MAX for the s32 rerun).
 template <class T, int K, int LANES>
 int launch_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_t* codes,
                    const PairDesc* pairs, const int* list, const int* range, int* head, long rowsCap,
-                   int* score, int* arange, int* brange, int kind, int cls) {
+                   int* score, int* arange, int* brange, int kind, int cls, int allot_idx) {
   const int smem = smem_for<T, K, LANES>(e);
   const int grid = batched_grid<T, K, LANES>(e);
   int* ctl = rb.ctl;
@@ -288,17 +331,90 @@ int launch_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uin
   k_batched<T, K, LANES><<<grid, kThreads, smem, s>>>(
       e->sc, e->d_sim.as<int8_t>(), codes, pairs, list, range, head, rb.scratch->as<int2>(),
       rowsCap, score, arange, brange, rb.ovf->as<int>(), cells + CELLS_RERUN,
-      reinterpret_cast<DevStatus*>(ctl + CTL_STATUS));
+      reinterpret_cast<DevStatus*>(ctl + CTL_STATUS),
+      reinterpret_cast<const ClassAllot*>(ctl + CTL_ALLOT) + allot_idx);
+  CUDA_TRY(cudaGetLastError());
+  return timed_end(e, s);
+}
+
+// Launches the per-thread class over its list range; rowsCap = rows of
+// the boundary scratch per thread.
+template <int K>
+int launch_thread(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_t* codes,
+                  const PairDesc* pairs, const int* list, const int* range, int* head, long rowsCap,
+                  int* score, int* arange, int* brange, int cls) {
+  const int smem = thread_smem<K>(e);
+  const int grid = occupancy_grid(e, k_thread<K>, smem);
+  int* ctl = rb.ctl;
+  auto* cells = reinterpret_cast<unsigned long long*>(ctl + CTL_CELLS);
+  int rc;
+  if ((rc = timed_begin(e, s, kClasses[cls].kind, cls))) return rc;
+  k_thread<K><<<grid, kThreads, smem, s>>>(e->sc, e->d_sim.as<int8_t>(), codes, pairs, list, range, head,
+                                           rb.scratch->as<int2>(), rowsCap, score, arange, brange,
+                                           rb.ovf->as<int>(), cells + CELLS_RERUN,
+                                           reinterpret_cast<DevStatus*>(ctl + CTL_STATUS),
+                                           reinterpret_cast<const ClassAllot*>(ctl + CTL_ALLOT) + cls);
   CUDA_TRY(cudaGetLastError());
   return timed_end(e, s);
 }
 
 // Grows every buffer run_batched uses for a batch of this shape, so that
 // the pipeline itself allocates nothing (graph capture).
-int reserve_bufs(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, int n, int maxB) {
+// Rows of the per-thread class's boundary scratch (0 when no pair of the
+// batch can need a second strip there).  The class only takes pairs of at
+// most kThrMaxRows rows, unless option tile_k forces every pair into it.
+long thread_rows(const ipuma_engine* e, int maxA, int maxB) {
+  if (maxA <= kClasses[kClsThread].width) return 0;
+  return e->tile_k == kClsThread + 1 ? maxB : std::min(maxB, kThrMaxRows);
+}
+
+// Strip-boundary scratch (int2) of one run: the wavefront classes need two
+// columns of rowsCap per lane group, the per-thread class one column of
+// thread_rows per thread.
+// Full-occupancy grid and strip scratch (int2) per block of every class.
+void class_grids(ipuma_engine* e, int maxA, int maxB, int* grid, long long* spb) {
+  const long long rowsCap = std::max(1, maxB);
+  for (int c = 0; c <= kNumS16; ++c) {
+    switch (c) {
+      case 0: grid[c] = batched_grid<LaneS16x2, 4, 16>(e); break;
+      case 1: grid[c] = batched_grid<LaneS16x2, 8, 16>(e); break;
+      case 2: grid[c] = batched_grid<LaneS16x2, 12, 16>(e); break;
+      case 3: grid[c] = batched_grid<LaneS16x2, 16, 16>(e); break;
+      case 4: grid[c] = batched_grid<LaneS16x2, 12, 32>(e); break;
+      case 5: grid[c] = batched_grid<LaneS16x2, 16, 32>(e); break;
+      case kClsThread: grid[c] = (int)(thread_threads<16>(e) / kThreads); break;
+      default: grid[c] = batched_grid<LaneS32, 16, 32>(e); break;
+    }
+    if (c == kClsThread)
+      spb[c] = (long long)kThreads * thread_rows(e, maxA, maxB);
+    else
+      spb[c] = (long long)kWarpsPerBlock * (32 / kClasses[c].lanes) * 2 * rowsCap;
+  }
+}
+
+// Scratch for any split of the GPU between the classes: shares are
+// fractions f_c of each class's full grid with sum f_c = 1, rounded up.
+// With two alternating streams (option concurrent = 2) two full-grid
+// launches may run at once: two regions of the largest full grid.
+size_t scratch_int2(ipuma_engine* e, int maxA, int maxB) {
+  int grid[NCLASS_MAX + 1];
+  long long spb[NCLASS_MAX + 1];
+  class_grids(e, maxA, maxB, grid, spb);
+  long long full = 0, round = 0;
+  for (int c = 0; c <= kNumS16; ++c) {
+    full = std::max(full, (long long)grid[c] * spb[c]);
+    round += spb[c];
+  }
+  return (size_t)std::max(full + round, 2 * full);
+}
+
+// Launch order of the classes (longest-tail classes first) and, for two
+// alternating streams, the stream (and scratch region) of each.
+constexpr int kLaunchOrder[kNumS16 + 1] = {7, 5, 4, 6, 3, 2, 1, 0};
+
+int reserve_bufs(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, int n, int maxA, int maxB) {
   int rc;
-  const long rowsCap = std::max(1, maxB);
-  if ((rc = rb.scratch->ensure(sizeof(int2) * 2 * rowsCap * max_batched_groups(e), s))) return rc;
+  if ((rc = rb.scratch->ensure(sizeof(int2) * scratch_int2(e, maxA, maxB), s))) return rc;
   if ((rc = rb.list->ensure(sizeof(int) * (size_t)n + 64, s))) return rc;
   if ((rc = rb.ovf->ensure(sizeof(int) * (size_t)n + 64, s))) return rc;
   if ((rc = rb.flag->ensure((size_t)n + 64, s))) return rc;
@@ -308,8 +424,7 @@ int reserve_bufs(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, int n, int 
 int reserve_batched(ipuma_engine* e, cudaStream_t s, int n, int maxA, int maxB) {
   int rc;
   if ((rc = e->d_ctl.ensure(sizeof(int) * CTL_INTS, s))) return rc;
-  (void)maxA;
-  return reserve_bufs(e, main_bufs(e), s, n, maxB);
+  return reserve_bufs(e, main_bufs(e), s, n, maxA, maxB);
 }
 
 // Runs the persistent cost-binned pipeline over n device-resident pairs.
@@ -340,8 +455,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
 
   // Scratch for strip boundaries and the lists.
   const long rowsCap = std::max(1, maxB);
-  const long groups = max_batched_groups(e);
-  if ((rc = rb.scratch->ensure(sizeof(int2) * 2 * rowsCap * groups, s))) return rc;
+  if ((rc = rb.scratch->ensure(sizeof(int2) * scratch_int2(e, maxA, maxB), s))) return rc;
   if ((rc = rb.list->ensure(sizeof(int) * (size_t)n + 64, s))) return rc;
   if ((rc = rb.ovf->ensure(sizeof(int) * (size_t)n + 64, s))) return rc;
 
@@ -353,11 +467,37 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   bp.force_s32 = e->s16_ok ? 0 : 1;
   for (int c = 0; c <= kNumS16; ++c) {
     bp.lanes[c] = kClasses[c].lanes;
-    bp.width[c] = kClasses[c].lanes * kClasses[c].k;
+    bp.width[c] = kClasses[c].width;
     bp.slot_ps[c] = e->slot_ps[c];
     bp.strip_ps[c] = e->strip_ps[c];
   }
-  bp.widest = kNumS16 - 1;
+  bp.widest = kClsWidest;
+  const long thrThreads = thread_threads<16>(e);
+  bp.thr_cls = kClsThread;
+  bp.thr_on = e->thread_class;
+  bp.thr_k = kClasses[kClsThread].width;
+  bp.thr_max_rows = kThrMaxRows;
+  bp.thr_cap_scale = kThrLatencyShare / (2.0f * (float)thrThreads);
+  bp.total_cells = reinterpret_cast<const unsigned long long*>(ctl + CTL_CELLS) + CELLS_TOTAL;
+  // Concurrent class launches, except when every launch is timed alone.
+  const int mode = e->time_launches ? 0 : e->concurrent;
+  const bool conc = mode != 0;
+  bp.concurrent = mode;
+  class_grids(e, maxA, maxB, bp.grid, bp.scr_per_block);
+  bp.scr_cap = (long long)(rb.scratch->cap / sizeof(int2));
+  float slot_min = 1e30f;
+  for (int c = 0; c < kNumS16; ++c) {
+    // cell slots one warp step covers: 32 lanes x k columns x 2 pairs
+    // (the per-thread class: 32 threads x 16 columns x 2 pairs per row)
+    bp.step_ps[c] = e->slot_ps[c] * 64.f * (float)kClasses[c].k * (float)(bp.grid[c] * kWarpsPerBlock);
+    if (c != kClsThread) slot_min = std::min(slot_min, e->slot_ps[c]);
+  }
+  bp.batch_ps_per_cell = slot_min / kPackingEfficiency;
+  bp.lat_share = kLatencyShare;
+  bp.lat_min_ps = kLatencyMinBatchPs;
+  bp.region = 0;
+  for (int c = 0; c <= kNumS16; ++c) bp.region = std::max(bp.region, (long long)bp.grid[c] * bp.scr_per_block[c]);
+  for (int k = 0; k <= kNumS16; ++k) bp.slot_of[kLaunchOrder[k]] = k & 1;
   bp.long_a = e->long_a;
   // tile_k > 0 forces one s16x2 class: every pair uses the chosen kernel,
   // long A crossing several strips.
@@ -370,37 +510,75 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   const int nkeys = bp.nclass * NBUCKET;
   const int tb = 256;
   const int gb = std::min<int>((n + tb - 1) / tb, e->nsm * 8);
+  k_bin_total<<<gb, tb, 0, s>>>(bp, pairs, n,
+                                reinterpret_cast<unsigned long long*>(ctl + CTL_CELLS) + CELLS_TOTAL);
   k_bin_count<<<gb, tb, 0, s>>>(bp, codes, e->d_sim.as<int8_t>(), pairs, n, ctl + CTL_HIST,
                                 rb.flag->as<uint8_t>(),
-                                reinterpret_cast<unsigned long long*>(ctl + CTL_CELLS), st, score,
+                                reinterpret_cast<unsigned long long*>(ctl + CTL_CELLS),
+                                reinterpret_cast<unsigned long long*>(ctl + CTL_COST), st, score,
                                 arange, brange);
-  k_bin_scan<<<1, 1024, 0, s>>>(nkeys, ctl + CTL_HIST, ctl + CTL_OFFS, ctl + CTL_RANGES);
+  k_bin_scan<<<1, 1024, 0, s>>>(bp, nkeys, ctl + CTL_HIST, ctl + CTL_OFFS, ctl + CTL_RANGES,
+                                reinterpret_cast<const unsigned long long*>(ctl + CTL_COST),
+                                reinterpret_cast<ClassAllot*>(ctl + CTL_ALLOT), st);
   k_bin_scatter<<<gb, tb, 0, s>>>(bp, pairs, n, rb.flag->as<uint8_t>(), ctl + CTL_OFFS,
                                   rb.list->as<int>());
   CUDA_TRY(cudaGetLastError());
-  *launches += 3;
+  *launches += 4;
 
   int* list = rb.list->as<int>();
   int* heads = ctl + CTL_HEADS;
-  // Long-tail first: the s32 class holds the longest high-scoring pairs,
-  // then the s16x2 classes from the widest down.
+  // Class launches: concurrently on the class streams (each on the share
+  // of the SMs k_bin_scan gave it, so every class starts its longest items
+  // at once and the classes finish together), or one after the other on
+  // `s`, longest-tail classes first.
+  if (conc) CUDA_TRY(cudaEventRecord(e->fork_ev, s));
+  // Stream of a class: its own (shares) or one of two by launch position.
+  auto stream_of = [&](int cls) -> int {
+    if (mode == 2) return bp.slot_of[cls];
+    return cls;
+  };
+  auto on = [&](int cls) -> cudaStream_t {
+    if (!conc) return s;
+    cudaStream_t cs = e->cls_stream[stream_of(cls)];
+    cudaStreamWaitEvent(cs, e->fork_ev, 0);
+    return cs;
+  };
+  auto done = [&](int cls) -> int {
+    if (!conc) return IPUMA_OK;
+    cudaStream_t cs = e->cls_stream[stream_of(cls)];
+    CUDA_TRY(cudaEventRecord(e->join_ev[cls], cs));
+    CUDA_TRY(cudaStreamWaitEvent(s, e->join_ev[cls], 0));
+    return IPUMA_OK;
+  };
   const int* R = ctl + CTL_RANGES;
-#define IPUMA_LAUNCH(T, K, L, cls)                                                              \
-  if ((rc = launch_batched<T, K, L>(e, rb, s, codes, pairs, list, R + 2 * (cls), heads + (cls), rowsCap, \
-                                    score, arange, brange, kClasses[cls].kind, cls)))          \
-    return rc;
-  IPUMA_LAUNCH(LaneS32, 16, 32, 6)
+#define IPUMA_LAUNCH(T, K, L, cls)                                                                     \
+  {                                                                                                    \
+    cudaStream_t cs = on(cls);                                                                         \
+    if ((rc = launch_batched<T, K, L>(e, rb, cs, codes, pairs, list, R + 2 * (cls), heads + (cls),     \
+                                      rowsCap, score, arange, brange, kClasses[cls].kind, cls, cls)))  \
+      return rc;                                                                                       \
+    if ((rc = done(cls))) return rc;                                                                   \
+  }
+  IPUMA_LAUNCH(LaneS32, 16, 32, 7)
   IPUMA_LAUNCH(LaneS16x2, 16, 32, 5)
   IPUMA_LAUNCH(LaneS16x2, 12, 32, 4)
+  {
+    cudaStream_t cs = on(kClsThread);
+    if ((rc = launch_thread<16>(e, rb, cs, codes, pairs, list, R + 2 * kClsThread, heads + kClsThread,
+                                thread_rows(e, maxA, maxB), score, arange, brange, kClsThread)))
+      return rc;
+    if ((rc = done(kClsThread))) return rc;
+  }
   IPUMA_LAUNCH(LaneS16x2, 16, 16, 3)
   IPUMA_LAUNCH(LaneS16x2, 12, 16, 2)
   IPUMA_LAUNCH(LaneS16x2, 8, 16, 1)
   IPUMA_LAUNCH(LaneS16x2, 4, 16, 0)
 #undef IPUMA_LAUNCH
-  // Exact 32-bit rerun of the s16x2 pairs whose score may have overflowed.
+  // Exact 32-bit rerun of the s16x2 pairs whose score may have overflowed
+  // (after every class: it reads their overflow list).
   if ((rc = launch_batched<LaneS32, 16, 32>(e, rb, s, codes, pairs, rb.ovf->as<int>(), ctl + CTL_STATUS + 1,
-                                            heads + 7, rowsCap, score, arange, brange,
-                                            IPUMA_KERNEL_S32_RERUN, CELLS_RERUN)))
+                                            heads + NCLASS_MAX, rowsCap, score, arange, brange,
+                                            IPUMA_KERNEL_S32_RERUN, CELLS_RERUN, NCLASS_MAX)))
     return rc;
   *launches += kNumS16 + 2;
   return IPUMA_OK;
@@ -420,9 +598,9 @@ int reset_ctl(ipuma_engine* e, cudaStream_t s) {
 // overflow reruns and per-class cells are summed).
 int check_status(ipuma_engine* e, cudaStream_t s, int nblk = 1) {
   DevStatus st{};
-  unsigned long long cells[NCLASS_MAX + 2] = {};
+  unsigned long long cells[NCELLS] = {};
   DevStatus stk[kMaxChunks];
-  unsigned long long cellsk[kMaxChunks][NCLASS_MAX + 2];
+  unsigned long long cellsk[kMaxChunks][NCELLS];
   nblk = std::max(1, std::min(nblk, kMaxChunks));
   for (int k = 0; k < nblk; ++k) {
     const int* ctl = e->d_ctl.as<int>() + (size_t)k * CTL_INTS;
@@ -433,7 +611,7 @@ int check_status(ipuma_engine* e, cudaStream_t s, int nblk = 1) {
   for (int k = 0; k < nblk; ++k) {
     if (!st.error) st.error = stk[k].error;
     st.overflow_count += stk[k].overflow_count;
-    for (int c = 0; c < NCLASS_MAX + 2; ++c) cells[c] += cellsk[k][c];
+    for (int c = 0; c < NCELLS; ++c) cells[c] += cellsk[k][c];
   }
   e->stats.overflow_reruns = st.overflow_count;
   e->stats.n_timed = e->n_timed;
@@ -443,7 +621,7 @@ int check_status(ipuma_engine* e, cudaStream_t s, int nblk = 1) {
     e->stats.timed_kind[k] = e->timed_kind[k];
     e->stats.timed_ms[k] = ms;
     const int c = e->timed_cls[k];
-    e->stats.timed_cells[k] = (c >= 0 && c < NCLASS_MAX + 2) ? (int64_t)cells[c] : 0;
+    e->stats.timed_cells[k] = (c >= 0 && c < NCELLS) ? (int64_t)cells[c] : 0;
   }
   e->n_timed = 0;
   if (st.error == ERR_LENGTH) return fail(IPUMA_ERR_TOO_LONG, "a pair exceeds the stated maximum length");
@@ -504,13 +682,22 @@ int validate_algo(const ipuma_algo_config* a) {
 // a cache file of "key<TAB>slot_ps...<TAB>strip_ps..." lines.
 // ---------------------------------------------------------------------------
 
+// The s32 class is not tuned (it is chosen by the overflow rules, not by
+// cost); for the GPU shares of concurrent launches it is modelled as the
+// widest s16x2 class with one pair per lane group instead of two.
+void set_s32_rates(ipuma_engine* e) {
+  e->slot_ps[kClsS32] = 2.f * e->slot_ps[kClsWidest];
+  e->strip_ps[kClsS32] = 2.f * e->strip_ps[kClsWidest];
+}
+
 void set_default_rates(ipuma_engine* e) {
   // Measured on B200 with the nucleic-acid alphabet (uniform related pairs).
-  const float slot[kNumS16] = {0.385f, 0.286f, 0.263f, 0.25f, 0.3125f, 0.3125f};
+  const float slot[kNumS16] = {0.385f, 0.286f, 0.263f, 0.25f, 0.3125f, 0.3125f, 0.2f};
   for (int c = 0; c < kNumS16; ++c) {
     e->slot_ps[c] = slot[c];
     e->strip_ps[c] = 0.f;
   }
+  set_s32_rates(e);
   e->tuned = false;
   e->tune_source = "defaults";
 }
@@ -522,7 +709,7 @@ std::string tune_key(const ipuma_engine* e) {
   cudaDeviceProp prop;
   cudaGetDeviceProperties(&prop, e->device);
   char buf[512];
-  snprintf(buf, sizeof(buf), "%s|sm%d%d|M=%d|sim=%d|gI=%d|gE=%d|v1", prop.name, prop.major, prop.minor, e->M,
+  snprintf(buf, sizeof(buf), "%s|sm%d%d|M=%d|sim=%d|gI=%d|gE=%d|v3", prop.name, prop.major, prop.minor, e->M,
            e->sw.similarity, e->sw.gap_init, e->sw.gap_extend);
   for (char* c = buf; *c; ++c)
     if (*c == '\t' || *c == '\n') *c = ' ';
@@ -534,6 +721,7 @@ void apply_rates(ipuma_engine* e, const std::vector<float>& v, const char* sourc
     e->slot_ps[c] = v[c];
     e->strip_ps[c] = v[kNumS16 + c];
   }
+  set_s32_rates(e);
   e->tuned = true;
   e->tune_source = source;
 }
@@ -645,8 +833,11 @@ int run_autotune(ipuma_engine* e, const char* cache_path) {
   CUDA_TRY(cudaMemcpy(dl.p, letters.data(), letters.size(), cudaMemcpyHostToDevice));
   v.assign(2 * kNumS16, 0.f);
   for (int c = 0; c < kNumS16 && rc == IPUMA_OK; ++c) {
-    const int W = kClasses[c].lanes * kClasses[c].k, L = kClasses[c].lanes;
-    const int perItem = (32 / L) * 2;
+    const int W = kClasses[c].width, L = kClasses[c].lanes;
+    // Pairs per warp item; the per-thread class keeps 64 pairs per warp and
+    // far more pairs resident, so two rounds of items suffice there.
+    const int perItem = L > 0 ? (32 / L) * 2 : 64;
+    const int rounds = L > 0 ? 6 : 2;
     int grid = 1;
     switch (c) {
       case 0: grid = batched_grid<LaneS16x2, 4, 16>(e); break;
@@ -654,21 +845,30 @@ int run_autotune(ipuma_engine* e, const char* cache_path) {
       case 2: grid = batched_grid<LaneS16x2, 12, 16>(e); break;
       case 3: grid = batched_grid<LaneS16x2, 16, 16>(e); break;
       case 4: grid = batched_grid<LaneS16x2, 12, 32>(e); break;
-      default: grid = batched_grid<LaneS16x2, 16, 32>(e); break;
+      case 5: grid = batched_grid<LaneS16x2, 16, 32>(e); break;
+      default: grid = (int)(thread_threads<16>(e) / kThreads); break;
     }
-    const int minPairs = grid * kWarpsPerBlock * perItem * 6;
-    const int shapes[2][3] = {{1, 1024, 0}, {8, 128, 0}};
+    const int minPairs = grid * kWarpsPerBlock * perItem * rounds;
+    // (strips, rows) of the two calibration batches.  The per-thread class
+    // passes a boundary column through global memory at every strip, so
+    // its shapes have several strips and a boundary working set larger
+    // than L2, as real batches do.
+    const int shapes[2][2] = {{1, 1024}, {8, 128}};
+    const int thr_shapes[2][2] = {{4, 1024}, {16, 512}};
     double tpp[2] = {0, 0};
     for (int sh = 0; sh < 2 && rc == IPUMA_OK; ++sh) {
-      const int alen = shapes[sh][0] * W, blen = shapes[sh][1];
+      const int* shp = L > 0 ? shapes[sh] : thr_shapes[sh];
+      const int alen = shp[0] * W, blen = shp[1];
       const int n = std::max(minPairs, (int)std::min(2.0e6, 1.5e9 / ((double)alen * blen)));
       float ms = -1.f;
       rc = time_class(e, c, n, alen, blen, dl, (int)letters.size(), 0x5eed0000u + 16 * c + sh, &ms);
       tpp[sh] = ms > 0 ? ms * 1e9 / n : 0;  // ps per pair
     }
     // tpp = strips * ((rows + L) * W * slot + strip)
-    const double a1 = (1024.0 + L) * W, a2 = 8.0 * (128.0 + L) * W;
-    const double b1 = 1.0, b2 = 8.0;
+    const int* s1 = L > 0 ? shapes[0] : thr_shapes[0];
+    const int* s2 = L > 0 ? shapes[1] : thr_shapes[1];
+    const double a1 = (double)s1[0] * (s1[1] + L) * W, a2 = (double)s2[0] * (s2[1] + L) * W;
+    const double b1 = s1[0], b2 = s2[0];
     const double det = a1 * b2 - a2 * b1;
     double slot = (tpp[0] * b2 - tpp[1] * b1) / det;
     double strip = (a1 * tpp[1] - a2 * tpp[0]) / det;
@@ -820,6 +1020,13 @@ int ipuma_gpu_create(const ipuma_sw_config* sw, const ipuma_algo_config* algo, i
   e->nsm = prop.multiProcessorCount;
   CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
   for (auto& ev : e->ev) CUDA_TRY(cudaEventCreate(&ev));
+  // Class streams and their fork/join events (created here: no stream or
+  // event is created while a stream is being captured).
+  CUDA_TRY(cudaEventCreateWithFlags(&e->fork_ev, cudaEventDisableTiming));
+  for (int c = 0; c < NCLASS_MAX; ++c) {
+    CUDA_TRY(cudaStreamCreateWithFlags(&e->cls_stream[c], cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&e->join_ev[c], cudaEventDisableTiming));
+  }
 
   // Substitution matrix (swatlib::selectMatrix, ipu_batch_affine.cpp:390).
   int32_t m = 0, n = 0;
@@ -854,6 +1061,7 @@ int ipuma_gpu_create(const ipuma_sw_config* sw, const ipuma_algo_config* algo, i
   e->s16_max_len = e->maxSub > 0 ? (e->sc.s16Limit / e->maxSub) : (1 << 30);
   set_default_rates(e.get());
   max_batched_groups(e.get());  // warm the grid cache
+  thread_threads<16>(e.get());
   *out = e.release();
   return IPUMA_OK;
 }
@@ -872,6 +1080,12 @@ void ipuma_gpu_destroy(ipuma_engine* e) {
     b->release();
   for (auto& ev : e->cev)
     if (ev) cudaEventDestroy(ev);
+  for (int c = 0; c < NCLASS_MAX; ++c) {
+    if (e->cls_stream[c]) cudaStreamSynchronize(e->cls_stream[c]);
+    if (e->cls_stream[c]) cudaStreamDestroy(e->cls_stream[c]);
+    if (e->join_ev[c]) cudaEventDestroy(e->join_ev[c]);
+  }
+  if (e->fork_ev) cudaEventDestroy(e->fork_ev);
   if (e->stream2) cudaStreamDestroy(e->stream2);
   if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
   for (auto& ev : e->ev)
@@ -899,6 +1113,11 @@ int ipuma_gpu_set_option(ipuma_engine* e, const char* name, int64_t value) {
     e->autotune = value ? 1 : 0;
   } else if (k == "time_launches") {
     e->time_launches = value ? 1 : 0;
+  } else if (k == "concurrent") {
+    if (value < 0 || value > 2) return fail(IPUMA_ERR_INVALID_ARG, "concurrent must be 0, 1 or 2");
+    e->concurrent = (int)value;
+  } else if (k == "thread_class") {
+    e->thread_class = value ? 1 : 0;
   } else if (k == "chunks") {
     if (value < 0 || value > kMaxChunks)
       return fail(IPUMA_ERR_INVALID_ARG, "chunks must be 0 (automatic) .. %d", kMaxChunks);
@@ -1103,8 +1322,8 @@ int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes, con
     for (int k = 0; k < nch; ++k) nmax = std::max(nmax, cbeg[k + 1] - cbeg[k]);
     const RunBufs rb1{nullptr, &e->x_scratch, &e->x_list, &e->x_ovf, &e->x_flag};
     if ((rc = e->d_ctl.ensure(sizeof(int) * CTL_INTS * (size_t)nch, s))) return rc;
-    if ((rc = reserve_bufs(e, main_bufs(e), s, nmax, maxB))) return rc;
-    if ((rc = reserve_bufs(e, rb1, s, nmax, maxB))) return rc;
+    if ((rc = reserve_bufs(e, main_bufs(e), s, nmax, maxA, maxB))) return rc;
+    if ((rc = reserve_bufs(e, rb1, s, nmax, maxA, maxB))) return rc;
     const bool pinned_out = is_pinned(score) && is_pinned(arange) && is_pinned(brange);
     cudaStream_t run_s[2] = {s, e->stream2};
     CUDA_TRY(cudaEventRecord(e->ev[0], s));

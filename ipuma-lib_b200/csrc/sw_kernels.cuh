@@ -40,6 +40,17 @@ struct DevStatus {
   int pad;
 };
 
+// Share of the GPU one class launch may use: blocks with blockIdx.x >=
+// `blocks` exit at once, and the launch's strip scratch starts `base` int2
+// into the scratch buffer.  Written on the device by the binning pre-pass
+// (k_bin_scan) so that concurrent class launches split the SMs in
+// proportion to their modelled work and never share scratch.
+struct ClassAllot {
+  long long base;
+  int blocks;
+  int pad;
+};
+
 constexpr int ERR_SCRATCH = 1;  // a pass needed more scratch rows than provided
 constexpr int ERR_LENGTH = 2;   // a pair exceeded the stated maximum lengths
 
@@ -128,7 +139,10 @@ __global__ void __launch_bounds__(128) k_batched(SwConst sc, const int8_t* __res
                                                  const int* __restrict__ range, int* queue_head,
                                                  int2* scratch, long rowsCap, int* score,
                                                  int* arange, int* brange, int* overflow_list,
-                                                 unsigned long long* rerun_cells, DevStatus* st) {
+                                                 unsigned long long* rerun_cells, DevStatus* st,
+                                                 const ClassAllot* __restrict__ allot) {
+  if ((int)blockIdx.x >= allot->blocks) return;  // outside this launch's share
+  scratch += allot->base;
   using L = SmemLayout<T, K, LANES>;
   constexpr int NP = T::NP;
   constexpr int GROUPS = L::GROUPS;
@@ -349,6 +363,16 @@ struct BinParams {
   int width[NCLASS_MAX];   // strip width (lanes * K) of each class
   float slot_ps[NCLASS_MAX];   // time per cell slot of a strip (autotuned)
   float strip_ps[NCLASS_MAX];  // fixed time per strip (autotuned)
+  // Latency bound: one warp item of class c advances one step (row) every
+  // step_ps[c] when the GPU is full, so a pair of `strips` strips takes
+  // strips * (|B| + lanes) * step_ps[c].  A class is not chosen for a pair
+  // whose item would take longer than lat_share * (modelled batch time =
+  // cells of the batch * batch_ps_per_cell), when that batch time is at
+  // least lat_min_ps: a few such items would end their launch alone.
+  float step_ps[NCLASS_MAX];
+  float batch_ps_per_cell;
+  float lat_share;
+  float lat_min_ps;
   int long_a;                  // |A| above which the widest class is used
   int widest;                  // that class
   int forced_class;        // >= 0: every s16x2 pair goes to this class
@@ -356,7 +380,34 @@ struct BinParams {
   int max_a, max_b;        // stated maxima (violations set ERR_LENGTH)
   int M;                   // alphabet size of `sim`
   int force_s32;           // 1: every pair goes to the s32 class
+  // Per-thread class (k_thread): one thread per two pairs, so a pair's time
+  // is long.  A pair may use it only when |B| <= thr_max_rows and its cells
+  // stay below thr_cap_scale * (cells of the whole batch): that bounds its
+  // latency to a fraction of the batch's time (thr_cap_scale = fraction /
+  // pair slots the class keeps resident).
+  // Concurrent class launches (k_bin_scan turns modelled costs into block
+  // shares): full-occupancy grid and strip scratch (int2) per block of
+  // each class, and the scratch available.
+  int concurrent;          // 0 sequential, 1 shares, 2 two alternating streams
+  int slot_of[NCLASS_MAX + 1];  // mode 2: scratch region (0 / 1) of each class
+  long long region;             // mode 2: int2 per region
+  int grid[NCLASS_MAX + 1];
+  long long scr_per_block[NCLASS_MAX + 1];
+  long long scr_cap;
+  int thr_cls;             // class index
+  int thr_on;              // 0: the class is never chosen (unless forced)
+  int thr_k;               // columns per strip
+  int thr_max_rows;
+  float thr_cap_scale;
+  const unsigned long long* total_cells;  // written by k_bin_total
 };
+
+// Buckets of the per-thread class: exact strip counts up to 24 (then one
+// bucket), rows log-linear with 16 sub-buckets per octave (< 144 for rows
+// up to 2048); both descending.
+constexpr int THR_NSB = 25;
+constexpr int THR_NRB = 144;
+static_assert(THR_NSB * THR_NRB <= NBUCKET, "per-thread buckets");
 
 // Best ungapped score along the main diagonal (a lower bound of the local
 // alignment score): pairs that surely pass the s16 limit go straight to
@@ -376,7 +427,8 @@ static __device__ int diagonal_bound(const uint8_t* a, const uint8_t* b, int n, 
 // each strip's wavefront, and slot_ps / strip_ps are the per-class rates
 // the autotuner measured.  Key = class, then strip count (descending), then
 // rows (descending).
-__device__ __forceinline__ int pair_key(const BinParams& bp, int alen, int blen, bool s32) {
+__device__ __forceinline__ int pair_key(const BinParams& bp, int alen, int blen, bool s32, float thr_cap,
+                                        float* cost_out = nullptr) {
   int cls;
   if (bp.force_s32 || s32) {
     cls = bp.cls_s32;
@@ -389,9 +441,20 @@ __device__ __forceinline__ int pair_key(const BinParams& bp, int alen, int blen,
     cls = bp.widest;
   } else {
     cls = 0;
-    float bestCost = -1.f;
+    float bestCost = -1.f, bestLat = -1.f;
+    int latCls = 0;
+    const bool thr_ok = bp.thr_on && blen <= bp.thr_max_rows && (float)alen * (float)blen <= thr_cap;
+    const float batch_ps = bp.total_cells ? (float)(*bp.total_cells) * bp.batch_ps_per_cell : 0.f;
+    const float lat_cap = batch_ps >= bp.lat_min_ps ? bp.lat_share * batch_ps : 3.0e38f;
     for (int c = 0; c < bp.n_s16_classes; ++c) {
+      if (c == bp.thr_cls && !thr_ok) continue;
       const int strips = (alen + bp.width[c] - 1) / bp.width[c];
+      const float lat = (float)strips * (float)(blen + bp.lanes[c]) * bp.step_ps[c];
+      if (bestLat < 0.f || lat < bestLat) {
+        bestLat = lat;
+        latCls = c;
+      }
+      if (lat > lat_cap) continue;
       const float cost =
           (float)strips * ((float)(blen + bp.lanes[c]) * (float)bp.width[c] * bp.slot_ps[c] + bp.strip_ps[c]);
       if (bestCost < 0.f || cost < bestCost) {
@@ -399,16 +462,43 @@ __device__ __forceinline__ int pair_key(const BinParams& bp, int alen, int blen,
         cls = c;
       }
     }
+    if (bestCost < 0.f) cls = latCls;  // every class is too slow: the fastest
   }
   const int strips = (alen + bp.width[cls] - 1) / bp.width[cls];
+  if (cost_out)
+    *cost_out = (float)strips *
+                ((float)(blen + bp.lanes[cls]) * (float)bp.width[cls] * bp.slot_ps[cls] + bp.strip_ps[cls]);
+  if (cls == bp.thr_cls) {
+    const int sb = THR_NSB - 1 - min(strips - 1, THR_NSB - 1);
+    return cls * NBUCKET + sb * THR_NRB + (THR_NRB - 1 - min(rows_bucket(blen), THR_NRB - 1));
+  }
   const int sb = NSTRIPB - 1 - min(strips - 1, NSTRIPB - 1);
   return cls * NBUCKET + sb * NROWB + (NROWB - 1 - rows_bucket(blen));
 }
 
+// Latency cap of the per-thread class for this batch (cells per pair).
+__device__ __forceinline__ float thread_cap(const BinParams& bp) {
+  return (bp.thr_on && bp.total_cells) ? (float)(*bp.total_cells) * bp.thr_cap_scale : 0.f;
+}
+
+// Sum of |A| * |B| over the pairs the pipeline will align (the batch size
+// the per-thread class's latency cap is measured against).
+static __global__ void k_bin_total(BinParams bp, const PairDesc* __restrict__ pairs, int n,
+                                   unsigned long long* total) {
+  unsigned long long local = 0;
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
+    const PairDesc d = pairs[p];
+    if (d.a_len <= 0 || d.b_len <= 0 || d.a_len > bp.max_a || d.b_len > bp.max_b) continue;
+    local += (unsigned long long)d.a_len * (unsigned long long)d.b_len;
+  }
+  for (int off = 16; off > 0; off >>= 1) local += __shfl_xor_sync(FULL, local, off);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(total, local);
+}
+
 static __global__ void k_bin_count(BinParams bp, const uint8_t* __restrict__ codes, const int8_t* __restrict__ sim,
                             const PairDesc* __restrict__ pairs, int n, int* hist, uint8_t* s32_flag,
-                            unsigned long long* class_cells, DevStatus* st, int* score, int* arange,
-                            int* brange) {
+                            unsigned long long* class_cells, unsigned long long* class_cost, DevStatus* st,
+                            int* score, int* arange, int* brange) {
   for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
     const PairDesc d = pairs[p];
     if (d.a_len <= 0 || d.b_len <= 0) {
@@ -429,9 +519,11 @@ static __global__ void k_bin_count(BinParams bp, const uint8_t* __restrict__ cod
       s32 = diagonal_bound(codes + d.a_off, codes + d.b_off, min(d.a_len, d.b_len), sim, bp.M) >
             bp.s16_limit;
     s32_flag[p] = s32 ? 1 : 0;
-    const int key = pair_key(bp, d.a_len, d.b_len, s32);
+    float cost = 0.f;
+    const int key = pair_key(bp, d.a_len, d.b_len, s32, thread_cap(bp), &cost);
     atomicAdd(&hist[key], 1);
     atomicAdd(&class_cells[key / NBUCKET], (unsigned long long)d.a_len * (unsigned long long)d.b_len);
+    atomicAdd(&class_cost[key / NBUCKET], (unsigned long long)fmaxf(cost, 1.f));
   }
 }
 
@@ -441,7 +533,8 @@ __device__ __forceinline__ int run_total(const int* hist, const int* offs, int n
 
 // Single block: exclusive scan of the histogram into `offs`, and per class
 // the {start, count} range consumed by k_batched.
-static __global__ void k_bin_scan(int nkeys, const int* hist, int* offs, int* class_range) {
+static __global__ void k_bin_scan(BinParams bp, int nkeys, const int* hist, int* offs, int* class_range,
+                                  const unsigned long long* class_cost, ClassAllot* allot, DevStatus* st) {
   __shared__ int s_sum[1024];
   const int tid = threadIdx.x;
   const int per = (nkeys + blockDim.x - 1) / blockDim.x;
@@ -467,6 +560,37 @@ static __global__ void k_bin_scan(int nkeys, const int* hist, int* offs, int* cl
     class_range[2 * c + 1] = ((c + 1) * NBUCKET < nkeys ? offs[(c + 1) * NBUCKET] : run_total(hist, offs, nkeys)) -
                              offs[c * NBUCKET];
   }
+  __syncthreads();
+  if (tid == 0) {
+    // Block shares: sequential launches each take the whole GPU; concurrent
+    // ones split it by modelled cost, scratch regions laid end to end.
+    const int nc = nkeys / NBUCKET;
+    double total = 0.0;
+    for (int c = 0; c < nc; ++c)
+      if (class_range[2 * c + 1] > 0) total += (double)class_cost[c];
+    long long base = 0;
+    for (int c = 0; c < nc; ++c) {
+      int blocks = 0;
+      if (class_range[2 * c + 1] > 0) {
+        blocks = bp.grid[c];
+        if (bp.concurrent == 1 && total > 0.0)
+          blocks = min(bp.grid[c], max(1, (int)ceil((double)class_cost[c] / total * bp.grid[c])));
+      }
+      const long long start = bp.concurrent == 1 ? base : bp.concurrent == 2 ? bp.slot_of[c] * bp.region : 0;
+      const long long need = (long long)blocks * bp.scr_per_block[c];
+      if (start + need > bp.scr_cap) {
+        // Never reached when the host sized the scratch for these shares.
+        blocks = bp.scr_per_block[c] > 0 ? (int)max(0ll, (bp.scr_cap - start) / bp.scr_per_block[c]) : blocks;
+        if (blocks == 0 && class_range[2 * c + 1] > 0) atomicCAS(&st->error, 0, ERR_SCRATCH);
+      }
+      allot[c].blocks = blocks;
+      allot[c].base = start;
+      if (bp.concurrent == 1) base += (long long)blocks * bp.scr_per_block[c];
+    }
+    // The s32 rerun runs alone after every class: the whole GPU, base 0.
+    allot[nc].blocks = bp.grid[bp.cls_s32];
+    allot[nc].base = 0;
+  }
 }
 
 static __global__ void k_bin_scatter(BinParams bp, const PairDesc* __restrict__ pairs, int n,
@@ -474,7 +598,7 @@ static __global__ void k_bin_scatter(BinParams bp, const PairDesc* __restrict__ 
   for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
     const PairDesc d = pairs[p];
     if (d.a_len <= 0 || d.b_len <= 0 || d.a_len > bp.max_a || d.b_len > bp.max_b) continue;
-    const int pos = atomicAdd(&offs[pair_key(bp, d.a_len, d.b_len, s32_flag[p] != 0)], 1);
+    const int pos = atomicAdd(&offs[pair_key(bp, d.a_len, d.b_len, s32_flag[p] != 0, thread_cap(bp))], 1);
     list[pos] = (int)p;
   }
 }

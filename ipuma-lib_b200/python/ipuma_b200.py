@@ -48,7 +48,7 @@ KERNEL_NAMES = {0: "k_batched<s32,L32,K16>", 1: "k_batched<s16x2,L16,K4>",
                 2: "k_batched<s16x2,L16,K8>", 3: "k_batched<s16x2,L16,K12>",
                 4: "k_batched<s16x2,L16,K16>", 5: "k_batched<s16x2,L32,K12>",
                 6: "k_batched<s16x2,L32,K16>", 7: "k_batched<s32,L32,K16> rerun",
-                8: "k_plain<K>", 9: "k_exact"}
+                8: "k_plain<K>", 9: "k_exact", 10: "k_thread<s16x2,K16>"}
 
 
 class SwConfig(ctypes.Structure):

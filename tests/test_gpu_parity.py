@@ -110,11 +110,12 @@ def test_reference_codelet_answers(fixture, forward_only):
         _assert_same(_gpu(case, forward_only), want, case["name"])
 
 
-@pytest.mark.parametrize("tile_k", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("tile_k", [1, 2, 3, 4, 5, 6, 7])
 def test_random_answers_each_tile_width(tile_k):
     """Forces every pair through one s16x2 kernel class (16 or 32 lanes per
-    group, 4..16 columns per lane), so that long pairs cross several strips
-    (global scratch hand-over)."""
+    group, 4..16 columns per lane, or 7: one thread per two pairs with
+    16-column strips), so that long pairs cross several strips (global
+    scratch hand-over)."""
     for case in json.load(open(os.path.join(GOLD, "random_ref.json")))["cases"]:
         want = (case["ref"]["score"], case["ref"]["arange"], case["ref"]["brange"])
         _assert_same(_gpu(case, False, tile_k=tile_k), want, "%s class=%d" % (case["name"], tile_k))
@@ -178,6 +179,105 @@ def test_s16_rerun_of_unpredicted_overflow():
         _assert_same(got, want, "overflow fwd=%s" % fwd)
         assert want[0][0] > 32767
         assert st.overflow_reruns >= 1
+
+
+# ----------------------------------------------- per-thread class (7) ---
+
+THREAD_CLASS = 7
+
+
+@pytest.mark.parametrize("forward_only", [True, False])
+def test_thread_class_dna_and_protein_samples(forward_only):
+    """Every pair through the per-thread class: two pairs per thread with
+    different lengths, boundary columns in global scratch across strips."""
+    for wl in (workloads.dna_batched(n=3_000, seed=61), workloads.protein(n=2_000, seed=62)):
+        got, want, _ = _wl_run(wl, forward_only, tile_k=THREAD_CLASS)
+        _assert_same(got, want, "%s thread class" % wl.name)
+
+
+def test_thread_class_edges_ties_and_strip_boundaries():
+    rng = np.random.default_rng(63)
+    A, B = [], []
+    for la in [1, 2, 15, 16, 17, 31, 32, 33, 47, 48, 49, 255, 256, 257]:
+        for lb in [1, 2, 3, 4, 5, 7, 8, 9, 63, 64, 65, 300]:
+            a = "".join(rng.choice(list("ACGT"), la))
+            b = a[: max(1, lb // 2)] + "".join(rng.choice(list("ACGT"), max(0, lb - lb // 2)))
+            A.append(a)
+            B.append(b[:lb])
+    A += ["", "A", "AAAA", "ACGT" * 100, "T" * 700, "ACACACACAC", "GATTACA" * 9, "A" * 300]
+    B += ["A", "", "AAAA", "ACGT" * 100, "A" * 700, "ACACAC" * 5, "GATTACA" * 20, "A" * 77]
+    case = {"similarity": "na", "match": 1, "mismatch": -1, "ambiguity": -1, "datatype": "na",
+            "gapInit": 0, "gapExtend": -1, "A": A, "B": B}
+    for fwd in (False, True):
+        _assert_same(_gpu(case, fwd, tile_k=THREAD_CLASS), _oracle(case, fwd),
+                     "thread edges fwd=%s" % fwd)
+
+
+def test_thread_class_s16_overflow_goes_to_s32_rerun():
+    """A pair passing the s16 limit inside the per-thread class is rerun
+    in 32-bit lanes; its partner in the other halfword is unaffected."""
+    rng = np.random.default_rng(64)
+    w, c = oracle.encode("aa", "W")[0], oracle.encode("aa", "C")[0]
+    a = np.where(rng.random(3500) < 0.5, w, c).astype(np.uint8)
+    b = np.concatenate([[oracle.encode("aa", "A")[0]], a]).astype(np.uint8)
+    others = workloads.protein(n=63, seed=65)
+    codes = np.concatenate([a, b, others.codes])
+    base = a.size + b.size
+    pairs = ib.make_pairs(np.concatenate([[0], base + others.a_off]),
+                          np.concatenate([[a.size], others.a_len]),
+                          np.concatenate([[a.size], base + others.b_off]),
+                          np.concatenate([[b.size], others.b_len]))
+    case = {"similarity": "blosum62", "match": 1, "mismatch": -1, "ambiguity": -1,
+            "datatype": "aa", "gapInit": -10, "gapExtend": -1}
+    sim = oracle.select_matrix("blosum62")
+    for fwd in (False, True):
+        with _engine(case, fwd, tile_k=THREAD_CLASS) as e:
+            got = e.compare(codes, pairs)
+            st = e.stats()
+        want = oracle.sw_batch(codes, pairs["a_off"], pairs["a_len"], pairs["b_off"],
+                               pairs["b_len"], sim, -10, -1, forward_only=fwd)
+        _assert_same(got, want, "thread overflow fwd=%s" % fwd)
+        assert want[0][0] > 32767
+        assert st.overflow_reruns >= 1
+
+
+def test_thread_class_chosen_automatically_for_large_batches():
+    """With the class enabled (option thread_class) a large batch sends part
+    of its pairs to it; results equal the run with the class disabled."""
+    wl = workloads.dna_batched(n=120_000, seed=66)
+    case = _wl_case(wl)
+    pairs = ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len)
+    outs = []
+    for on in (1, 0):
+        with _engine(case, True, thread_class=on, time_launches=1) as e:
+            outs.append(e.compare(wl.codes, pairs))
+            st = e.stats()
+            kinds = {st.timed_kind[k]: st.timed_cells[k] for k in range(st.n_timed)}
+        assert (kinds.get(10, 0) > 0) == bool(on)
+    _assert_same(outs[0], outs[1], "thread class on/off")
+    idx = np.random.default_rng(1).choice(wl.n, 2_000, replace=False)
+    sim = oracle.select_matrix(wl.similarity)
+    want = oracle.sw_batch(wl.codes, wl.a_off[idx], wl.a_len[idx], wl.b_off[idx], wl.b_len[idx],
+                           sim, wl.gap_init, wl.gap_extend, forward_only=True)
+    _assert_same(tuple(o[idx] for o in outs[0]), want, "thread class sample")
+
+
+# ------------------------------------------------- concurrent classes ---
+
+@pytest.mark.parametrize("forward_only", [True, False])
+def test_concurrent_class_launches_equal_sequential(forward_only):
+    """Classes launched concurrently on shares of the SMs (default) give the
+    results of one-after-the-other launches, with s32 pairs, s16x2 give-ups
+    rerun after all classes, and multi-strip pairs in several classes at
+    once (each with its own scratch region)."""
+    wl = workloads.protein_mixed(n=2_500, seed=67, long_identical_frac=0.004)
+    outs, reruns = [], []
+    for conc in (1, 0):
+        got, want, st = _wl_run(wl, forward_only, concurrent=conc)
+        _assert_same(got, want, "%s concurrent=%d" % (wl.name, conc))
+        outs.append(got)
+        reruns.append(st.overflow_reruns)
+    assert reruns[0] == reruns[1]
 
 
 # --------------------------------------------------------------- edges ---
