@@ -110,6 +110,8 @@ typedef struct ipuma_pair {
 } ipuma_pair;
 
 /* Timing and work counters of the last completed call on an engine. */
+#define IPUMA_MAX_TIMED 16  /* launches ipuma_stats can time per call */
+
 typedef struct ipuma_stats {
   double kernel_ms;     /* device time of the alignment kernels (CUDA events) */
   double total_ms;      /* device time including copies                      */
@@ -122,9 +124,9 @@ typedef struct ipuma_stats {
   /* With option "time_launches" = 1: device time and forward-pass cells of
    * each alignment-kernel launch of the call, in launch order. */
   int32_t n_timed;
-  int32_t timed_kind[10];   /* IPUMA_KERNEL_* */
-  double timed_ms[10];
-  int64_t timed_cells[10];
+  int32_t timed_kind[IPUMA_MAX_TIMED];   /* IPUMA_KERNEL_* */
+  double timed_ms[IPUMA_MAX_TIMED];
+  int64_t timed_cells[IPUMA_MAX_TIMED];
   /* ipuma_gpu_compare: chunks the batch was split into for upload/compute
    * overlap (1 = one upload, then the kernels). */
   int32_t chunks;
@@ -144,6 +146,9 @@ typedef struct ipuma_stats {
 #define IPUMA_KERNEL_PLAIN 8       /* one-launch-per-batch wire kernel      */
 #define IPUMA_KERNEL_EXACT 9       /* per-thread exact kernel               */
 #define IPUMA_KERNEL_S16_T_K16 10  /* s16x2, one thread per two pairs, 16-column strips */
+#define IPUMA_KERNEL_S16_L16_K6 11
+#define IPUMA_KERNEL_S16_L16_K10 12
+#define IPUMA_KERNEL_S16_L16_K14 13
 
 typedef struct ipuma_engine ipuma_engine;
 
@@ -175,7 +180,8 @@ void ipuma_gpu_destroy(ipuma_engine* e);
  *   "graphs"      1 = capture and replay CUDA graphs for repeated shapes
  *   "tile_k"      0 = kernel class by |A| (default); 1..6 = every pair
  *                 through s16x2 class IPUMA_KERNEL_S16_* (value = kind),
- *                 7 = every pair through IPUMA_KERNEL_S16_T_K16
+ *                 7 = every pair through IPUMA_KERNEL_S16_T_K16, 8, 9, 10 =
+ *                 IPUMA_KERNEL_S16_L16_K6, _K10, _K14
  *   "concurrent"  2 = class launches alternate between two streams, so
  *                 each starts on the SMs the previous one frees (default);
  *                 1 = all classes at once, each on a share of the SMs

@@ -95,14 +95,17 @@ struct DevBuf {
 struct ClassDef {
   int lanes, k, kind, width;
 };
-constexpr int kNumS16 = 7;
+constexpr int kNumS16 = 10;
 constexpr ClassDef kClasses[kNumS16 + 1] = {
     {16, 4, IPUMA_KERNEL_S16_L16_K4, 64},    {16, 8, IPUMA_KERNEL_S16_L16_K8, 128},
     {16, 12, IPUMA_KERNEL_S16_L16_K12, 192}, {16, 16, IPUMA_KERNEL_S16_L16_K16, 256},
     {32, 12, IPUMA_KERNEL_S16_L32_K12, 384}, {32, 16, IPUMA_KERNEL_S16_L32_K16, 512},
-    {0, 16, IPUMA_KERNEL_S16_T_K16, 16},     {32, 16, IPUMA_KERNEL_S32_K16, 512},
+    {0, 16, IPUMA_KERNEL_S16_T_K16, 16},     {16, 6, IPUMA_KERNEL_S16_L16_K6, 96},
+    {16, 10, IPUMA_KERNEL_S16_L16_K10, 160}, {16, 14, IPUMA_KERNEL_S16_L16_K14, 224},
+    {32, 16, IPUMA_KERNEL_S32_K16, 512},
 };
 constexpr int kClsWidest = 5;  // widest wavefront class (very long |A|)
+constexpr int kMaxTimed = IPUMA_MAX_TIMED;  // launches timed per call (time_launches)
 constexpr int kClsThread = 6;  // per-thread class k_thread<16>
 constexpr int kClsS32 = kNumS16;
 // Per-thread class: rows it accepts (its boundary scratch is rows x threads)
@@ -162,10 +165,10 @@ struct ipuma_engine {
   std::string tune_source = "defaults";
 
   // per-launch timing of the current call (time_launches)
-  cudaEvent_t tev[2 * 10] = {};
+  cudaEvent_t tev[2 * kMaxTimed] = {};
   int n_timed = 0;
-  int timed_kind[10] = {};
-  int timed_cls[10] = {};
+  int timed_kind[kMaxTimed] = {};
+  int timed_cls[kMaxTimed] = {};
 
   DevBuf d_sim, d_codes, d_pairs, d_list, d_res, d_scratch, d_cf, d_ovf, d_ctl, d_inputs, d_wres, d_flag;
   // Second buffer set and streams of the chunked host-to-host path
@@ -199,9 +202,8 @@ namespace {
 constexpr int CTL_STATUS = 0;                       // DevStatus (4 ints)
 constexpr int CTL_RANGES = 4;                       // 2 * NCLASS_MAX
 constexpr int CTL_HEADS = CTL_RANGES + 2 * NCLASS_MAX;  // NCLASS_MAX + 1
-constexpr int CTL_INFO = 30;                        // wire check {maxA, maxB, bad} (+1 pad)
-constexpr int CTL_CELLS = 34;                       // 8-byte aligned: NCELLS uint64
-static_assert(CTL_HEADS + NCLASS_MAX + 1 <= CTL_INFO, "control block layout");
+constexpr int CTL_INFO = CTL_HEADS + NCLASS_MAX + 1;    // wire check {maxA, maxB, bad} (+1 pad)
+constexpr int CTL_CELLS = ((CTL_INFO + 4) + 1) & ~1;    // 8-byte aligned: NCELLS uint64
 constexpr int NCELLS = NCLASS_MAX + 3;              // per class, rerun, wire check, batch total
 constexpr int CTL_COST = CTL_CELLS + 2 * NCELLS;    // modelled cost per class (uint64, ps)
 constexpr int CTL_ALLOT = CTL_COST + 2 * NCLASS_MAX;  // ClassAllot per class + rerun (4 ints each)
@@ -274,6 +276,9 @@ int max_batched_groups(ipuma_engine* e) {
   g = std::max(g, batched_grid<LaneS16x2, 8, 16>(e) * 2);
   g = std::max(g, batched_grid<LaneS16x2, 12, 16>(e) * 2);
   g = std::max(g, batched_grid<LaneS16x2, 16, 16>(e) * 2);
+  g = std::max(g, batched_grid<LaneS16x2, 6, 16>(e) * 2);
+  g = std::max(g, batched_grid<LaneS16x2, 10, 16>(e) * 2);
+  g = std::max(g, batched_grid<LaneS16x2, 14, 16>(e) * 2);
   g = std::max(g, batched_grid<LaneS16x2, 12, 32>(e));
   g = std::max(g, batched_grid<LaneS16x2, 16, 32>(e));
   g = std::max(g, batched_grid<LaneS32, 16, 32>(e));
@@ -298,7 +303,7 @@ RunBufs main_bufs(ipuma_engine* e) {
 
 // Brackets one alignment-kernel launch with events when time_launches is set.
 int timed_begin(ipuma_engine* e, cudaStream_t s, int kind, int cls) {
-  if (!e->time_launches || e->n_timed >= 10) return IPUMA_OK;
+  if (!e->time_launches || e->n_timed >= kMaxTimed) return IPUMA_OK;
   if (!e->tev[2 * e->n_timed]) {
     CUDA_TRY(cudaEventCreate(&e->tev[2 * e->n_timed]));
     CUDA_TRY(cudaEventCreate(&e->tev[2 * e->n_timed + 1]));
@@ -310,7 +315,7 @@ int timed_begin(ipuma_engine* e, cudaStream_t s, int kind, int cls) {
 }
 
 int timed_end(ipuma_engine* e, cudaStream_t s) {
-  if (!e->time_launches || e->n_timed >= 10) return IPUMA_OK;
+  if (!e->time_launches || e->n_timed >= kMaxTimed) return IPUMA_OK;
   CUDA_TRY(cudaEventRecord(e->tev[2 * e->n_timed + 1], s));
   e->n_timed++;
   return IPUMA_OK;
@@ -383,6 +388,9 @@ void class_grids(ipuma_engine* e, int maxA, int maxB, int* grid, long long* spb)
       case 4: grid[c] = batched_grid<LaneS16x2, 12, 32>(e); break;
       case 5: grid[c] = batched_grid<LaneS16x2, 16, 32>(e); break;
       case kClsThread: grid[c] = (int)(thread_threads<16>(e) / kThreads); break;
+      case 7: grid[c] = batched_grid<LaneS16x2, 6, 16>(e); break;
+      case 8: grid[c] = batched_grid<LaneS16x2, 10, 16>(e); break;
+      case 9: grid[c] = batched_grid<LaneS16x2, 14, 16>(e); break;
       default: grid[c] = batched_grid<LaneS32, 16, 32>(e); break;
     }
     if (c == kClsThread)
@@ -410,7 +418,7 @@ size_t scratch_int2(ipuma_engine* e, int maxA, int maxB) {
 
 // Launch order of the classes (longest-tail classes first) and, for two
 // alternating streams, the stream (and scratch region) of each.
-constexpr int kLaunchOrder[kNumS16 + 1] = {7, 5, 4, 6, 3, 2, 1, 0};
+constexpr int kLaunchOrder[kNumS16 + 1] = {10, 5, 4, 6, 3, 9, 2, 8, 1, 7, 0};
 
 int reserve_bufs(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, int n, int maxA, int maxB) {
   int rc;
@@ -559,7 +567,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
       return rc;                                                                                       \
     if ((rc = done(cls))) return rc;                                                                   \
   }
-  IPUMA_LAUNCH(LaneS32, 16, 32, 7)
+  IPUMA_LAUNCH(LaneS32, 16, 32, 10)
   IPUMA_LAUNCH(LaneS16x2, 16, 32, 5)
   IPUMA_LAUNCH(LaneS16x2, 12, 32, 4)
   {
@@ -570,8 +578,11 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
     if ((rc = done(kClsThread))) return rc;
   }
   IPUMA_LAUNCH(LaneS16x2, 16, 16, 3)
+  IPUMA_LAUNCH(LaneS16x2, 14, 16, 9)
   IPUMA_LAUNCH(LaneS16x2, 12, 16, 2)
+  IPUMA_LAUNCH(LaneS16x2, 10, 16, 8)
   IPUMA_LAUNCH(LaneS16x2, 8, 16, 1)
+  IPUMA_LAUNCH(LaneS16x2, 6, 16, 7)
   IPUMA_LAUNCH(LaneS16x2, 4, 16, 0)
 #undef IPUMA_LAUNCH
   // Exact 32-bit rerun of the s16x2 pairs whose score may have overflowed
@@ -692,7 +703,7 @@ void set_s32_rates(ipuma_engine* e) {
 
 void set_default_rates(ipuma_engine* e) {
   // Measured on B200 with the nucleic-acid alphabet (uniform related pairs).
-  const float slot[kNumS16] = {0.385f, 0.286f, 0.263f, 0.25f, 0.3125f, 0.3125f, 0.2f};
+  const float slot[kNumS16] = {0.385f, 0.286f, 0.263f, 0.25f, 0.3125f, 0.3125f, 0.3f, 0.33f, 0.27f, 0.25f};
   for (int c = 0; c < kNumS16; ++c) {
     e->slot_ps[c] = slot[c];
     e->strip_ps[c] = 0.f;
@@ -709,7 +720,7 @@ std::string tune_key(const ipuma_engine* e) {
   cudaDeviceProp prop;
   cudaGetDeviceProperties(&prop, e->device);
   char buf[512];
-  snprintf(buf, sizeof(buf), "%s|sm%d%d|M=%d|sim=%d|gI=%d|gE=%d|v3", prop.name, prop.major, prop.minor, e->M,
+  snprintf(buf, sizeof(buf), "%s|sm%d%d|M=%d|sim=%d|gI=%d|gE=%d|v4", prop.name, prop.major, prop.minor, e->M,
            e->sw.similarity, e->sw.gap_init, e->sw.gap_extend);
   for (char* c = buf; *c; ++c)
     if (*c == '\t' || *c == '\n') *c = ' ';
@@ -846,6 +857,9 @@ int run_autotune(ipuma_engine* e, const char* cache_path) {
       case 3: grid = batched_grid<LaneS16x2, 16, 16>(e); break;
       case 4: grid = batched_grid<LaneS16x2, 12, 32>(e); break;
       case 5: grid = batched_grid<LaneS16x2, 16, 32>(e); break;
+      case 7: grid = batched_grid<LaneS16x2, 6, 16>(e); break;
+      case 8: grid = batched_grid<LaneS16x2, 10, 16>(e); break;
+      case 9: grid = batched_grid<LaneS16x2, 14, 16>(e); break;
       default: grid = (int)(thread_threads<16>(e) / kThreads); break;
     }
     const int minPairs = grid * kWarpsPerBlock * perItem * rounds;

@@ -154,24 +154,32 @@ __device__ __forceinline__ bool better(int s1, int i1, int j1, int s2, int i2, i
 }
 
 // -------------------------------------------------------------------------
-// Query profile of one group's strip: prof[x * SW + col] =
-// sim[A[col0 + col]][x] as int8, SW = LANES * K columns.  Row M (the padding
-// letter) and columns past |A| hold SUB_PAD.
+// Query profile of one group's strip: lane l's K columns of letter x at
+// prof[x * LANES * KP + l * KP + c] = sim[A[col0 + l * K + c]][x] as int8,
+// KP = K rounded up to whole 32-bit words (bytes c >= K are unused).  Row M
+// (the padding letter) and columns past |A| hold SUB_PAD.
 // -------------------------------------------------------------------------
+template <int K>
+struct ProfileWords {
+  static constexpr int KP = ((K + 3) / 4) * 4;  // profile bytes per lane
+  static constexpr int W = KP / 4;              // 32-bit words per lane
+};
+
 template <int K, int LANES>
 __device__ __forceinline__ void build_profile(uint8_t* prof, const int8_t* s_simp, int M,
                                               const PassSeq& ps, int col0, int lane) {
   // s_simp[a * (M + 1) + x] = sim[a][x] and SUB_PAD for x == M.
-  constexpr int SW = LANES * K;
-  int acode[K];
+  constexpr int KP = ProfileWords<K>::KP;
+  constexpr int SWP = LANES * KP;
+  int acode[KP];
 #pragma unroll
-  for (int c = 0; c < K; ++c) {
+  for (int c = 0; c < KP; ++c) {
     const int col = col0 + lane * K + c;
-    acode[c] = (col < ps.alen) ? (int)ps.a[(long)col * ps.da] : -1;
+    acode[c] = (c < K && col < ps.alen) ? (int)ps.a[(long)col * ps.da] : -1;
   }
   for (int x = 0; x <= M; ++x) {
 #pragma unroll
-    for (int w = 0; w < K / 4; ++w) {
+    for (int w = 0; w < KP / 4; ++w) {
       uint32_t word = 0;
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
@@ -179,11 +187,12 @@ __device__ __forceinline__ void build_profile(uint8_t* prof, const int8_t* s_sim
         const int v = (a >= 0) ? (int)s_simp[a * (M + 1) + x] : SUB_PAD;
         word |= ((uint32_t)(uint8_t)(int8_t)v) << (8 * q);
       }
-      *reinterpret_cast<uint32_t*>(prof + x * SW + lane * K + 4 * w) = word;
+      *reinterpret_cast<uint32_t*>(prof + x * SWP + lane * KP + 4 * w) = word;
     }
   }
 }
 
+// Loads KB bytes (a multiple of 4) of a profile row into words.
 template <int K>
 __device__ __forceinline__ void load_profile_row(uint32_t (&w)[K / 4], const uint8_t* p) {
   if constexpr (K % 16 == 0) {
@@ -261,11 +270,13 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
                                         uint16_t* s_bring, const PassSeq (&ps)[T::NP], int2* scr,
                                         long rowsCap, Best (&out)[T::NP]) {
   using V = typename T::V;
-  constexpr int SW = LANES * K;
+  constexpr int SW = LANES * K;          // columns per strip
+  constexpr int KP = ProfileWords<K>::KP;
+  constexpr int SWP = LANES * KP;        // profile bytes per letter
   constexpr int NP = T::NP;
   const int lane = threadIdx.x & (LANES - 1);
   const int M = sc.M;
-  const int profStride = (M + 1) * SW;
+  const int profStride = (M + 1) * SWP;
 
   int rowsG = 0, amax = 0;
 #pragma unroll
@@ -293,7 +304,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
   // (Measured on B200: 8 steps for K <= 12, 4 for K = 16; the full LANES
   // steps stalled on instruction fetch.)
   constexpr int kStepUnroll = IPUMA_STEP_UNROLL > 0 ? (IPUMA_STEP_UNROLL < LANES ? IPUMA_STEP_UNROLL : LANES)
-                                                   : (K >= 16 ? 4 : 8);
+                                                   : (K > 12 ? 4 : 8);
 
   for (int strip = 0; strip < nstrips; ++strip) {
     const int col0 = strip * SW;
@@ -364,14 +375,14 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
       diagIn = T::addmax(recvE, vgIgE, recvY);
       const int i = t - lane;
       if (!decltype(check)::value || (i >= 0 && i < rowsG)) {
-        uint32_t wp[K / 4], wq[K / 4];
+        uint32_t wp[KP / 4], wq[KP / 4];
         const uint32_t letters = s_bring[i & 63];
-        load_profile_row<K>(wp, s_prof + (letters & 0xff) * SW + lane * K);
+        load_profile_row<KP>(wp, s_prof + (letters & 0xff) * SWP + lane * KP);
         if constexpr (NP == 2) {
-          load_profile_row<K>(wq, s_prof + profStride + (letters >> 8) * SW + lane * K);
+          load_profile_row<KP>(wq, s_prof + profStride + (letters >> 8) * SWP + lane * KP);
         } else {
 #pragma unroll
-          for (int q = 0; q < K / 4; ++q) wq[q] = 0;
+          for (int q = 0; q < KP / 4; ++q) wq[q] = 0;
         }
         // The left neighbour hands over (Y, Ê) of its last column; lane 0
         // of the first strip starts the row with Y = 0, Ê = -gE.

@@ -61,7 +61,7 @@ struct SmemLayout {
   static constexpr int SW = LANES * K;
   static constexpr int GROUPS = 32 / LANES;
   __host__ __device__ static int simp_bytes(int M) { return ((M * (M + 1)) + 15) & ~15; }
-  __host__ __device__ static int prof_bytes(int M) { return T::NP * (M + 1) * SW; }
+  __host__ __device__ static int prof_bytes(int M) { return T::NP * (M + 1) * LANES * ProfileWords<K>::KP; }
   __host__ __device__ static int ring_bytes() { return 64 * 2; }
   __host__ __device__ static int group_bytes(int M) { return (prof_bytes(M) + ring_bytes() + 15) & ~15; }
   __host__ __device__ static int warp_bytes(int M) { return GROUPS * group_bytes(M); }
@@ -343,7 +343,7 @@ static __global__ void k_exact(SwConst sc, const int8_t* __restrict__ sim, const
 constexpr int NROWB = 256;    // row buckets (16 per power of two)
 constexpr int NSTRIPB = 16;   // strip-count buckets
 constexpr int NBUCKET = NROWB * NSTRIPB;
-constexpr int NCLASS_MAX = 8;
+constexpr int NCLASS_MAX = 11;
 
 // Log-linear bucket of |B| (16 sub-buckets per power of two): pairs that
 // share a bucket differ by at most 1/16 in rows, so the groups of a warp

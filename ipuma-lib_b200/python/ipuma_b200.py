@@ -48,7 +48,9 @@ KERNEL_NAMES = {0: "k_batched<s32,L32,K16>", 1: "k_batched<s16x2,L16,K4>",
                 2: "k_batched<s16x2,L16,K8>", 3: "k_batched<s16x2,L16,K12>",
                 4: "k_batched<s16x2,L16,K16>", 5: "k_batched<s16x2,L32,K12>",
                 6: "k_batched<s16x2,L32,K16>", 7: "k_batched<s32,L32,K16> rerun",
-                8: "k_plain<K>", 9: "k_exact", 10: "k_thread<s16x2,K16>"}
+                8: "k_plain<K>", 9: "k_exact", 10: "k_thread<s16x2,K16>",
+                11: "k_batched<s16x2,L16,K6>", 12: "k_batched<s16x2,L16,K10>",
+                13: "k_batched<s16x2,L16,K14>"}
 
 
 class SwConfig(ctypes.Structure):
@@ -80,8 +82,8 @@ class Stats(ctypes.Structure):
                 ("cells", ctypes.c_int64), ("pairs", ctypes.c_int64),
                 ("s32_pairs", ctypes.c_int64), ("overflow_reruns", ctypes.c_int64),
                 ("launches", ctypes.c_int32), ("used_graph", ctypes.c_int32),
-                ("n_timed", ctypes.c_int32), ("timed_kind", ctypes.c_int32 * 10),
-                ("timed_ms", ctypes.c_double * 10), ("timed_cells", ctypes.c_int64 * 10),
+                ("n_timed", ctypes.c_int32), ("timed_kind", ctypes.c_int32 * 16),
+                ("timed_ms", ctypes.c_double * 16), ("timed_cells", ctypes.c_int64 * 16),
                 ("chunks", ctypes.c_int32)]
 
 

@@ -110,12 +110,12 @@ def test_reference_codelet_answers(fixture, forward_only):
         _assert_same(_gpu(case, forward_only), want, case["name"])
 
 
-@pytest.mark.parametrize("tile_k", [1, 2, 3, 4, 5, 6, 7])
+@pytest.mark.parametrize("tile_k", [1, 2, 3, 4, 5, 6, 7, 8, 9, 10])
 def test_random_answers_each_tile_width(tile_k):
     """Forces every pair through one s16x2 kernel class (16 or 32 lanes per
-    group, 4..16 columns per lane, or 7: one thread per two pairs with
-    16-column strips), so that long pairs cross several strips (global
-    scratch hand-over)."""
+    group, 4..16 columns per lane -- 6, 10 and 14 with word-padded profile
+    rows -- or 7: one thread per two pairs with 16-column strips), so that
+    long pairs cross several strips (global scratch hand-over)."""
     for case in json.load(open(os.path.join(GOLD, "random_ref.json")))["cases"]:
         want = (case["ref"]["score"], case["ref"]["arange"], case["ref"]["brange"])
         _assert_same(_gpu(case, False, tile_k=tile_k), want, "%s class=%d" % (case["name"], tile_k))
@@ -285,7 +285,8 @@ def test_concurrent_class_launches_equal_sequential(forward_only):
 def test_edge_lengths_and_strip_boundaries():
     rng = np.random.default_rng(21)
     A, B = [], []
-    for la in [1, 2, 3, 31, 32, 33, 127, 128, 129, 255, 256, 257, 511, 512, 513, 1023, 1024, 1025]:
+    for la in [1, 2, 3, 31, 32, 33, 95, 96, 97, 127, 128, 129, 159, 160, 161, 223, 224, 225, 255, 256,
+               257, 511, 512, 513, 1023, 1024, 1025]:
         for lb in [1, 2, 17, 63, 64, 65, 300]:
             a = "".join(rng.choice(list("ACGT"), la))
             b = a[: max(1, lb // 2)] + "".join(rng.choice(list("ACGT"), max(0, lb - lb // 2)))
