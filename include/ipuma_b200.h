@@ -110,7 +110,7 @@ typedef struct ipuma_pair {
 } ipuma_pair;
 
 /* Timing and work counters of the last completed call on an engine. */
-#define IPUMA_MAX_TIMED 16  /* launches ipuma_stats can time per call */
+#define IPUMA_MAX_TIMED 24  /* launches ipuma_stats can time per call */
 
 typedef struct ipuma_stats {
   double kernel_ms;     /* device time of the alignment kernels (CUDA events) */
@@ -149,6 +149,12 @@ typedef struct ipuma_stats {
 #define IPUMA_KERNEL_S16_L16_K6 11
 #define IPUMA_KERNEL_S16_L16_K10 12
 #define IPUMA_KERNEL_S16_L16_K14 13
+#define IPUMA_KERNEL_S16_L16_K5 14
+#define IPUMA_KERNEL_S16_L16_K7 15
+#define IPUMA_KERNEL_S16_L16_K9 16
+#define IPUMA_KERNEL_S16_L16_K11 17
+#define IPUMA_KERNEL_S16_L16_K13 18
+#define IPUMA_KERNEL_S16_L16_K15 19
 
 typedef struct ipuma_engine ipuma_engine;
 
@@ -181,7 +187,8 @@ void ipuma_gpu_destroy(ipuma_engine* e);
  *   "tile_k"      0 = kernel class by |A| (default); 1..6 = every pair
  *                 through s16x2 class IPUMA_KERNEL_S16_* (value = kind),
  *                 7 = every pair through IPUMA_KERNEL_S16_T_K16, 8, 9, 10 =
- *                 IPUMA_KERNEL_S16_L16_K6, _K10, _K14
+ *                 IPUMA_KERNEL_S16_L16_K6, _K10, _K14, 11 .. 16 =
+ *                 IPUMA_KERNEL_S16_L16_K5, _K7, _K9, _K11, _K13, _K15
  *   "concurrent"  2 = class launches alternate between two streams, so
  *                 each starts on the SMs the previous one frees (default);
  *                 1 = all classes at once, each on a share of the SMs

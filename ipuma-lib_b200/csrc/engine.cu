@@ -95,13 +95,16 @@ struct DevBuf {
 struct ClassDef {
   int lanes, k, kind, width;
 };
-constexpr int kNumS16 = 10;
+constexpr int kNumS16 = 16;
 constexpr ClassDef kClasses[kNumS16 + 1] = {
     {16, 4, IPUMA_KERNEL_S16_L16_K4, 64},    {16, 8, IPUMA_KERNEL_S16_L16_K8, 128},
     {16, 12, IPUMA_KERNEL_S16_L16_K12, 192}, {16, 16, IPUMA_KERNEL_S16_L16_K16, 256},
     {32, 12, IPUMA_KERNEL_S16_L32_K12, 384}, {32, 16, IPUMA_KERNEL_S16_L32_K16, 512},
     {0, 16, IPUMA_KERNEL_S16_T_K16, 16},     {16, 6, IPUMA_KERNEL_S16_L16_K6, 96},
     {16, 10, IPUMA_KERNEL_S16_L16_K10, 160}, {16, 14, IPUMA_KERNEL_S16_L16_K14, 224},
+    {16, 5, IPUMA_KERNEL_S16_L16_K5, 80},    {16, 7, IPUMA_KERNEL_S16_L16_K7, 112},
+    {16, 9, IPUMA_KERNEL_S16_L16_K9, 144},   {16, 11, IPUMA_KERNEL_S16_L16_K11, 176},
+    {16, 13, IPUMA_KERNEL_S16_L16_K13, 208}, {16, 15, IPUMA_KERNEL_S16_L16_K15, 240},
     {32, 16, IPUMA_KERNEL_S32_K16, 512},
 };
 constexpr int kClsWidest = 5;  // widest wavefront class (very long |A|)
@@ -279,6 +282,12 @@ int max_batched_groups(ipuma_engine* e) {
   g = std::max(g, batched_grid<LaneS16x2, 6, 16>(e) * 2);
   g = std::max(g, batched_grid<LaneS16x2, 10, 16>(e) * 2);
   g = std::max(g, batched_grid<LaneS16x2, 14, 16>(e) * 2);
+  g = std::max(g, batched_grid<LaneS16x2, 5, 16>(e) * 2);
+  g = std::max(g, batched_grid<LaneS16x2, 7, 16>(e) * 2);
+  g = std::max(g, batched_grid<LaneS16x2, 9, 16>(e) * 2);
+  g = std::max(g, batched_grid<LaneS16x2, 11, 16>(e) * 2);
+  g = std::max(g, batched_grid<LaneS16x2, 13, 16>(e) * 2);
+  g = std::max(g, batched_grid<LaneS16x2, 15, 16>(e) * 2);
   g = std::max(g, batched_grid<LaneS16x2, 12, 32>(e));
   g = std::max(g, batched_grid<LaneS16x2, 16, 32>(e));
   g = std::max(g, batched_grid<LaneS32, 16, 32>(e));
@@ -391,6 +400,12 @@ void class_grids(ipuma_engine* e, int maxA, int maxB, int* grid, long long* spb)
       case 7: grid[c] = batched_grid<LaneS16x2, 6, 16>(e); break;
       case 8: grid[c] = batched_grid<LaneS16x2, 10, 16>(e); break;
       case 9: grid[c] = batched_grid<LaneS16x2, 14, 16>(e); break;
+      case 10: grid[c] = batched_grid<LaneS16x2, 5, 16>(e); break;
+      case 11: grid[c] = batched_grid<LaneS16x2, 7, 16>(e); break;
+      case 12: grid[c] = batched_grid<LaneS16x2, 9, 16>(e); break;
+      case 13: grid[c] = batched_grid<LaneS16x2, 11, 16>(e); break;
+      case 14: grid[c] = batched_grid<LaneS16x2, 13, 16>(e); break;
+      case 15: grid[c] = batched_grid<LaneS16x2, 15, 16>(e); break;
       default: grid[c] = batched_grid<LaneS32, 16, 32>(e); break;
     }
     if (c == kClsThread)
@@ -418,7 +433,7 @@ size_t scratch_int2(ipuma_engine* e, int maxA, int maxB) {
 
 // Launch order of the classes (longest-tail classes first) and, for two
 // alternating streams, the stream (and scratch region) of each.
-constexpr int kLaunchOrder[kNumS16 + 1] = {10, 5, 4, 6, 3, 9, 2, 8, 1, 7, 0};
+constexpr int kLaunchOrder[kNumS16 + 1] = {16, 5, 4, 6, 3, 15, 9, 14, 2, 13, 8, 12, 1, 11, 7, 10, 0};
 
 int reserve_bufs(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, int n, int maxA, int maxB) {
   int rc;
@@ -567,7 +582,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
       return rc;                                                                                       \
     if ((rc = done(cls))) return rc;                                                                   \
   }
-  IPUMA_LAUNCH(LaneS32, 16, 32, 10)
+  IPUMA_LAUNCH(LaneS32, 16, 32, 16)
   IPUMA_LAUNCH(LaneS16x2, 16, 32, 5)
   IPUMA_LAUNCH(LaneS16x2, 12, 32, 4)
   {
@@ -578,11 +593,17 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
     if ((rc = done(kClsThread))) return rc;
   }
   IPUMA_LAUNCH(LaneS16x2, 16, 16, 3)
+  IPUMA_LAUNCH(LaneS16x2, 15, 16, 15)
   IPUMA_LAUNCH(LaneS16x2, 14, 16, 9)
+  IPUMA_LAUNCH(LaneS16x2, 13, 16, 14)
   IPUMA_LAUNCH(LaneS16x2, 12, 16, 2)
+  IPUMA_LAUNCH(LaneS16x2, 11, 16, 13)
   IPUMA_LAUNCH(LaneS16x2, 10, 16, 8)
+  IPUMA_LAUNCH(LaneS16x2, 9, 16, 12)
   IPUMA_LAUNCH(LaneS16x2, 8, 16, 1)
+  IPUMA_LAUNCH(LaneS16x2, 7, 16, 11)
   IPUMA_LAUNCH(LaneS16x2, 6, 16, 7)
+  IPUMA_LAUNCH(LaneS16x2, 5, 16, 10)
   IPUMA_LAUNCH(LaneS16x2, 4, 16, 0)
 #undef IPUMA_LAUNCH
   // Exact 32-bit rerun of the s16x2 pairs whose score may have overflowed
@@ -703,7 +724,8 @@ void set_s32_rates(ipuma_engine* e) {
 
 void set_default_rates(ipuma_engine* e) {
   // Measured on B200 with the nucleic-acid alphabet (uniform related pairs).
-  const float slot[kNumS16] = {0.385f, 0.286f, 0.263f, 0.25f, 0.3125f, 0.3125f, 0.3f, 0.33f, 0.27f, 0.25f};
+  const float slot[kNumS16] = {0.385f, 0.286f, 0.263f, 0.25f, 0.3125f, 0.3125f, 0.3f, 0.33f,
+                               0.27f,  0.25f,  0.36f,  0.31f, 0.28f,   0.26f,   0.25f, 0.25f};
   for (int c = 0; c < kNumS16; ++c) {
     e->slot_ps[c] = slot[c];
     e->strip_ps[c] = 0.f;
@@ -720,7 +742,7 @@ std::string tune_key(const ipuma_engine* e) {
   cudaDeviceProp prop;
   cudaGetDeviceProperties(&prop, e->device);
   char buf[512];
-  snprintf(buf, sizeof(buf), "%s|sm%d%d|M=%d|sim=%d|gI=%d|gE=%d|v4", prop.name, prop.major, prop.minor, e->M,
+  snprintf(buf, sizeof(buf), "%s|sm%d%d|M=%d|sim=%d|gI=%d|gE=%d|v5", prop.name, prop.major, prop.minor, e->M,
            e->sw.similarity, e->sw.gap_init, e->sw.gap_extend);
   for (char* c = buf; *c; ++c)
     if (*c == '\t' || *c == '\n') *c = ' ';
@@ -860,6 +882,12 @@ int run_autotune(ipuma_engine* e, const char* cache_path) {
       case 7: grid = batched_grid<LaneS16x2, 6, 16>(e); break;
       case 8: grid = batched_grid<LaneS16x2, 10, 16>(e); break;
       case 9: grid = batched_grid<LaneS16x2, 14, 16>(e); break;
+      case 10: grid = batched_grid<LaneS16x2, 5, 16>(e); break;
+      case 11: grid = batched_grid<LaneS16x2, 7, 16>(e); break;
+      case 12: grid = batched_grid<LaneS16x2, 9, 16>(e); break;
+      case 13: grid = batched_grid<LaneS16x2, 11, 16>(e); break;
+      case 14: grid = batched_grid<LaneS16x2, 13, 16>(e); break;
+      case 15: grid = batched_grid<LaneS16x2, 15, 16>(e); break;
       default: grid = (int)(thread_threads<16>(e) / kThreads); break;
     }
     const int minPairs = grid * kWarpsPerBlock * perItem * rounds;

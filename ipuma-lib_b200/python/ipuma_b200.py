@@ -50,7 +50,11 @@ KERNEL_NAMES = {0: "k_batched<s32,L32,K16>", 1: "k_batched<s16x2,L16,K4>",
                 6: "k_batched<s16x2,L32,K16>", 7: "k_batched<s32,L32,K16> rerun",
                 8: "k_plain<K>", 9: "k_exact", 10: "k_thread<s16x2,K16>",
                 11: "k_batched<s16x2,L16,K6>", 12: "k_batched<s16x2,L16,K10>",
-                13: "k_batched<s16x2,L16,K14>"}
+                13: "k_batched<s16x2,L16,K14>", 14: "k_batched<s16x2,L16,K5>",
+                15: "k_batched<s16x2,L16,K7>", 16: "k_batched<s16x2,L16,K9>",
+                17: "k_batched<s16x2,L16,K11>", 18: "k_batched<s16x2,L16,K13>",
+                19: "k_batched<s16x2,L16,K15>"}
+MAX_TIMED = 24  # IPUMA_MAX_TIMED
 
 
 class SwConfig(ctypes.Structure):
@@ -82,8 +86,8 @@ class Stats(ctypes.Structure):
                 ("cells", ctypes.c_int64), ("pairs", ctypes.c_int64),
                 ("s32_pairs", ctypes.c_int64), ("overflow_reruns", ctypes.c_int64),
                 ("launches", ctypes.c_int32), ("used_graph", ctypes.c_int32),
-                ("n_timed", ctypes.c_int32), ("timed_kind", ctypes.c_int32 * 16),
-                ("timed_ms", ctypes.c_double * 16), ("timed_cells", ctypes.c_int64 * 16),
+                ("n_timed", ctypes.c_int32), ("timed_kind", ctypes.c_int32 * MAX_TIMED),
+                ("timed_ms", ctypes.c_double * MAX_TIMED), ("timed_cells", ctypes.c_int64 * MAX_TIMED),
                 ("chunks", ctypes.c_int32)]
 
 

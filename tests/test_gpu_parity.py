@@ -110,12 +110,13 @@ def test_reference_codelet_answers(fixture, forward_only):
         _assert_same(_gpu(case, forward_only), want, case["name"])
 
 
-@pytest.mark.parametrize("tile_k", [1, 2, 3, 4, 5, 6, 7, 8, 9, 10])
+@pytest.mark.parametrize("tile_k", list(range(1, 17)))
 def test_random_answers_each_tile_width(tile_k):
     """Forces every pair through one s16x2 kernel class (16 or 32 lanes per
-    group, 4..16 columns per lane -- 6, 10 and 14 with word-padded profile
-    rows -- or 7: one thread per two pairs with 16-column strips), so that
-    long pairs cross several strips (global scratch hand-over)."""
+    group, 4..16 columns per lane -- widths that are not whole words use
+    word-padded profile rows -- or 7: one thread per two pairs with
+    16-column strips), so that long pairs cross several strips (global
+    scratch hand-over)."""
     for case in json.load(open(os.path.join(GOLD, "random_ref.json")))["cases"]:
         want = (case["ref"]["score"], case["ref"]["arange"], case["ref"]["brange"])
         _assert_same(_gpu(case, False, tile_k=tile_k), want, "%s class=%d" % (case["name"], tile_k))
