@@ -511,6 +511,12 @@ def main():
                "timing": "host wall clock around ipuma_gpu_compare (validation, H2D, kernels, D2H; "
                          "uploads of later chunks overlap the kernels of earlier ones)"}
 
+    # DRAM bytes per forward-pass cell of the dominant launch, from the ncu
+    # capture of k_batched<s16x2,L16,K15> on 300,000 pairs of this workload
+    # (profiles/k_batched_s16x2_L16_K15_dna_300k.md: 24.61 MB / 2.2408 G
+    # cells); a launch's traffic is the codes of its pairs, so it scales
+    # with its cells.
+    traffic_per_cell = {"dna_batched": 0.01098}.get(args.workload)
     peaks, peak_src = measured_peaks()
     int_peak = ib.measure_int_peak(local)
     rl = None
@@ -521,7 +527,8 @@ def main():
               "peak": int_peak / 1e9, "unit": "G int lane-ops/s", "frac": achieved * 1e9 / int_peak,
               "per_unit": "%d lane-ops per cell; %d cells in this launch" % (LANE_OPS_PER_CELL, dcells),
               "launch_ms": dms, "peak_source": "ipuma_measure_int_peak (s16x2 DPX mix, this GPU)",
-              "traffic": None}
+              "traffic": (dcells * traffic_per_cell) if traffic_per_cell else None,
+              "traffic_unit": "bytes per launch (ncu dram__bytes_read+write per cell x launch cells)"}
     algo_bytes = algorithmic_bytes(wl)
     roof_hbm = {"bound": "hbm", "achieved": algo_bytes / (ms_step * 1e-3) / 1e9,
                 "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
