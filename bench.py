@@ -39,7 +39,7 @@ LANE_OPS_PER_CELL = 7  # E: 2, F: 2, H: 2, running max: 1 (int lane-ops)
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="dna_batched",
@@ -110,9 +110,27 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
-    def stop(self):
+    def wait_first(self, timeout_s=5.0):
+        """Blocks until nvidia-smi printed its first sample (its start-up
+        takes longer than a short timed region)."""
+        t0 = time.perf_counter()
+        while self.proc is not None and not self.lines and time.perf_counter() - t0 < timeout_s:
+            time.sleep(0.01)
+
+    def mark(self):
+        """Index of the next sample: samples from here on are taken during
+        the timed region."""
+        return len(self.lines)
+
+    def stop(self, first=0, last=None):
+        """Stops sampling; summarises samples [first, last) (the timed
+        region), plus the one sample that straddles its end."""
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        if last is None:
+            last = len(self.lines)
+        time.sleep(0.12)  # the sample covering the end of the region
+        self.lines = self.lines[first:last + 1]
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -408,14 +426,16 @@ def main():
         dist.barrier()
     clocks = ClockSampler(local)
     clocks.start()
+    clocks.wait_first()
     torch.cuda.synchronize()
+    clk_first = clocks.mark()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
         step()
     ev1.record(stream)
     torch.cuda.synchronize()
-    clk = clocks.stop()
+    clk = clocks.stop(clk_first, clocks.mark())
     ms = max_over_ranks(dist, ev0.elapsed_time(ev1), dev)
     ms_step = ms / args.steps
     total_cells = wl.cells * ws

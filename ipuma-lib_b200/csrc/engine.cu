@@ -121,10 +121,20 @@ constexpr float kThrLatencyShare = 0.5f;
 constexpr float kLatencyShare = 0.25f;
 constexpr float kPackingEfficiency = 0.85f;
 constexpr float kLatencyMinBatchPs = 1.0e9f;
+// The 16-lane classes at 16-column steps (every K from 4 to 16) cut column
+// padding on large batches; a smaller batch uses the 64-column steps only
+// (K = 4, 8, 12, 16), since every class launch costs a few microseconds
+// even when empty.
+constexpr int kFineClassMinPairs = 150000;
+constexpr unsigned kCoarseClasses = (1u << 0) | (1u << 1) | (1u << 2) | (1u << 3) | (1u << 4) | (1u << 5);
+constexpr unsigned kFineClasses = (1u << 7) | (1u << 8) | (1u << 9) | (1u << 10) | (1u << 11) | (1u << 12) |
+                                  (1u << 13) | (1u << 14) | (1u << 15);
 constexpr int kWarpsPerBlock = 4;
 // Chunked upload/compute overlap of ipuma_gpu_compare.
 constexpr int kMaxChunks = 8;
-constexpr int kChunkMinPairs = 65536;         // automatic chunks hold at least this many pairs
+constexpr int kChunkMinPairs = 250000;        // automatic chunks hold at least this many pairs
+constexpr int kValidateMaxThreads = 8;        // host threads checking pair descriptors
+constexpr int kValidatePairsPerThread = 131072;
 constexpr size_t kChunkMinBytes = 32u << 20;  // and the batch uploads at least this much
 constexpr int kThreads = 32 * kWarpsPerBlock;
 
@@ -506,6 +516,12 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   const int mode = e->time_launches ? 0 : e->concurrent;
   const bool conc = mode != 0;
   bp.concurrent = mode;
+  // Classes this batch may use (the others are not launched).
+  unsigned enabled = kCoarseClasses | (1u << kClsS32);
+  if (n >= kFineClassMinPairs) enabled |= kFineClasses;
+  if (e->thread_class) enabled |= 1u << kClsThread;
+  if (e->tile_k > 0) enabled |= 1u << (e->tile_k - 1);
+  bp.enabled = enabled;
   class_grids(e, maxA, maxB, bp.grid, bp.scr_per_block);
   bp.scr_cap = (long long)(rb.scratch->cap / sizeof(int2));
   float slot_min = 1e30f;
@@ -520,7 +536,13 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   bp.lat_min_ps = kLatencyMinBatchPs;
   bp.region = 0;
   for (int c = 0; c <= kNumS16; ++c) bp.region = std::max(bp.region, (long long)bp.grid[c] * bp.scr_per_block[c]);
-  for (int k = 0; k <= kNumS16; ++k) bp.slot_of[kLaunchOrder[k]] = k & 1;
+  // Two alternating streams: stream (and scratch region) by position
+  // among the launched classes.
+  for (int k = 0, pos = 0; k <= kNumS16; ++k) {
+    const int c = kLaunchOrder[k];
+    bp.slot_of[c] = pos & 1;
+    if ((enabled >> c) & 1u) ++pos;
+  }
   bp.long_a = e->long_a;
   // tile_k > 0 forces one s16x2 class: every pair uses the chosen kernel,
   // long A crossing several strips.
@@ -575,22 +597,24 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   };
   const int* R = ctl + CTL_RANGES;
 #define IPUMA_LAUNCH(T, K, L, cls)                                                                     \
-  {                                                                                                    \
+  if ((enabled >> (cls)) & 1u) {                                                                       \
     cudaStream_t cs = on(cls);                                                                         \
     if ((rc = launch_batched<T, K, L>(e, rb, cs, codes, pairs, list, R + 2 * (cls), heads + (cls),     \
                                       rowsCap, score, arange, brange, kClasses[cls].kind, cls, cls)))  \
       return rc;                                                                                       \
     if ((rc = done(cls))) return rc;                                                                   \
+    ++*launches;                                                                                       \
   }
   IPUMA_LAUNCH(LaneS32, 16, 32, 16)
   IPUMA_LAUNCH(LaneS16x2, 16, 32, 5)
   IPUMA_LAUNCH(LaneS16x2, 12, 32, 4)
-  {
+  if ((enabled >> kClsThread) & 1u) {
     cudaStream_t cs = on(kClsThread);
     if ((rc = launch_thread<16>(e, rb, cs, codes, pairs, list, R + 2 * kClsThread, heads + kClsThread,
                                 thread_rows(e, maxA, maxB), score, arange, brange, kClsThread)))
       return rc;
     if ((rc = done(kClsThread))) return rc;
+    ++*launches;
   }
   IPUMA_LAUNCH(LaneS16x2, 16, 16, 3)
   IPUMA_LAUNCH(LaneS16x2, 15, 16, 15)
@@ -612,7 +636,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
                                             heads + NCLASS_MAX, rowsCap, score, arange, brange,
                                             IPUMA_KERNEL_S32_RERUN, CELLS_RERUN, NCLASS_MAX)))
     return rc;
-  *launches += kNumS16 + 2;
+  *launches += 1;
   return IPUMA_OK;
 }
 
@@ -973,6 +997,39 @@ int chunk_count(const ipuma_engine* e, int32_t n, size_t n_codes) {
   return std::min(kMaxChunks, n / kChunkMinPairs);
 }
 
+// Bounds check of pairs [lo, hi) (the kernels trust the descriptors), with
+// their maxima, cells and the code ranges each chunk's pairs read.
+struct PairScan {
+  int32_t bad = -1;  // first pair outside the code array
+  int maxA = 0, maxB = 0;
+  int64_t cells = 0;
+  ChunkSpan span[kMaxChunks];
+};
+
+void scan_pairs(const ipuma_pair* pairs, size_t n_codes, int32_t lo, int32_t hi, const int32_t* cbeg,
+                int nch, PairScan& r) {
+  int k = 0;
+  while (k + 1 < nch && cbeg[k + 1] <= lo) ++k;
+  for (int32_t p = lo; p < hi; ++p) {
+    while (p >= cbeg[k + 1]) ++k;
+    const ipuma_pair& d = pairs[p];
+    if (d.a_len < 0 || d.b_len < 0 || d.a_off < 0 || d.b_off < 0 ||
+        (size_t)d.a_off + (size_t)d.a_len > n_codes || (size_t)d.b_off + (size_t)d.b_len > n_codes) {
+      r.bad = p;
+      return;
+    }
+    r.maxA = std::max(r.maxA, d.a_len);
+    r.maxB = std::max(r.maxB, d.b_len);
+    r.cells += (int64_t)d.a_len * d.b_len;
+    if (d.a_len == 0 || d.b_len == 0) continue;
+    ChunkSpan& sp = r.span[k];
+    sp.lo[0] = std::min(sp.lo[0], (size_t)d.a_off);
+    sp.hi[0] = std::max(sp.hi[0], (size_t)d.a_off + (size_t)d.a_len);
+    sp.lo[1] = std::min(sp.lo[1], (size_t)d.b_off);
+    sp.hi[1] = std::max(sp.hi[1], (size_t)d.b_off + (size_t)d.b_len);
+  }
+}
+
 bool is_pinned(const void* p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -1240,7 +1297,8 @@ int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_c
                                        (uint64_t)(uintptr_t)e->d_scratch.p, (uint64_t)e->d_scratch.cap,
                                        (uint64_t)(uintptr_t)e->d_list.p, (uint64_t)(uintptr_t)e->d_ctl.p,
                                        (uint64_t)(uintptr_t)e->d_ovf.p, (uint64_t)(uintptr_t)e->d_flag.p,
-                                       (uint64_t)e->tile_k, (uint64_t)e->long_a};
+                                       (uint64_t)e->tile_k, (uint64_t)e->long_a, (uint64_t)e->thread_class,
+                                       (uint64_t)e->concurrent};
     auto it = e->graphs_cache.find(key);
     if (it == e->graphs_cache.end()) {
       if (e->graphs_cache.size() >= 16) {
@@ -1297,28 +1355,34 @@ int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes, con
   std::lock_guard<std::mutex> lk(e->mu);
   const int nch = e->time_launches ? 1 : chunk_count(e, n, n_codes);
   // Host-side bounds check of every pair (the kernels trust the
-  // descriptors), with the code ranges each chunk of pairs reads.
+  // descriptors), with the code ranges each chunk of pairs reads; large
+  // batches are checked on several threads.
+  int32_t cbeg[kMaxChunks + 1];
+  for (int k = 0; k <= nch; ++k) cbeg[k] = (int32_t)((int64_t)n * k / nch);
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int nthr = std::max(1, std::min({kValidateMaxThreads, hw, n / kValidatePairsPerThread}));
+  std::vector<PairScan> part(nthr);
+  {
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nthr; ++t)
+      pool.emplace_back(scan_pairs, pairs, n_codes, (int32_t)((int64_t)n * t / nthr),
+                        (int32_t)((int64_t)n * (t + 1) / nthr), cbeg, nch, std::ref(part[t]));
+    scan_pairs(pairs, n_codes, 0, (int32_t)((int64_t)n / nthr), cbeg, nch, part[0]);
+    for (auto& th : pool) th.join();
+  }
   int maxA = 0, maxB = 0;
   int64_t cells = 0;
   ChunkSpan span[kMaxChunks];
-  int32_t cbeg[kMaxChunks + 1];
-  for (int k = 0; k <= nch; ++k) cbeg[k] = (int32_t)((int64_t)n * k / nch);
-  for (int k = 0; k < nch; ++k) {
-    ChunkSpan& sp = span[k];
-    for (int32_t p = cbeg[k]; p < cbeg[k + 1]; ++p) {
-      const ipuma_pair& d = pairs[p];
-      if (d.a_len < 0 || d.b_len < 0 || d.a_off < 0 || d.b_off < 0 ||
-          (size_t)d.a_off + (size_t)d.a_len > n_codes || (size_t)d.b_off + (size_t)d.b_len > n_codes)
-        return fail(IPUMA_ERR_INVALID_ARG, "pair %d lies outside the code array", p);
-      maxA = std::max(maxA, d.a_len);
-      maxB = std::max(maxB, d.b_len);
-      cells += (int64_t)d.a_len * d.b_len;
-      if (d.a_len == 0 || d.b_len == 0) continue;
-      sp.lo[0] = std::min(sp.lo[0], (size_t)d.a_off);
-      sp.hi[0] = std::max(sp.hi[0], (size_t)d.a_off + (size_t)d.a_len);
-      sp.lo[1] = std::min(sp.lo[1], (size_t)d.b_off);
-      sp.hi[1] = std::max(sp.hi[1], (size_t)d.b_off + (size_t)d.b_len);
-    }
+  for (const PairScan& r : part) {
+    if (r.bad >= 0) return fail(IPUMA_ERR_INVALID_ARG, "pair %d lies outside the code array", r.bad);
+    maxA = std::max(maxA, r.maxA);
+    maxB = std::max(maxB, r.maxB);
+    cells += r.cells;
+    for (int k = 0; k < nch; ++k)
+      for (int q = 0; q < 2; ++q) {
+        span[k].lo[q] = std::min(span[k].lo[q], r.span[k].lo[q]);
+        span[k].hi[q] = std::max(span[k].hi[q], r.span[k].hi[q]);
+      }
   }
   if (maxA > 65535 || maxB > 65535)
     return fail(IPUMA_ERR_TOO_LONG, "sequence longer than 65535 (ranges are uint16)");

@@ -388,6 +388,7 @@ struct BinParams {
   // Concurrent class launches (k_bin_scan turns modelled costs into block
   // shares): full-occupancy grid and strip scratch (int2) per block of
   // each class, and the scratch available.
+  unsigned int enabled;    // bit c: class c may be chosen by cost (and is launched)
   int concurrent;          // 0 sequential, 1 shares, 2 two alternating streams
   int slot_of[NCLASS_MAX + 1];  // mode 2: scratch region (0 / 1) of each class
   long long region;             // mode 2: int2 per region
@@ -447,6 +448,7 @@ __device__ __forceinline__ int pair_key(const BinParams& bp, int alen, int blen,
     const float batch_ps = bp.total_cells ? (float)(*bp.total_cells) * bp.batch_ps_per_cell : 0.f;
     const float lat_cap = batch_ps >= bp.lat_min_ps ? bp.lat_share * batch_ps : 3.0e38f;
     for (int c = 0; c < bp.n_s16_classes; ++c) {
+      if (!((bp.enabled >> c) & 1u)) continue;
       if (c == bp.thr_cls && !thr_ok) continue;
       const int strips = (alen + bp.width[c] - 1) / bp.width[c];
       const float lat = (float)strips * (float)(blen + bp.lanes[c]) * bp.step_ps[c];

@@ -114,8 +114,9 @@ def test_chunked_into_pinned_buffers():
 
 
 def test_automatic_chunking_of_a_large_batch():
-    """Above 131,072 pairs and 32 MB of codes the call chunks by itself."""
-    wl = workloads.dna_batched(n=140_000, seed=45)
+    """From 500,000 pairs and 32 MB of codes the call chunks by itself (one
+    chunk per 250,000 pairs); the pairs are checked on several host threads."""
+    wl = workloads.dna_batched(n=520_000, seed=45)
     pairs = ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len)
     assert wl.codes.size >= 32 << 20
     auto, st = _run(wl, wl.codes, pairs, True, 0)
@@ -125,3 +126,20 @@ def test_automatic_chunking_of_a_large_batch():
     _same(auto, single, "auto vs single")
     idx = np.random.default_rng(0).choice(wl.n, 2_000, replace=False)
     _same(tuple(a[idx] for a in auto), _oracle(wl, wl.codes, pairs, True, idx), "auto sample")
+
+
+def test_bad_pair_deep_in_a_large_batch_is_reported():
+    """The threaded host check reports the first pair outside the code array,
+    whichever thread finds it, and the engine stays usable."""
+    wl = workloads.dna_batched(n=400_000, seed=46)
+    pairs = ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len)
+    pairs["b_off"][301_234] = wl.codes.size - 3
+    pairs["b_off"][350_000] = wl.codes.size + 10
+    with _engine(wl, True) as e:
+        with pytest.raises(ib.IpumaError) as ei:
+            e.compare(wl.codes, pairs)
+        assert ei.value.code == ib.ERR_INVALID_ARG
+        assert "301234" in str(ei.value)
+        small = pairs[:1000].copy()
+        got = e.compare(wl.codes, small)
+        _same(got, _oracle(wl, wl.codes, small, True), "after a rejected call")
