@@ -189,11 +189,12 @@ void ipuma_gpu_destroy(ipuma_engine* e);
  *                 7 = every pair through IPUMA_KERNEL_S16_T_K16, 8, 9, 10 =
  *                 IPUMA_KERNEL_S16_L16_K6, _K10, _K14, 11 .. 16 =
  *                 IPUMA_KERNEL_S16_L16_K5, _K7, _K9, _K11, _K13, _K15
- *   "concurrent"  2 = class launches alternate between two streams, so
- *                 each starts on the SMs the previous one frees (default);
- *                 1 = all classes at once, each on a share of the SMs
- *                 proportional to its modelled work; 0 = one launch after
- *                 the other (always the case with time_launches)
+ *   "concurrent"  3 = by batch size (default): mode 1 below 48,000 pairs,
+ *                 mode 2 above; 2 = class launches alternate between two
+ *                 streams, so each starts on the SMs the previous one
+ *                 frees; 1 = all classes at once, each on a share of the
+ *                 SMs proportional to its modelled work; 0 = one launch
+ *                 after the other (always the case with time_launches)
  *   "thread_class" 1 = the per-thread class IPUMA_KERNEL_S16_T_K16 may be
  *                 chosen for pairs that are small relative to the batch,
  *                 0 = never (default) unless tile_k forces it

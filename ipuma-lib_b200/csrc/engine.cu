@@ -117,10 +117,17 @@ constexpr int kThrMaxRows = 2048;
 constexpr float kThrLatencyShare = 0.5f;
 // Latency bound of every class (BinParams::lat_share): an item may take at
 // most this share of the batch's modelled time (cells x fastest slot time
-// / packing efficiency), for batches of at least 1 ms.
+// / packing efficiency).  In small batches that sends pairs to the class
+// that finishes them soonest: there one long pair, not throughput, sets the
+// batch's time.
 constexpr float kLatencyShare = 0.25f;
 constexpr float kPackingEfficiency = 0.85f;
-constexpr float kLatencyMinBatchPs = 1.0e9f;
+constexpr float kLatencyMinBatchPs = 0.f;
+// Option "concurrent" = 3 (default) picks the launch mode by batch size:
+// smaller batches leave most class launches with fewer items than resident
+// warps, so the classes share the SMs (mode 1); larger ones alternate two
+// streams (mode 2), which keeps one class per SM.
+constexpr int kShareModeMaxPairs = 48000;
 // The 16-lane classes at 16-column steps (every K from 4 to 16) cut column
 // padding on large batches; a smaller batch uses the 64-column steps only
 // (K = 4, 8, 12, 16), since every class launch costs a few microseconds
@@ -193,7 +200,7 @@ struct ipuma_engine {
   cudaStream_t cls_stream[NCLASS_MAX] = {};
   cudaEvent_t fork_ev = nullptr;
   cudaEvent_t join_ev[NCLASS_MAX] = {};
-  int concurrent = 2;
+  int concurrent = 3;
   cudaStream_t stream2 = nullptr, copy_stream = nullptr;
   cudaEvent_t cev[2 * kMaxChunks + 2] = {};
   int chunks = 0;  // option "chunks": 0 automatic, 1 off, n fixed
@@ -513,7 +520,9 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   bp.thr_cap_scale = kThrLatencyShare / (2.0f * (float)thrThreads);
   bp.total_cells = reinterpret_cast<const unsigned long long*>(ctl + CTL_CELLS) + CELLS_TOTAL;
   // Concurrent class launches, except when every launch is timed alone.
-  const int mode = e->time_launches ? 0 : e->concurrent;
+  const int mode = e->time_launches ? 0
+                   : e->concurrent == 3 ? (n < kShareModeMaxPairs ? 1 : 2)
+                                        : e->concurrent;
   const bool conc = mode != 0;
   bp.concurrent = mode;
   // Classes this batch may use (the others are not launched).
@@ -1213,7 +1222,7 @@ int ipuma_gpu_set_option(ipuma_engine* e, const char* name, int64_t value) {
   } else if (k == "time_launches") {
     e->time_launches = value ? 1 : 0;
   } else if (k == "concurrent") {
-    if (value < 0 || value > 2) return fail(IPUMA_ERR_INVALID_ARG, "concurrent must be 0, 1 or 2");
+    if (value < 0 || value > 3) return fail(IPUMA_ERR_INVALID_ARG, "concurrent must be 0, 1, 2 or 3");
     e->concurrent = (int)value;
   } else if (k == "thread_class") {
     e->thread_class = value ? 1 : 0;
