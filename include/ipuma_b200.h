@@ -155,6 +155,7 @@ typedef struct ipuma_stats {
 #define IPUMA_KERNEL_S16_L16_K11 17
 #define IPUMA_KERNEL_S16_L16_K13 18
 #define IPUMA_KERNEL_S16_L16_K15 19
+#define IPUMA_KERNEL_S16_HYBRID 20 /* s16x2 strips while safe, then s32 (high scores) */
 
 typedef struct ipuma_engine ipuma_engine;
 
@@ -195,6 +196,12 @@ void ipuma_gpu_destroy(ipuma_engine* e);
  *                 frees; 1 = all classes at once, each on a share of the
  *                 SMs proportional to its modelled work; 0 = one launch
  *                 after the other (always the case with time_launches)
+ *   "latency_share" share of the batch's modelled time (per mille,
+ *                 default 60) one pair's item may take in its class; a
+ *                 pair over it takes a class that finishes it sooner
+ *   "hybrid"      1 = pairs whose score can pass int16 run their strips in
+ *                 s16x2 while a strip's values provably fit, then in s32
+ *                 (IPUMA_KERNEL_S16_HYBRID, default); 0 = all in s32
  *   "thread_class" 1 = the per-thread class IPUMA_KERNEL_S16_T_K16 may be
  *                 chosen for pairs that are small relative to the batch,
  *                 0 = never (default) unless tile_k forces it

@@ -95,8 +95,9 @@ struct DevBuf {
 struct ClassDef {
   int lanes, k, kind, width;
 };
-constexpr int kNumS16 = 16;
-constexpr ClassDef kClasses[kNumS16 + 1] = {
+constexpr int kNumS16 = 16;     // s16x2 classes chosen by cost
+constexpr int kNumClasses = kNumS16 + 2;  // + the s32 class + the hybrid class
+constexpr ClassDef kClasses[kNumClasses] = {
     {16, 4, IPUMA_KERNEL_S16_L16_K4, 64},    {16, 8, IPUMA_KERNEL_S16_L16_K8, 128},
     {16, 12, IPUMA_KERNEL_S16_L16_K12, 192}, {16, 16, IPUMA_KERNEL_S16_L16_K16, 256},
     {32, 12, IPUMA_KERNEL_S16_L32_K12, 384}, {32, 16, IPUMA_KERNEL_S16_L32_K16, 512},
@@ -105,12 +106,15 @@ constexpr ClassDef kClasses[kNumS16 + 1] = {
     {16, 5, IPUMA_KERNEL_S16_L16_K5, 80},    {16, 7, IPUMA_KERNEL_S16_L16_K7, 112},
     {16, 9, IPUMA_KERNEL_S16_L16_K9, 144},   {16, 11, IPUMA_KERNEL_S16_L16_K11, 176},
     {16, 13, IPUMA_KERNEL_S16_L16_K13, 208}, {16, 15, IPUMA_KERNEL_S16_L16_K15, 240},
-    {32, 16, IPUMA_KERNEL_S32_K16, 512},
+    {32, 16, IPUMA_KERNEL_S32_K16, 512},     {32, 16, IPUMA_KERNEL_S16_HYBRID, 512},
 };
 constexpr int kClsWidest = 5;  // widest wavefront class (very long |A|)
 constexpr int kMaxTimed = IPUMA_MAX_TIMED;  // launches timed per call (time_launches)
 constexpr int kClsThread = 6;  // per-thread class k_thread<16>
 constexpr int kClsS32 = kNumS16;
+// Hybrid class: pairs whose score can pass int16 (main-diagonal bound) run
+// their safe strips in s16x2 and the rest in s32 (option "hybrid").
+constexpr int kClsHi = kNumS16 + 1;
 // Per-thread class: rows it accepts (its boundary scratch is rows x threads)
 // and the share of the batch's time one of its pairs may take.
 constexpr int kThrMaxRows = 2048;
@@ -120,7 +124,7 @@ constexpr float kThrLatencyShare = 0.5f;
 // / packing efficiency).  In small batches that sends pairs to the class
 // that finishes them soonest: there one long pair, not throughput, sets the
 // batch's time.
-constexpr float kLatencyShare = 0.25f;
+constexpr float kLatencyShare = 0.06f;  // measured best of 0.03-0.25 on the protein workloads
 constexpr float kPackingEfficiency = 0.85f;
 constexpr float kLatencyMinBatchPs = 0.f;
 // Option "concurrent" = 3 (default) picks the launch mode by batch size:
@@ -201,6 +205,8 @@ struct ipuma_engine {
   cudaEvent_t fork_ev = nullptr;
   cudaEvent_t join_ev[NCLASS_MAX] = {};
   int concurrent = 3;
+  int hybrid = 1;  // option "hybrid": high-scoring pairs run s16x2 strips while provably safe
+  float latency_share = kLatencyShare;  // option "latency_share" (per mille)
   cudaStream_t stream2 = nullptr, copy_stream = nullptr;
   cudaEvent_t cev[2 * kMaxChunks + 2] = {};
   int chunks = 0;  // option "chunks": 0 automatic, 1 off, n fixed
@@ -272,10 +278,10 @@ int smem_for(const ipuma_engine* e) {
   return SmemLayout<T, K, LANES>::total(e->M, kWarpsPerBlock);
 }
 
-// Grid of a k_batched<T, K, LANES> launch.
-template <class T, int K, int LANES>
+// Grid of a k_batched<T, K, LANES, HYB> launch.
+template <class T, int K, int LANES, bool HYB = false>
 int batched_grid(ipuma_engine* e) {
-  return occupancy_grid(e, k_batched<T, K, LANES>, smem_for<T, K, LANES>(e));
+  return occupancy_grid(e, k_batched<T, K, LANES, HYB>, smem_for<T, K, LANES>(e));
 }
 
 template <int K>
@@ -308,6 +314,7 @@ int max_batched_groups(ipuma_engine* e) {
   g = std::max(g, batched_grid<LaneS16x2, 12, 32>(e));
   g = std::max(g, batched_grid<LaneS16x2, 16, 32>(e));
   g = std::max(g, batched_grid<LaneS32, 16, 32>(e));
+  g = std::max(g, batched_grid<LaneS16x2, 16, 32, true>(e));
   return g * kWarpsPerBlock;
 }
 
@@ -349,17 +356,17 @@ int timed_end(ipuma_engine* e, cudaStream_t s) {
 
 // allot_idx = entry of the control block's ClassAllot table (the class, or
 // NCLASS_MAX for the s32 rerun).
-template <class T, int K, int LANES>
+template <class T, int K, int LANES, bool HYB = false>
 int launch_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_t* codes,
                    const PairDesc* pairs, const int* list, const int* range, int* head, long rowsCap,
                    int* score, int* arange, int* brange, int kind, int cls, int allot_idx) {
   const int smem = smem_for<T, K, LANES>(e);
-  const int grid = batched_grid<T, K, LANES>(e);
+  const int grid = batched_grid<T, K, LANES, HYB>(e);
   int* ctl = rb.ctl;
   auto* cells = reinterpret_cast<unsigned long long*>(ctl + CTL_CELLS);
   int rc;
   if ((rc = timed_begin(e, s, kind, cls))) return rc;
-  k_batched<T, K, LANES><<<grid, kThreads, smem, s>>>(
+  k_batched<T, K, LANES, HYB><<<grid, kThreads, smem, s>>>(
       e->sc, e->d_sim.as<int8_t>(), codes, pairs, list, range, head, rb.scratch->as<int2>(),
       rowsCap, score, arange, brange, rb.ovf->as<int>(), cells + CELLS_RERUN,
       reinterpret_cast<DevStatus*>(ctl + CTL_STATUS),
@@ -405,8 +412,9 @@ long thread_rows(const ipuma_engine* e, int maxA, int maxB) {
 // Full-occupancy grid and strip scratch (int2) per block of every class.
 void class_grids(ipuma_engine* e, int maxA, int maxB, int* grid, long long* spb) {
   const long long rowsCap = std::max(1, maxB);
-  for (int c = 0; c <= kNumS16; ++c) {
+  for (int c = 0; c < kNumClasses; ++c) {
     switch (c) {
+      case kClsHi: grid[c] = batched_grid<LaneS16x2, 16, 32, true>(e); break;
       case 0: grid[c] = batched_grid<LaneS16x2, 4, 16>(e); break;
       case 1: grid[c] = batched_grid<LaneS16x2, 8, 16>(e); break;
       case 2: grid[c] = batched_grid<LaneS16x2, 12, 16>(e); break;
@@ -428,7 +436,7 @@ void class_grids(ipuma_engine* e, int maxA, int maxB, int* grid, long long* spb)
     if (c == kClsThread)
       spb[c] = (long long)kThreads * thread_rows(e, maxA, maxB);
     else
-      spb[c] = (long long)kWarpsPerBlock * (32 / kClasses[c].lanes) * 2 * rowsCap;
+      spb[c] = (long long)kWarpsPerBlock * (32 / kClasses[c].lanes) * (c == kClsHi ? 3 : 2) * rowsCap;
   }
 }
 
@@ -441,7 +449,7 @@ size_t scratch_int2(ipuma_engine* e, int maxA, int maxB) {
   long long spb[NCLASS_MAX + 1];
   class_grids(e, maxA, maxB, grid, spb);
   long long full = 0, round = 0;
-  for (int c = 0; c <= kNumS16; ++c) {
+  for (int c = 0; c < kNumClasses; ++c) {
     full = std::max(full, (long long)grid[c] * spb[c]);
     round += spb[c];
   }
@@ -450,7 +458,7 @@ size_t scratch_int2(ipuma_engine* e, int maxA, int maxB) {
 
 // Launch order of the classes (longest-tail classes first) and, for two
 // alternating streams, the stream (and scratch region) of each.
-constexpr int kLaunchOrder[kNumS16 + 1] = {16, 5, 4, 6, 3, 15, 9, 14, 2, 13, 8, 12, 1, 11, 7, 10, 0};
+constexpr int kLaunchOrder[kNumClasses] = {17, 16, 5, 4, 6, 3, 15, 9, 14, 2, 13, 8, 12, 1, 11, 7, 10, 0};
 
 int reserve_bufs(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, int n, int maxA, int maxB) {
   int rc;
@@ -502,10 +510,11 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   BinParams bp{};
   bp.n_s16_classes = kNumS16;
   bp.cls_s32 = kClsS32;
-  bp.nclass = kNumS16 + 1;
+  bp.cls_hi = e->hybrid ? kClsHi : kClsS32;
+  bp.nclass = kNumClasses;
   bp.s16_max_len = e->s16_max_len;
   bp.force_s32 = e->s16_ok ? 0 : 1;
-  for (int c = 0; c <= kNumS16; ++c) {
+  for (int c = 0; c < kNumClasses; ++c) {
     bp.lanes[c] = kClasses[c].lanes;
     bp.width[c] = kClasses[c].width;
     bp.slot_ps[c] = e->slot_ps[c];
@@ -527,6 +536,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   bp.concurrent = mode;
   // Classes this batch may use (the others are not launched).
   unsigned enabled = kCoarseClasses | (1u << kClsS32);
+  if (e->hybrid) enabled |= 1u << kClsHi;
   if (n >= kFineClassMinPairs) enabled |= kFineClasses;
   if (e->thread_class) enabled |= 1u << kClsThread;
   if (e->tile_k > 0) enabled |= 1u << (e->tile_k - 1);
@@ -541,13 +551,13 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
     if (c != kClsThread) slot_min = std::min(slot_min, e->slot_ps[c]);
   }
   bp.batch_ps_per_cell = slot_min / kPackingEfficiency;
-  bp.lat_share = kLatencyShare;
+  bp.lat_share = e->latency_share;
   bp.lat_min_ps = kLatencyMinBatchPs;
   bp.region = 0;
-  for (int c = 0; c <= kNumS16; ++c) bp.region = std::max(bp.region, (long long)bp.grid[c] * bp.scr_per_block[c]);
+  for (int c = 0; c < kNumClasses; ++c) bp.region = std::max(bp.region, (long long)bp.grid[c] * bp.scr_per_block[c]);
   // Two alternating streams: stream (and scratch region) by position
   // among the launched classes.
-  for (int k = 0, pos = 0; k <= kNumS16; ++k) {
+  for (int k = 0, pos = 0; k < kNumClasses; ++k) {
     const int c = kLaunchOrder[k];
     bp.slot_of[c] = pos & 1;
     if ((enabled >> c) & 1u) ++pos;
@@ -613,6 +623,15 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
       return rc;                                                                                       \
     if ((rc = done(cls))) return rc;                                                                   \
     ++*launches;                                                                                       \
+  }
+  if ((enabled >> kClsHi) & 1u) {
+    cudaStream_t cs = on(kClsHi);
+    if ((rc = launch_batched<LaneS16x2, 16, 32, true>(e, rb, cs, codes, pairs, list, R + 2 * kClsHi,
+                                                      heads + kClsHi, rowsCap, score, arange, brange,
+                                                      kClasses[kClsHi].kind, kClsHi, kClsHi)))
+      return rc;
+    if ((rc = done(kClsHi))) return rc;
+    ++*launches;
   }
   IPUMA_LAUNCH(LaneS32, 16, 32, 16)
   IPUMA_LAUNCH(LaneS16x2, 16, 32, 5)
@@ -753,6 +772,10 @@ int validate_algo(const ipuma_algo_config* a) {
 void set_s32_rates(ipuma_engine* e) {
   e->slot_ps[kClsS32] = 2.f * e->slot_ps[kClsWidest];
   e->strip_ps[kClsS32] = 2.f * e->strip_ps[kClsWidest];
+  // Hybrid class: between the two; modelled like s32 (its pairs' later
+  // strips run there).
+  e->slot_ps[kClsHi] = e->slot_ps[kClsS32];
+  e->strip_ps[kClsHi] = e->strip_ps[kClsS32];
 }
 
 void set_default_rates(ipuma_engine* e) {
@@ -1165,6 +1188,7 @@ int ipuma_gpu_create(const ipuma_sw_config* sw, const ipuma_algo_config* algo, i
                (minSub - (gI + gE) >= -128) && (gI + gE > -1000) && (gE > -1000);
   // s16x2 lanes: H <= 32767 - maxSub guarantees no halfword overflow.
   e->sc.s16Limit = 32767 - std::max(0, e->maxSub);
+  e->sc.maxSub = std::max(0, e->maxSub);
   e->s16_ok = e->fast_ok;
   e->s16_max_len = e->maxSub > 0 ? (e->sc.s16Limit / e->maxSub) : (1 << 30);
   set_default_rates(e.get());
@@ -1221,6 +1245,11 @@ int ipuma_gpu_set_option(ipuma_engine* e, const char* name, int64_t value) {
     e->autotune = value ? 1 : 0;
   } else if (k == "time_launches") {
     e->time_launches = value ? 1 : 0;
+  } else if (k == "latency_share") {
+    if (value < 1 || value > 100000) return fail(IPUMA_ERR_INVALID_ARG, "latency_share is in per mille, 1..100000");
+    e->latency_share = (float)value / 1000.f;
+  } else if (k == "hybrid") {
+    e->hybrid = value ? 1 : 0;
   } else if (k == "concurrent") {
     if (value < 0 || value > 3) return fail(IPUMA_ERR_INVALID_ARG, "concurrent must be 0, 1, 2 or 3");
     e->concurrent = (int)value;
@@ -1307,7 +1336,8 @@ int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_c
                                        (uint64_t)(uintptr_t)e->d_list.p, (uint64_t)(uintptr_t)e->d_ctl.p,
                                        (uint64_t)(uintptr_t)e->d_ovf.p, (uint64_t)(uintptr_t)e->d_flag.p,
                                        (uint64_t)e->tile_k, (uint64_t)e->long_a, (uint64_t)e->thread_class,
-                                       (uint64_t)e->concurrent};
+                                       (uint64_t)e->concurrent, (uint64_t)e->hybrid,
+                                       (uint64_t)(e->latency_share * 1e6f)};
     auto it = e->graphs_cache.find(key);
     if (it == e->graphs_cache.end()) {
       if (e->graphs_cache.size() >= 16) {

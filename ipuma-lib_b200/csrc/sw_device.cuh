@@ -62,6 +62,21 @@ struct SwConst {
   int M;        // alphabet size (rows/cols of the substitution matrix)
   int forwardOnly;
   int s16Limit; // a pair whose score exceeds this is rerun in s32
+  int maxSub;   // largest substitution score (strip bound of the hybrid pass)
+};
+
+// Control of a hybrid pass (sw_pass with HYB): an s16x2 pass that stops
+// before the first strip whose values could pass sc.s16Limit, and the s32
+// pass that continues one of its pairs from there.  A strip's H values are
+// at most max(0, H of the boundary column entering it) + maxSub * strip
+// width: a path enters from that column or starts inside the strip, and
+// gains at most maxSub per diagonal step, of which a strip holds at most
+// its width.
+struct PassCtl {
+  int strip0 = 0;          // first strip of this pass
+  int bndHalf = -1;        // strip0 > 0: half (0/1) of the packed s16x2 boundary to read
+  int scrBase = 0;         // scratch buffer (0..2) holding that boundary
+  int stoppedAt = -1;      // out (s16x2 pass): strip it stopped before, -1: none
 };
 
 // -------------------------------------------------------------------------
@@ -265,10 +280,15 @@ __device__ __forceinline__ uint32_t keep_mask(LaneS32, int rm, int b) {
 //              pass needs more than one strip)
 //   out      : best cell per pair, in pass coordinates
 // -------------------------------------------------------------------------
-template <class T, int K, int LANES>
+// HYB: three scratch buffers of rowsCap per group, and `ctl` in use -- an
+// s16x2 pass (ctl->strip0 == 0) stops before an unsafe strip and reports
+// it; an s32 pass with ctl->strip0 > 0 starts there from the packed
+// boundary half ctl->bndHalf in buffer ctl->scrBase, keeping `out` (the
+// best of the strips before) and using the two other buffers.
+template <class T, int K, int LANES, bool HYB = false>
 __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, const int8_t* s_simp,
                                         uint16_t* s_bring, const PassSeq (&ps)[T::NP], int2* scr,
-                                        long rowsCap, Best (&out)[T::NP]) {
+                                        long rowsCap, Best (&out)[T::NP], PassCtl* ctl = nullptr) {
   using V = typename T::V;
   constexpr int SW = LANES * K;          // columns per strip
   constexpr int KP = ProfileWords<K>::KP;
@@ -278,14 +298,17 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
   const int M = sc.M;
   const int profStride = (M + 1) * SWP;
 
+  const int strip0 = HYB ? ctl->strip0 : 0;
   int rowsG = 0, amax = 0;
 #pragma unroll
   for (int h = 0; h < NP; ++h) {
     rowsG = max(rowsG, ps[h].blen);
     amax = max(amax, ps[h].alen);
-    out[h].s = 0;
-    out[h].i = 0;
-    out[h].j = 0;
+    if (strip0 == 0) {
+      out[h].s = 0;
+      out[h].i = 0;
+      out[h].j = 0;
+    }
   }
   const int rowsW = __reduce_max_sync(FULL, rowsG);
   const int rowsMin = __reduce_min_sync(FULL, rowsG);
@@ -306,12 +329,45 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
   constexpr int kStepUnroll = IPUMA_STEP_UNROLL > 0 ? (IPUMA_STEP_UNROLL < LANES ? IPUMA_STEP_UNROLL : LANES)
                                                    : (K > 12 ? 4 : 8);
 
-  for (int strip = 0; strip < nstrips; ++strip) {
+  // Scratch buffer written by strip s: 0/1 alternating, or for an s32
+  // continuation the two buffers other than the one holding its input.
+  auto wbuf = [&](int sidx) -> int {
+    if (!HYB || strip0 == 0) return sidx & 1;
+    return (ctl->scrBase + 1 + ((sidx - strip0) & 1)) % 3;
+  };
+  // H of the last column, maximum over rows, per half (HYB s16x2 pass):
+  // the bound of the next strip.
+  V bmax = vZero;
+
+  for (int strip = strip0; strip < nstrips; ++strip) {
     const int col0 = strip * SW;
     const bool hasIn = strip > 0;
     const bool hasOut = strip + 1 < nstrips;
-    const int2* scrIn = scr + ((strip & 1) ? rowsCap : 0);
-    int2* scrOut = scr + ((strip & 1) ? 0 : rowsCap);
+    const bool packedIn = HYB && strip == strip0 && strip0 > 0;  // unpack a half of the s16x2 boundary
+    const int2* scrIn = scr + (packedIn ? ctl->scrBase : hasIn ? wbuf(strip - 1) : 0) * rowsCap;
+    int2* scrOut = scr + wbuf(strip) * rowsCap;
+    if constexpr (HYB && NP == 2) {
+      if (strip > 0) {
+        // Stop before a strip that could leave int16: the caller continues
+        // each pair in s32 from the boundary this pass left behind.
+        const V bm = __shfl_sync(FULL, bmax, LANES - 1, LANES);
+        const int lim2 = lim - sc.maxSub * SW;
+        if (__any_sync(FULL, T::half(bm, 0) > lim2 || T::half(bm, 1) > lim2)) {
+          ctl->stoppedAt = strip;
+          ctl->scrBase = wbuf(strip - 1);
+          return true;
+        }
+        bmax = vZero;
+      }
+    }
+    auto bnd = [&](int r) -> int2 {
+      const int2 v = scrIn[r];
+      if (HYB && NP == 1 && packedIn) {
+        const int sh = 16 * ctl->bndHalf;
+        return make_int2((int)(int16_t)((uint32_t)v.x >> sh), (int)(int16_t)((uint32_t)v.y >> sh));
+      }
+      return v;
+    };
 
     __syncwarp();
 #pragma unroll
@@ -336,8 +392,8 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
     // group's chunk registers holds row (chunkBase + k).
     int2 chunk = make_int2(0, 0), chunkNext = make_int2(0, 0);
     if (hasIn) {
-      if (lane < rowsG) chunk = scrIn[lane];
-      if (LANES + lane < rowsG) chunkNext = scrIn[LANES + lane];
+      if (lane < rowsG) chunk = bnd(lane);
+      if (LANES + lane < rowsG) chunkNext = bnd(LANES + lane);
     }
 
     // B letters, LANES rows at a time: lane k of `bnext` holds the letters
@@ -429,6 +485,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
           for (int c = 0; c < K; ++c) snap[c] = (V)(((uint32_t)snap[c] & keep) | ((uint32_t)H[c] & ~keep));
         }
         if (hasOut && lane == LANES - 1) scrOut[i] = make_int2((int)outY, (int)outE);
+        if constexpr (HYB && NP == 2) bmax = T::max2(bmax, T::addmax(outE, vgIgE, outY));
       }
     };
 
@@ -451,7 +508,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
       if (hasIn && t0 > 0) {
         chunk = chunkNext;
         const int r = t0 + LANES + lane;
-        chunkNext = (r < rowsG) ? scrIn[r] : make_int2(0, 0);
+        chunkNext = (r < rowsG) ? bnd(r) : make_int2(0, 0);
       }
       if (t0 >= LANES - 1 && t0 + LANES - 1 < rowsMin) {
 #pragma unroll kStepUnroll

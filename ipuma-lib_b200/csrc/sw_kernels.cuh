@@ -118,6 +118,63 @@ __device__ __forceinline__ void align_pairs(const SwConst& sc, uint8_t* s_prof,
   }
 }
 
+// One pass of the hybrid class for the two pairs of a 32-lane group: s16x2
+// while every strip is provably inside int16, then each pair alone in s32
+// lanes from the first strip that is not (its half of the packed boundary
+// column as input).  Returns false when the s16x2 part gave up anyway.
+template <int K>
+__device__ __forceinline__ bool hybrid_pass(const SwConst& sc, uint8_t* s_prof, const int8_t* s_simp,
+                                            uint16_t* s_bring, const PassSeq (&ps)[2], int2* scr,
+                                            long rowsCap, Best (&out)[2]) {
+  PassCtl c16;
+  if (!sw_pass<LaneS16x2, K, 32, true>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, out, &c16)) return false;
+  if (c16.stoppedAt < 0) return true;
+#pragma unroll 1
+  for (int h = 0; h < 2; ++h) {
+    if (ps[h].alen <= c16.stoppedAt * 32 * K || ps[h].blen <= 0) continue;  // no strip left
+    PassCtl c32;
+    c32.strip0 = c16.stoppedAt;
+    c32.bndHalf = h;
+    c32.scrBase = c16.scrBase;
+    const PassSeq one[1] = {ps[h]};
+    Best o[1] = {out[h]};
+    sw_pass<LaneS32, K, 32, true>(sc, s_prof, s_simp, s_bring, one, scr, rowsCap, o, &c32);
+    out[h] = o[0];
+  }
+  return true;
+}
+
+// Forward (+ reverse) pass of the hybrid class; as align_pairs.
+template <int K>
+__device__ __forceinline__ void align_pairs_hybrid(const SwConst& sc, uint8_t* s_prof, const int8_t* s_simp,
+                                                   uint16_t* s_bring, const uint8_t* const (&a0)[2],
+                                                   const uint8_t* const (&b0)[2], const int (&alen)[2],
+                                                   const int (&blen)[2], int2* scr, long rowsCap,
+                                                   Best (&fw)[2], Best (&rv)[2], bool (&ovf)[2]) {
+  PassSeq ps[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const bool empty = alen[h] <= 0 || blen[h] <= 0;
+    ps[h] = PassSeq{a0[h], b0[h], empty ? 0 : alen[h], empty ? 0 : blen[h], 1, 1};
+  }
+  const bool done = hybrid_pass<K>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, fw);
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    ovf[h] = !done;
+    rv[h] = Best{0, 0, 0};
+  }
+  if (done && !sc.forwardOnly) {
+    PassSeq rs[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+      rs[h] = fw[h].s > 0 ? PassSeq{a0[h] + fw[h].j, b0[h] + fw[h].i, fw[h].j + 1, fw[h].i + 1, -1, -1}
+                          : PassSeq{a0[h], b0[h], 0, 0, 1, 1};
+    if (!hybrid_pass<K>(sc, s_prof, s_simp, s_bring, rs, scr, rowsCap, rv)) {
+      ovf[0] = ovf[1] = true;
+    }
+  }
+}
+
 __device__ __forceinline__ void write_result(const SwConst& sc, const Best& fw, const Best& rv,
                                              int* score, int* arange, int* brange, long idx) {
   const int aend = fw.j, bend = fw.i;
@@ -131,7 +188,7 @@ __device__ __forceinline__ void write_result(const SwConst& sc, const Best& fw, 
 // Persistent batched kernel.  `list` holds pair ids in processing order;
 // a warp takes items of 32 / LANES * NP consecutive entries (ids < 0 are
 // padding), lane group g aligning entries [g * NP, g * NP + NP).
-template <class T, int K, int LANES>
+template <class T, int K, int LANES, bool HYB = false>
 __global__ void __launch_bounds__(128) k_batched(SwConst sc, const int8_t* __restrict__ sim,
                                                  const uint8_t* __restrict__ codes,
                                                  const PairDesc* __restrict__ pairs,
@@ -166,7 +223,8 @@ __global__ void __launch_bounds__(128) k_batched(SwConst sc, const int8_t* __res
   list += range[0];
   const int items = (n + PER_ITEM - 1) / PER_ITEM;
   const long gw = (long)blockIdx.x * warps + wib;
-  int2* scr = scratch + (gw * GROUPS + group) * 2 * rowsCap;
+  constexpr int NBUF = HYB ? 3 : 2;  // strip-boundary buffers per group
+  int2* scr = scratch + (gw * GROUPS + group) * NBUF * rowsCap;
   while (true) {
     int item = 0;
     if (lane32 == 0) item = atomicAdd(queue_head, 1);
@@ -194,7 +252,12 @@ __global__ void __launch_bounds__(128) k_batched(SwConst sc, const int8_t* __res
     }
     Best fw[NP], rv[NP];
     bool ovf[NP];
-    align_pairs<T, K, LANES>(sc, s_prof, s_simp, s_bring, a0, b0, alen, blen, scr, rowsCap, fw, rv, ovf);
+    if constexpr (HYB) {
+      static_assert(NP == 2 && LANES == 32, "the hybrid class pairs two s16x2 pairs per 32-lane warp");
+      align_pairs_hybrid<K>(sc, s_prof, s_simp, s_bring, a0, b0, alen, blen, scr, rowsCap, fw, rv, ovf);
+    } else {
+      align_pairs<T, K, LANES>(sc, s_prof, s_simp, s_bring, a0, b0, alen, blen, scr, rowsCap, fw, rv, ovf);
+    }
     if (glane == 0) {
 #pragma unroll
       for (int h = 0; h < NP; ++h) {
@@ -343,7 +406,7 @@ static __global__ void k_exact(SwConst sc, const int8_t* __restrict__ sim, const
 constexpr int NROWB = 256;    // row buckets (16 per power of two)
 constexpr int NSTRIPB = 16;   // strip-count buckets
 constexpr int NBUCKET = NROWB * NSTRIPB;
-constexpr int NCLASS_MAX = 17;
+constexpr int NCLASS_MAX = 18;
 
 // Log-linear bucket of |B| (16 sub-buckets per power of two): pairs that
 // share a bucket differ by at most 1/16 in rows, so the groups of a warp
@@ -357,6 +420,8 @@ __device__ __forceinline__ int rows_bucket(int b) {
 struct BinParams {
   int nclass;
   int cls_s32;             // class index of the exact-32-bit kernel
+  int cls_hi;              // class of pairs the diagonal bound sends to 32 bits:
+                           // the hybrid class (or cls_s32 when it is off)
   int s16_max_len;         // min(|A|,|B|) above which s16x2 could overflow
   int s16_limit;           // scores above this need s32 lanes
   int lanes[NCLASS_MAX];   // lanes per group of each class
@@ -431,8 +496,10 @@ static __device__ int diagonal_bound(const uint8_t* a, const uint8_t* b, int n, 
 __device__ __forceinline__ int pair_key(const BinParams& bp, int alen, int blen, bool s32, float thr_cap,
                                         float* cost_out = nullptr) {
   int cls;
-  if (bp.force_s32 || s32) {
+  if (bp.force_s32) {
     cls = bp.cls_s32;
+  } else if (s32) {
+    cls = bp.cls_hi;
   } else if (bp.forced_class >= 0) {
     cls = bp.forced_class;
   } else if (alen > bp.long_a) {

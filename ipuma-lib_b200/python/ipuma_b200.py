@@ -53,7 +53,7 @@ KERNEL_NAMES = {0: "k_batched<s32,L32,K16>", 1: "k_batched<s16x2,L16,K4>",
                 13: "k_batched<s16x2,L16,K14>", 14: "k_batched<s16x2,L16,K5>",
                 15: "k_batched<s16x2,L16,K7>", 16: "k_batched<s16x2,L16,K9>",
                 17: "k_batched<s16x2,L16,K11>", 18: "k_batched<s16x2,L16,K13>",
-                19: "k_batched<s16x2,L16,K15>"}
+                19: "k_batched<s16x2,L16,K15>", 20: "k_hybrid<s16x2->s32,L32,K16>"}
 MAX_TIMED = 24  # IPUMA_MAX_TIMED
 
 

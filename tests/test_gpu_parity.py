@@ -263,6 +263,77 @@ def test_thread_class_chosen_automatically_for_large_batches():
     _assert_same(tuple(o[idx] for o in outs[0]), want, "thread class sample")
 
 
+# ------------------------------------------------------- hybrid class ---
+
+HYBRID_KIND = 20
+
+
+def _mutated(rng, seq, rate, alphabet):
+    out = seq.copy()
+    hit = rng.random(seq.size) < rate
+    out[hit] = rng.choice(alphabet, hit.sum())
+    return out
+
+
+@pytest.mark.parametrize("forward_only", [True, False])
+def test_hybrid_class_for_scores_above_int16(forward_only):
+    """Near-identical long protein pairs (scores above int16) of different
+    lengths, in warps with short pairs: their strips run in s16x2 while the
+    strip bound holds, then each pair continues in s32.  Same results with
+    the hybrid class on and off, equal to the oracle."""
+    rng = np.random.default_rng(71)
+    alpha = np.arange(20, dtype=np.uint8)
+    seqs_a, seqs_b = [], []
+    for la in (7000, 6500, 7300, 5000, 4100, 3600):
+        a = rng.choice(alpha, la).astype(np.uint8)
+        seqs_a.append(a)
+        seqs_b.append(_mutated(rng, a[: la - int(rng.integers(0, 300))], 0.01, alpha))
+    for la in (40, 300, 900):
+        a = rng.choice(alpha, la).astype(np.uint8)
+        seqs_a.append(a)
+        seqs_b.append(_mutated(rng, a, 0.3, alpha))
+    codes, a_off, a_len, b_off, b_len = oracle.pack_pairs(seqs_a, seqs_b)
+    pairs = ib.make_pairs(a_off, a_len, b_off, b_len)
+    case = {"similarity": "blosum62", "match": 1, "mismatch": -1, "ambiguity": -1,
+            "datatype": "aa", "gapInit": -10, "gapExtend": -1}
+    sim = oracle.select_matrix("blosum62")
+    want = oracle.sw_batch(codes, a_off, a_len, b_off, b_len, sim, -10, -1,
+                           forward_only=forward_only)
+    assert (want[0] > 32767).sum() >= 3
+    for hyb in (1, 0):
+        with _engine(case, forward_only, hybrid=hyb, time_launches=1) as e:
+            got = e.compare(codes, pairs)
+            st = e.stats()
+            kinds = {st.timed_kind[k]: st.timed_cells[k] for k in range(st.n_timed)}
+        _assert_same(got, want, "hybrid=%d fwd=%s" % (hyb, forward_only))
+        assert (kinds.get(HYBRID_KIND, 0) > 0) == bool(hyb)
+
+
+def test_hybrid_class_switches_at_the_first_strip():
+    """DNA scored +50/-40: the strip bound fails from the second strip on,
+    so long identical pairs switch to s32 right after strip 0 (and short
+    ones never leave s16x2)."""
+    rng = np.random.default_rng(72)
+    acgt = np.array([1, 2, 3, 4], dtype=np.uint8)
+    seqs_a, seqs_b = [], []
+    for la in (2100, 1800, 1300, 900, 520, 511):
+        a = rng.choice(acgt, la).astype(np.uint8)
+        seqs_a.append(a)
+        seqs_b.append(_mutated(rng, a, 0.002, acgt))
+    codes, a_off, a_len, b_off, b_len = oracle.pack_pairs(seqs_a, seqs_b)
+    pairs = ib.make_pairs(a_off, a_len, b_off, b_len)
+    case = {"similarity": "na", "match": 50, "mismatch": -40, "ambiguity": -40,
+            "datatype": "na", "gapInit": 0, "gapExtend": -1}
+    sim = oracle.select_matrix("na", 50, -40, -40)
+    for fwd in (True, False):
+        want = oracle.sw_batch(codes, a_off, a_len, b_off, b_len, sim, 0, -1, forward_only=fwd)
+        assert (want[0] > 32767).sum() >= 3
+        for hyb in (1, 0):
+            with _engine(case, fwd, hybrid=hyb) as e:
+                got = e.compare(codes, pairs)
+            _assert_same(got, want, "dna +50 hybrid=%d fwd=%s" % (hyb, fwd))
+
+
 # ------------------------------------------------- concurrent classes ---
 
 @pytest.mark.parametrize("forward_only", [True, False])
