@@ -244,13 +244,14 @@ def test_thread_class_s16_overflow_goes_to_s32_rerun():
 
 def test_thread_class_chosen_automatically_for_large_batches():
     """With the class enabled (option thread_class) a large batch sends part
-    of its pairs to it; results equal the run with the class disabled."""
+    of its pairs to it; results equal the run with the class disabled.  (Its
+    items are long, so the latency share is widened to let it qualify.)"""
     wl = workloads.dna_batched(n=120_000, seed=66)
     case = _wl_case(wl)
     pairs = ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len)
     outs = []
     for on in (1, 0):
-        with _engine(case, True, thread_class=on, time_launches=1) as e:
+        with _engine(case, True, thread_class=on, time_launches=1, latency_share=500) as e:
             outs.append(e.compare(wl.codes, pairs))
             st = e.stats()
             kinds = {st.timed_kind[k]: st.timed_cells[k] for k in range(st.n_timed)}
