@@ -308,7 +308,7 @@ def serving_section(args, ib, torch, dev, stream, local):
         sets = [srv.add_sequences(wl.codes) for wl in wls]
         res["sizes_1_4096_resident"] = slim(serving.sweep(srv, wls, peak, loads, dur, 1, 4096,
                                                           set_ids=sets, seed=10))
-        res["pairs_64_resident"] = slim(serving.sweep(srv, wls, peak, [0.5, 0.8, 1.0], dur, 64, 64,
+        res["pairs_64_resident"] = slim(serving.sweep(srv, wls, peak, [0.5, 0.8, 0.9, 1.0], dur, 64, 64,
                                                       set_ids=sets, seed=30))
         res["sizes_1_4096_staged"] = slim(serving.sweep(srv, wls, peak, loads, dur, 1, 4096,
                                                         seed=20))

@@ -314,7 +314,7 @@ typedef struct ipuma_server_config {
   int32_t device;
   int32_t one_request_per_batch;   /* 1: no coalescing (each batch = one request or
                                       part of one), the per-request baseline */
-  int64_t max_batch_cells;         /* cells per device batch (latency bound); 0 = 2e9 */
+  int64_t max_batch_cells;         /* cells per device batch (latency bound); 0 = 4e9 */
   int32_t reserve_b_len;           /* |B| the engines' buffers are sized for at start;
                                       0 = 2048 (longer pairs grow them on demand) */
 } ipuma_server_config;
