@@ -164,6 +164,10 @@ const char* ipuma_last_error(void);
 const char* ipuma_version(void);
 /* Number of CUDA devices (0 when none is usable). */
 int32_t ipuma_device_count(void);
+/* Page-locked host memory for wire buffers (uploads at full bus speed, and
+ * results are copied straight into it); *out = NULL when bytes = 0. */
+int ipuma_host_alloc(size_t bytes, void** out);
+void ipuma_host_free(void* p);
 
 /* Host-only helpers (no GPU needed). */
 /* Encodes n chars into codes; unknown NA characters (code 16, which has no
@@ -225,14 +229,24 @@ int ipuma_gpu_set_option(ipuma_engine* e, const char* name, int64_t value);
  *             ranges pack start | end << 16 (uint16 halves). */
 int ipuma_gpu_run_buffer(ipuma_engine* e, const int32_t* inputs, size_t n_inputs, int32_t* results,
                          size_t n_results);
-/* Asynchronous form: the buffers must stay valid until ipuma_gpu_join. */
+/* Asynchronous form: the buffers must stay valid until ipuma_gpu_join.
+ * Returns once the work is enqueued.  Jobs alternate between two device
+ * buffer sets and streams, so one job's upload and result copy overlap the
+ * previous job's kernels; only the tiles up to the last one with a
+ * non-zero Meta word are uploaded.  Pageable `results` receive the job's
+ * results through pinned staging, copied out by the join. */
 int ipuma_gpu_submit_buffer(ipuma_engine* e, const int32_t* inputs, size_t n_inputs,
                             int32_t* results, size_t n_results, uint64_t* job);
 /* *done = 1 once the job's results are in place (results are only
  * guaranteed after ipuma_gpu_join). */
 int ipuma_gpu_poll(ipuma_engine* e, uint64_t job, int32_t* done);
-/* Waits for a job (bounded by timeout_ms; < 0 waits without limit). */
+/* Waits for a job (bounded by timeout_ms; < 0 waits without limit).  A job
+ * is joined once; jobs may be joined in any order, from any thread. */
 int ipuma_gpu_join(ipuma_engine* e, uint64_t job, int64_t timeout_ms);
+/* ipuma_gpu_join that also returns the job's own statistics (kernel_ms =
+ * its kernels, total_ms = upload + kernels + result copy), whatever other
+ * jobs ran or were joined meanwhile.  `out` may be null. */
+int ipuma_gpu_join_stats(ipuma_engine* e, uint64_t job, int64_t timeout_ms, ipuma_stats* out);
 
 /* Aligns n pairs from host memory; results in input order.  Large batches
  * are split into chunks of consecutive pairs: each chunk uploads the byte

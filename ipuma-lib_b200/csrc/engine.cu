@@ -58,6 +58,7 @@ struct DevBuf {
   size_t cap = 0;
   int ensure(size_t bytes, cudaStream_t s) {
     if (bytes <= cap && p) return IPUMA_OK;
+    const size_t old = cap;
     if (p) {
       cudaStreamSynchronize(s);
       cudaFree(p);
@@ -66,7 +67,7 @@ struct DevBuf {
     }
     // Geometric growth: a stream of slowly growing batches reallocates
     // (and synchronises the device in cudaFree) only a few times.
-    size_t want = std::max<size_t>({bytes, (size_t)256, cap + cap / 2});
+    size_t want = std::max<size_t>({bytes, (size_t)256, old + old / 2});
     want = (want + (1u << 20) - 1) & ~(size_t)((1u << 20) - 1);
     cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
@@ -149,9 +150,29 @@ constexpr int kValidatePairsPerThread = 131072;
 constexpr size_t kChunkMinBytes = 32u << 20;  // and the batch uploads at least this much
 constexpr int kThreads = 32 * kWarpsPerBlock;
 
+// Status of one wire-buffer job, copied from its control block to pinned
+// host memory by the job's own stream before any later job can clear it.
+struct JobStatus {
+  DevStatus st;
+};
+
+// One asynchronous wire-buffer batch (ipuma_gpu_submit_buffer).
 struct Job {
-  cudaEvent_t done = nullptr;
-  bool finished = false;
+  cudaEvent_t ev[3] = {};       // start, inputs uploaded, kernels done
+  cudaEvent_t done = nullptr;   // after the job's last copy (timing too)
+  JobStatus* status = nullptr;  // pinned, from the engine's pool
+  int32_t* staged = nullptr;    // pinned results staging (pageable destination)
+  size_t staged_bytes = 0;
+  int32_t* results = nullptr;   // the caller's results buffer
+  size_t n_results = 0;
+  ipuma_stats stats{};
+};
+
+// Buffers and stream of one in-flight wire batch.  Wire jobs alternate
+// between two such sets, so one batch's upload and result copy overlap the
+// previous batch's kernels.
+struct WireBufs {
+  DevBuf inputs, results, pairs, ctl, list, scratch, ovf, flag;
 };
 
 }  // namespace
@@ -219,6 +240,17 @@ struct ipuma_engine {
   std::mutex mu;
   std::map<uint64_t, Job> jobs;
   uint64_t next_job = 1;
+  // Second wire-buffer set and its stream (the first set is the engine's
+  // main buffers on `stream`); wire jobs alternate between the two.
+  WireBufs w1;
+  cudaStream_t wstream1 = nullptr;
+  uint64_t wire_jobs = 0;
+  // Recycled per-job resources: timing events, pinned status slots and
+  // pinned result staging buffers (by size).
+  std::vector<cudaEvent_t> free_events;
+  std::vector<JobStatus*> free_status;
+  std::multimap<size_t, int32_t*> free_staging;
+  std::vector<void*> pinned_blocks;  // every pinned allocation, freed at destroy
 };
 
 namespace {
@@ -720,11 +752,11 @@ int plain_k_for(int maxAB) {
 }
 
 // Launches the one-launch-per-batch kernel over a wire buffer on the device.
-int run_plain_wire(ipuma_engine* e, cudaStream_t s, const int* d_inputs, long seqWordsPerTile,
+int run_plain_wire(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const int* d_inputs, long seqWordsPerTile,
                    long metaOffset, int maxBatches, int totalSlots, int maxB, int* d_results,
                    int* launches) {
   int rc;
-  int* ctl = e->d_ctl.as<int>();
+  int* ctl = rb.ctl;
   DevStatus* st = reinterpret_cast<DevStatus*>(ctl + CTL_STATUS);
   const long rowsCap = std::max(1, maxB);
   const int K = plain_k_for(e->algo.max_ab);
@@ -732,10 +764,10 @@ int run_plain_wire(ipuma_engine* e, cudaStream_t s, const int* d_inputs, long se
     const int grid = occupancy_grid(e, kern, smem);
     const long warps = (long)grid * kWarpsPerBlock;
     int r;
-    if ((r = e->d_scratch.ensure(sizeof(int2) * 2 * rowsCap * warps, s))) return r;
+    if ((r = rb.scratch->ensure(sizeof(int2) * 2 * rowsCap * warps, s))) return r;
     if ((r = timed_begin(e, s, IPUMA_KERNEL_PLAIN, CELLS_WIRE))) return r;
     kern<<<grid, kThreads, smem, s>>>(e->sc, e->d_sim.as<int8_t>(), d_inputs, seqWordsPerTile,
-                                      metaOffset, maxBatches, totalSlots, e->d_scratch.as<int2>(),
+                                      metaOffset, maxBatches, totalSlots, rb.scratch->as<int2>(),
                                       rowsCap, d_results, st);
     CUDA_TRY(cudaGetLastError());
     return timed_end(e, s);
@@ -1024,6 +1056,9 @@ void take_range(std::vector<std::pair<size_t, size_t>>& have, size_t lo, size_t 
 }
 
 int chunk_count(const ipuma_engine* e, int32_t n, size_t n_codes) {
+  // The exact kernel's row scratch is one engine buffer: its runs cannot
+  // overlap on two streams.
+  if (!e->fast_ok) return 1;
   if (e->chunks > 0) return std::min<int>(std::min(e->chunks, kMaxChunks), std::max(1, n));
   if (n < 2 * kChunkMinPairs || n_codes < kChunkMinBytes) return 1;
   return std::min(kMaxChunks, n / kChunkMinPairs);
@@ -1071,6 +1106,126 @@ bool is_pinned(const void* p) {
   return a.type == cudaMemoryTypeHost;
 }
 
+// Bounds check of a wire buffer's Meta (the kernels trust offsets and
+// lengths) with the maxima, the cells and the last slot holding any
+// non-zero Meta word.
+struct MetaScan {
+  long bad = -1;  // first slot pointing outside its tile
+  int maxA = 0, maxB = 0;
+  int64_t cells = 0;
+  long last = -1;
+};
+
+void scan_meta(const int32_t* meta, long lo, long hi, long tileBytes, MetaScan& r) {
+  for (long g = lo; g < hi; ++g) {
+    const int32_t al = meta[4 * g], ao = meta[4 * g + 1], bl = meta[4 * g + 2], bo = meta[4 * g + 3];
+    if ((al | ao | bl | bo) != 0) r.last = g;
+    if (al == 0 || bl == 0) continue;
+    if (al < 0 || bl < 0 || ao < 0 || bo < 0 || (long)ao + al > tileBytes || (long)bo + bl > tileBytes) {
+      r.bad = g;
+      return;
+    }
+    r.maxA = std::max(r.maxA, (int)al);
+    r.maxB = std::max(r.maxB, (int)bl);
+    r.cells += (int64_t)al * bl;
+  }
+}
+
+// Scans all slots, on several host threads for large buffers.
+MetaScan scan_wire(const int32_t* meta, long totalSlots, long tileBytes) {
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int nthr = (int)std::max<long>(1, std::min<long>({(long)kValidateMaxThreads, (long)hw,
+                                                          totalSlots / (2 * kValidatePairsPerThread)}));
+  std::vector<MetaScan> part(nthr);
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nthr; ++t)
+    pool.emplace_back(scan_meta, meta, totalSlots * t / nthr, totalSlots * (t + 1) / nthr, tileBytes,
+                      std::ref(part[t]));
+  scan_meta(meta, 0, totalSlots / nthr, tileBytes, part[0]);
+  for (auto& th : pool) th.join();
+  MetaScan r;
+  for (const auto& p : part) {
+    if (p.bad >= 0 && r.bad < 0) r.bad = p.bad;
+    r.maxA = std::max(r.maxA, p.maxA);
+    r.maxB = std::max(r.maxB, p.maxB);
+    r.cells += p.cells;
+    r.last = std::max(r.last, p.last);
+  }
+  return r;
+}
+
+// The buffers and stream of wire set k: 0 = the engine's main buffers on
+// `stream`, 1 = the second set on `wstream1`.  `rb.ctl` is valid once
+// `ctl` holds a control block.
+struct WireSet {
+  DevBuf *inputs, *results, *pairs, *ctl;
+  RunBufs rb;
+  cudaStream_t s;
+};
+
+WireSet wire_set(ipuma_engine* e, int k) {
+  if (k == 0) return WireSet{&e->d_inputs, &e->d_wres, &e->d_pairs, &e->d_ctl, main_bufs(e), e->stream};
+  WireBufs& w = e->w1;
+  return WireSet{&w.inputs, &w.results, &w.pairs, &w.ctl,
+                 RunBufs{w.ctl.as<int>(), &w.scratch, &w.list, &w.ovf, &w.flag}, e->wstream1};
+}
+
+int take_event(ipuma_engine* e, cudaEvent_t* ev) {
+  if (!e->free_events.empty()) {
+    *ev = e->free_events.back();
+    e->free_events.pop_back();
+    return IPUMA_OK;
+  }
+  CUDA_TRY(cudaEventCreate(ev));
+  return IPUMA_OK;
+}
+
+int take_status(ipuma_engine* e, JobStatus** out) {
+  if (e->free_status.empty()) {
+    constexpr int kSlots = 64;
+    void* block = nullptr;
+    CUDA_TRY(cudaHostAlloc(&block, sizeof(JobStatus) * kSlots, cudaHostAllocPortable));
+    e->pinned_blocks.push_back(block);
+    for (int i = 0; i < kSlots; ++i) e->free_status.push_back(static_cast<JobStatus*>(block) + i);
+  }
+  *out = e->free_status.back();
+  e->free_status.pop_back();
+  return IPUMA_OK;
+}
+
+// Pinned staging of at least `bytes`, reused when a free one is at most
+// twice that size.
+int take_staging(ipuma_engine* e, size_t bytes, int32_t** out, size_t* cap) {
+  auto it = e->free_staging.lower_bound(bytes);
+  if (it != e->free_staging.end() && it->first <= 2 * bytes) {
+    *out = it->second;
+    *cap = it->first;
+    e->free_staging.erase(it);
+    return IPUMA_OK;
+  }
+  void* p = nullptr;
+  CUDA_TRY(cudaHostAlloc(&p, bytes, cudaHostAllocPortable));
+  *out = static_cast<int32_t*>(p);
+  *cap = bytes;
+  return IPUMA_OK;
+}
+
+constexpr size_t kMaxFreeStaging = 8;
+
+// Returns a finished (or abandoned) job's events, status slot and staging
+// to the engine's pools.  Caller holds e->mu.
+void recycle_job(ipuma_engine* e, Job& j) {
+  for (auto& ev : j.ev)
+    if (ev) e->free_events.push_back(ev);
+  if (j.done) e->free_events.push_back(j.done);
+  if (j.status) e->free_status.push_back(j.status);
+  if (j.staged) {
+    if (e->free_staging.size() < kMaxFreeStaging) e->free_staging.emplace(j.staged_bytes, j.staged);
+    else cudaFreeHost(j.staged);
+  }
+  j = Job{};
+}
+
 }  // namespace
 
 extern "C" {
@@ -1086,6 +1241,23 @@ int32_t ipuma_device_count(void) {
     return 0;
   }
   return n;
+}
+
+int ipuma_host_alloc(size_t bytes, void** out) {
+  if (!out) return fail(IPUMA_ERR_INVALID_ARG, "null argument");
+  *out = nullptr;
+  if (bytes == 0) return IPUMA_OK;
+  cudaError_t e = cudaHostAlloc(out, bytes, cudaHostAllocPortable);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *out = nullptr;
+    return fail(IPUMA_ERR_NO_MEMORY, "cudaHostAlloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+  }
+  return IPUMA_OK;
+}
+
+void ipuma_host_free(void* p) {
+  if (p) cudaFreeHost(p);
 }
 
 int ipuma_encode(int32_t datatype, const char* s, size_t n, uint8_t* out) {
@@ -1202,13 +1374,17 @@ void ipuma_gpu_destroy(ipuma_engine* e) {
   if (!e) return;
   cudaSetDevice(e->device);
   if (e->stream) cudaStreamSynchronize(e->stream);
-  for (auto& kv : e->jobs)
-    if (kv.second.done) cudaEventDestroy(kv.second.done);
+  if (e->wstream1) cudaStreamSynchronize(e->wstream1);
+  for (auto& kv : e->jobs) recycle_job(e, kv.second);
+  for (auto ev : e->free_events) cudaEventDestroy(ev);
+  for (auto& kv : e->free_staging) cudaFreeHost(kv.second);
+  for (void* p : e->pinned_blocks) cudaFreeHost(p);
   if (e->stream2) cudaStreamSynchronize(e->stream2);
   if (e->copy_stream) cudaStreamSynchronize(e->copy_stream);
   for (auto* b : {&e->d_sim, &e->d_codes, &e->d_pairs, &e->d_list, &e->d_res, &e->d_scratch, &e->d_cf,
                   &e->d_ovf, &e->d_ctl, &e->d_inputs, &e->d_wres, &e->d_flag, &e->x_list, &e->x_scratch,
-                  &e->x_ovf, &e->x_flag})
+                  &e->x_ovf, &e->x_flag, &e->w1.inputs, &e->w1.results, &e->w1.pairs, &e->w1.ctl, &e->w1.list,
+                  &e->w1.scratch, &e->w1.ovf, &e->w1.flag})
     b->release();
   for (auto& ev : e->cev)
     if (ev) cudaEventDestroy(ev);
@@ -1219,6 +1395,7 @@ void ipuma_gpu_destroy(ipuma_engine* e) {
   }
   if (e->fork_ev) cudaEventDestroy(e->fork_ev);
   if (e->stream2) cudaStreamDestroy(e->stream2);
+  if (e->wstream1) cudaStreamDestroy(e->wstream1);
   if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
   for (auto& ev : e->ev)
     if (ev) cudaEventDestroy(ev);
@@ -1527,8 +1704,8 @@ int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes, con
 
 // Launches the alignment work of a wire buffer already on the device
 // (plain kernel or wire -> pair list -> batched pipeline).
-static int launch_wire(ipuma_engine* e, cudaStream_t s, const int* d_in, int* d_res, int maxA, int maxB,
-                       int* launches) {
+static int launch_wire(ipuma_engine* e, DevBuf* pairs, const RunBufs& rb, cudaStream_t s, const int* d_in,
+                       int* d_res, int maxA, int maxB, int* launches) {
   const ipuma_algo_config& a = e->algo;
   const long seqWordsPerTile = (a.bufsize + 3) / 4;
   const long metaOffset = (long)a.tiles_used * seqWordsPerTile;
@@ -1536,17 +1713,17 @@ static int launch_wire(ipuma_engine* e, cudaStream_t s, const int* d_in, int* d_
   int rc;
   if (totalSlots <= 0) return IPUMA_OK;
   if (e->scheduler == 1 && e->fast_ok) {
-    return run_plain_wire(e, s, d_in, seqWordsPerTile, metaOffset, a.max_batches, (int)totalSlots, maxB,
+    return run_plain_wire(e, rb, s, d_in, seqWordsPerTile, metaOffset, a.max_batches, (int)totalSlots, maxB,
                           d_res, launches);
   }
-  if ((rc = e->d_pairs.ensure(sizeof(PairDesc) * totalSlots, s))) return rc;
+  if ((rc = pairs->ensure(sizeof(PairDesc) * totalSlots, s))) return rc;
   const int gb = (int)std::min<long>((totalSlots + 255) / 256, e->nsm * 8);
   k_wire_to_pairs<<<gb, 256, 0, s>>>(d_in, seqWordsPerTile, metaOffset, a.max_batches, (int)totalSlots,
-                                     e->d_pairs.as<PairDesc>());
+                                     pairs->as<PairDesc>());
   CUDA_TRY(cudaGetLastError());
   *launches += 1;
-  return run_batched(e, main_bufs(e), s, reinterpret_cast<const uint8_t*>(d_in), e->d_pairs.as<PairDesc>(),
-                     (int)totalSlots, maxA, maxB, d_res, d_res + totalSlots, d_res + 2 * totalSlots, launches);
+  return run_batched(e, rb, s, reinterpret_cast<const uint8_t*>(d_in), pairs->as<PairDesc>(), (int)totalSlots,
+                     maxA, maxB, d_res, d_res + totalSlots, d_res + 2 * totalSlots, launches);
 }
 
 static int check_wire_sizes(const ipuma_algo_config& a, size_t n_inputs, size_t n_results) {
@@ -1559,42 +1736,73 @@ static int check_wire_sizes(const ipuma_algo_config& a, size_t n_inputs, size_t 
   return IPUMA_OK;
 }
 
-// Wire-buffer path shared by run/submit: enqueue everything on the stream.
+// Wire-buffer path of run/submit: validates Meta, then enqueues on the next
+// wire set's stream the upload of the tiles in use (trailing tiles whose
+// Meta is all zero are not copied: their Meta is cleared on the device),
+// the kernels, the status copy and the results copy (straight into pinned
+// results, else into pinned staging that the join copies out).
 static int enqueue_buffer(ipuma_engine* e, const int32_t* inputs, size_t n_inputs, int32_t* results,
-                          size_t n_results, int* launches, int64_t* cells_out) {
+                          size_t n_results, Job& j) {
   const ipuma_algo_config& a = e->algo;
   const long seqWordsPerTile = (a.bufsize + 3) / 4;
   const long metaOffset = (long)a.tiles_used * seqWordsPerTile;
   const long totalSlots = (long)a.tiles_used * a.max_batches;
   int rc;
   if ((rc = check_wire_sizes(a, n_inputs, n_results))) return rc;
-  // Host-side validation of Meta (the kernels trust offsets and lengths).
-  const int32_t* meta = inputs + metaOffset;
-  int maxB = 0, maxA = 0;
-  int64_t cells = 0;
-  const long tileBytes = seqWordsPerTile * 4;
-  for (long g = 0; g < totalSlots; ++g) {
-    const int32_t al = meta[4 * g], ao = meta[4 * g + 1], bl = meta[4 * g + 2], bo = meta[4 * g + 3];
-    if (al == 0 || bl == 0) continue;
-    if (al < 0 || bl < 0 || ao < 0 || bo < 0 || (long)ao + al > tileBytes || (long)bo + bl > tileBytes)
-      return fail(IPUMA_ERR_INVALID_ARG, "Meta slot %ld points outside its tile", g);
-    maxA = std::max(maxA, al);
-    maxB = std::max(maxB, bl);
-    cells += (int64_t)al * bl;
-  }
-  if (maxA > 65535 || maxB > 65535)
+  const MetaScan m = scan_wire(inputs + metaOffset, totalSlots, seqWordsPerTile * 4);
+  if (m.bad >= 0) return fail(IPUMA_ERR_INVALID_ARG, "Meta slot %ld points outside its tile", m.bad);
+  if (m.maxA > 65535 || m.maxB > 65535)
     return fail(IPUMA_ERR_TOO_LONG, "sequence longer than 65535 (ranges are uint16)");
-  *cells_out = cells;
-  cudaStream_t s = e->stream;
-  if ((rc = e->d_inputs.ensure(sizeof(int32_t) * std::max<size_t>(n_inputs, 1), s))) return rc;
-  if ((rc = e->d_wres.ensure(sizeof(int32_t) * std::max<size_t>(n_results, 1), s))) return rc;
-  if ((rc = reset_ctl(e, s))) return rc;
-  CUDA_TRY(cudaMemcpyAsync(e->d_inputs.p, inputs, sizeof(int32_t) * n_inputs, cudaMemcpyHostToDevice, s));
-  CUDA_TRY(cudaEventRecord(e->ev[1], s));
-  int* d_res = e->d_wres.as<int>();
-  if ((rc = launch_wire(e, s, e->d_inputs.as<int>(), d_res, maxA, maxB, launches))) return rc;
-  CUDA_TRY(cudaEventRecord(e->ev[2], s));
-  CUDA_TRY(cudaMemcpyAsync(results, d_res, sizeof(int32_t) * n_results, cudaMemcpyDeviceToHost, s));
+
+  // The second set needs the wavefront kernels (the exact kernel's row
+  // scratch is one engine buffer); per-launch timing stays on one stream.
+  const int k = (e->fast_ok && !e->time_launches) ? (int)(e->wire_jobs & 1) : 0;
+  e->wire_jobs++;
+  if (k == 1 && !e->wstream1) CUDA_TRY(cudaStreamCreateWithFlags(&e->wstream1, cudaStreamNonBlocking));
+  WireSet w = wire_set(e, k);
+  cudaStream_t s = w.s;
+  if ((rc = w.inputs->ensure(sizeof(int32_t) * std::max<size_t>(n_inputs, 1), s))) return rc;
+  if ((rc = w.results->ensure(sizeof(int32_t) * std::max<size_t>(n_results, 1), s))) return rc;
+  if ((rc = w.ctl->ensure(sizeof(int) * CTL_INTS, s))) return rc;
+  w.rb.ctl = w.ctl->as<int>();
+  for (auto& ev : j.ev)
+    if ((rc = take_event(e, &ev))) return rc;
+  if ((rc = take_event(e, &j.done))) return rc;
+  if ((rc = take_status(e, &j.status))) return rc;
+  j.results = results;
+  j.n_results = n_results;
+  const size_t resBytes = sizeof(int32_t) * n_results;
+  if (resBytes && !is_pinned(results) && (rc = take_staging(e, resBytes, &j.staged, &j.staged_bytes)))
+    return rc;
+
+  CUDA_TRY(cudaEventRecord(j.ev[0], s));
+  CUDA_TRY(cudaMemsetAsync(w.rb.ctl, 0, sizeof(int) * CTL_INTS, s));
+  e->n_timed = 0;
+  int32_t* d_in = w.inputs->as<int32_t>();
+  const long usedTiles = m.last < 0 ? 0 : m.last / std::max(1, a.max_batches) + 1;
+  const size_t seqWords = (size_t)usedTiles * seqWordsPerTile;
+  const size_t metaWords = (size_t)usedTiles * a.max_batches * 4;
+  const size_t metaTotal = (size_t)totalSlots * 4;
+  if (seqWords)
+    CUDA_TRY(cudaMemcpyAsync(d_in, inputs, sizeof(int32_t) * seqWords, cudaMemcpyHostToDevice, s));
+  if (metaWords)
+    CUDA_TRY(cudaMemcpyAsync(d_in + metaOffset, inputs + metaOffset, sizeof(int32_t) * metaWords,
+                             cudaMemcpyHostToDevice, s));
+  if (metaTotal > metaWords)
+    CUDA_TRY(cudaMemsetAsync(d_in + metaOffset + metaWords, 0, sizeof(int32_t) * (metaTotal - metaWords), s));
+  CUDA_TRY(cudaEventRecord(j.ev[1], s));
+  int launches = 1;
+  int* d_res = w.results->as<int>();
+  if ((rc = launch_wire(e, w.pairs, w.rb, s, d_in, d_res, m.maxA, m.maxB, &launches))) return rc;
+  CUDA_TRY(cudaEventRecord(j.ev[2], s));
+  CUDA_TRY(cudaMemcpyAsync(&j.status->st, w.rb.ctl + CTL_STATUS, sizeof(DevStatus), cudaMemcpyDeviceToHost, s));
+  if (resBytes)
+    CUDA_TRY(cudaMemcpyAsync(j.staged ? j.staged : results, d_res, resBytes, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaEventRecord(j.done, s));
+  j.stats.cells = m.cells;
+  j.stats.pairs = totalSlots;
+  j.stats.launches = launches;
+  j.stats.chunks = 1;
   return IPUMA_OK;
 }
 
@@ -1631,7 +1839,8 @@ int ipuma_gpu_run_buffer_device(ipuma_engine* e, const int32_t* d_inputs, size_t
     return fail(IPUMA_ERR_TOO_LONG, "sequence longer than 65535 (ranges are uint16)");
   int launches = 1;
   CUDA_TRY(cudaEventRecord(e->ev[1], s));
-  if ((rc = launch_wire(e, s, d_inputs, d_results, info[0], info[1], &launches))) return rc;
+  if ((rc = launch_wire(e, &e->d_pairs, main_bufs(e), s, d_inputs, d_results, info[0], info[1], &launches)))
+    return rc;
   CUDA_TRY(cudaEventRecord(e->ev[2], s));
   if ((rc = check_status(e, s))) return rc;
   float ms = 0;
@@ -1660,19 +1869,19 @@ int ipuma_gpu_submit_buffer(ipuma_engine* e, const int32_t* inputs, size_t n_inp
   CUDA_TRY(cudaSetDevice(e->device));
   int rc;
   if (e->scheduler == 0 && (rc = maybe_autotune(e))) return rc;
-  e->stats = ipuma_stats{};
-  int launches = 0;
-  int64_t cells = 0;
-  CUDA_TRY(cudaEventRecord(e->ev[0], e->stream));
-  rc = enqueue_buffer(e, inputs, n_inputs, results, n_results, &launches, &cells);
-  if (rc) return rc;
   Job j;
-  CUDA_TRY(cudaEventCreateWithFlags(&j.done, cudaEventDisableTiming));
-  CUDA_TRY(cudaEventRecord(j.done, e->stream));
-  CUDA_TRY(cudaEventRecord(e->ev[3], e->stream));
-  e->stats.cells = cells;
-  e->stats.pairs = (int64_t)e->algo.tiles_used * e->algo.max_batches;
-  e->stats.launches = launches;
+  rc = enqueue_buffer(e, inputs, n_inputs, results, n_results, j);
+  if (rc) {
+    // Nothing of a failed submission is joined: wait for what it enqueued
+    // before its resources go back to the pools.
+    if (j.done || j.ev[0]) {
+      cudaStreamSynchronize(e->stream);
+      if (e->wstream1) cudaStreamSynchronize(e->wstream1);
+    }
+    recycle_job(e, j);
+    return rc;
+  }
+  e->stats = j.stats;
   *job = e->next_job++;
   e->jobs[*job] = j;
   return IPUMA_OK;
@@ -1694,7 +1903,7 @@ int ipuma_gpu_poll(ipuma_engine* e, uint64_t job, int32_t* done) {
   return IPUMA_OK;
 }
 
-int ipuma_gpu_join(ipuma_engine* e, uint64_t job, int64_t timeout_ms) {
+int ipuma_gpu_join_stats(ipuma_engine* e, uint64_t job, int64_t timeout_ms, ipuma_stats* out) {
   if (!e) return fail(IPUMA_ERR_INVALID_ARG, "null engine");
   cudaEvent_t ev;
   {
@@ -1719,19 +1928,37 @@ int ipuma_gpu_join(ipuma_engine* e, uint64_t job, int64_t timeout_ms) {
     }
     std::this_thread::sleep_for(std::chrono::microseconds(50));
   }
-  std::lock_guard<std::mutex> lk(e->mu);
-  int rc = check_status(e, e->stream);
-  float kms = 0, tms = 0;
-  cudaEventElapsedTime(&kms, e->ev[1], e->ev[2]);
-  cudaEventElapsedTime(&tms, e->ev[0], e->ev[3]);
-  e->stats.kernel_ms = kms;
-  e->stats.total_ms = tms;
-  auto it = e->jobs.find(job);
-  if (it != e->jobs.end()) {
-    cudaEventDestroy(it->second.done);
+  Job j;
+  {
+    std::lock_guard<std::mutex> lk(e->mu);
+    auto it = e->jobs.find(job);
+    if (it == e->jobs.end()) return fail(IPUMA_ERR_UNKNOWN_JOB, "job %llu already joined", (unsigned long long)job);
+    j = it->second;
     e->jobs.erase(it);
   }
-  return rc;
+  // Everything the job enqueued has finished: its staging, status and
+  // events are only read here.
+  if (j.staged) std::memcpy(j.results, j.staged, sizeof(int32_t) * j.n_results);
+  float kms = 0, tms = 0;
+  cudaEventElapsedTime(&kms, j.ev[1], j.ev[2]);
+  cudaEventElapsedTime(&tms, j.ev[0], j.done);
+  j.stats.kernel_ms = kms;
+  j.stats.total_ms = tms;
+  j.stats.overflow_reruns = j.status->st.overflow_count;
+  const int err = j.status->st.error;
+  {
+    std::lock_guard<std::mutex> lk(e->mu);
+    e->stats = j.stats;
+    if (out) *out = j.stats;
+    recycle_job(e, j);
+  }
+  if (err == ERR_LENGTH) return fail(IPUMA_ERR_TOO_LONG, "a pair exceeds the stated maximum length");
+  if (err) return fail(IPUMA_ERR_DEVICE, "kernel status error %d", err);
+  return IPUMA_OK;
+}
+
+int ipuma_gpu_join(ipuma_engine* e, uint64_t job, int64_t timeout_ms) {
+  return ipuma_gpu_join_stats(e, job, timeout_ms, nullptr);
 }
 
 }  // extern "C"

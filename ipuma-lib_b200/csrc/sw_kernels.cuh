@@ -97,24 +97,38 @@ __device__ __forceinline__ void align_pairs(const SwConst& sc, uint8_t* s_prof,
     const bool empty = alen[h] <= 0 || blen[h] <= 0;
     ps[h] = PassSeq{a0[h], b0[h], empty ? 0 : alen[h], empty ? 0 : blen[h], 1, 1};
   }
-  const bool done = sw_pass<T, K, LANES>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, fw);
 #pragma unroll
-  for (int h = 0; h < NP; ++h) {
-    ovf[h] = (NP == 2) && (!done || fw[h].s > sc.s16Limit);
-    rv[h] = Best{0, 0, 0};
+  for (int h = 0; h < NP; ++h) rv[h] = Best{0, 0, 0};
+  if (sc.forwardOnly) {
+    const bool done = sw_pass<T, K, LANES>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, fw);
+#pragma unroll
+    for (int h = 0; h < NP; ++h) ovf[h] = (NP == 2) && (!done || fw[h].s > sc.s16Limit);
+    return;
   }
-  if (!sc.forwardOnly) {
-    PassSeq rs[NP];
+  // With start coordinates both passes run through one copy of sw_pass: two
+  // inlined copies alternating in the instruction cache slowed both down.
+  // (A forward-only launch runs only the copy above.)
+#pragma unroll 1
+  for (int pass = 0; pass < 2; ++pass) {
+    Best res[NP];
+    const bool done = sw_pass<T, K, LANES>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, res);
+    if (pass == 1) {
+#pragma unroll
+      for (int h = 0; h < NP; ++h) rv[h] = res[h];
+      break;
+    }
     bool any = false;
 #pragma unroll
     for (int h = 0; h < NP; ++h) {
+      fw[h] = res[h];
+      ovf[h] = (NP == 2) && (!done || fw[h].s > sc.s16Limit);
       const bool run = !ovf[h] && fw[h].s > 0;
       any |= run;
-      rs[h] = run ? PassSeq{a0[h] + fw[h].j, b0[h] + fw[h].i, fw[h].j + 1, fw[h].i + 1, -1, -1}
+      ps[h] = run ? PassSeq{a0[h] + fw[h].j, b0[h] + fw[h].i, fw[h].j + 1, fw[h].i + 1, -1, -1}
                   : PassSeq{a0[h], b0[h], 0, 0, 1, 1};
     }
     // Uniform across the warp: every group takes part in the shuffles.
-    if (__any_sync(FULL, any)) sw_pass<T, K, LANES>(sc, s_prof, s_simp, s_bring, rs, scr, rowsCap, rv);
+    if (!__any_sync(FULL, any)) break;
   }
 }
 
@@ -157,21 +171,36 @@ __device__ __forceinline__ void align_pairs_hybrid(const SwConst& sc, uint8_t* s
     const bool empty = alen[h] <= 0 || blen[h] <= 0;
     ps[h] = PassSeq{a0[h], b0[h], empty ? 0 : alen[h], empty ? 0 : blen[h], 1, 1};
   }
-  const bool done = hybrid_pass<K>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, fw);
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    ovf[h] = !done;
-    rv[h] = Best{0, 0, 0};
+  for (int h = 0; h < 2; ++h) rv[h] = Best{0, 0, 0};
+  if (sc.forwardOnly) {
+    const bool done = hybrid_pass<K>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, fw);
+    ovf[0] = ovf[1] = !done;
+    return;
   }
-  if (done && !sc.forwardOnly) {
-    PassSeq rs[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h)
-      rs[h] = fw[h].s > 0 ? PassSeq{a0[h] + fw[h].j, b0[h] + fw[h].i, fw[h].j + 1, fw[h].i + 1, -1, -1}
-                          : PassSeq{a0[h], b0[h], 0, 0, 1, 1};
-    if (!hybrid_pass<K>(sc, s_prof, s_simp, s_bring, rs, scr, rowsCap, rv)) {
-      ovf[0] = ovf[1] = true;
+  // With start coordinates one copy of the hybrid pass serves both
+  // directions (as align_pairs).
+#pragma unroll 1
+  for (int pass = 0; pass < 2; ++pass) {
+    Best res[2];
+    const bool done = hybrid_pass<K>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, res);
+    if (pass == 1) {
+      if (done) {
+        rv[0] = res[0];
+        rv[1] = res[1];
+      } else {
+        ovf[0] = ovf[1] = true;
+      }
+      break;
     }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      fw[h] = res[h];
+      ovf[h] = !done;
+      ps[h] = fw[h].s > 0 ? PassSeq{a0[h] + fw[h].j, b0[h] + fw[h].i, fw[h].j + 1, fw[h].i + 1, -1, -1}
+                          : PassSeq{a0[h], b0[h], 0, 0, 1, 1};
+    }
+    if (!done) break;
   }
 }
 

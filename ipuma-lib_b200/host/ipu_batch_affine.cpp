@@ -60,15 +60,13 @@ void encodeInto(const std::vector<uint8_t>& table, swatlib::DataType dtype, cons
 
 void Job::join() {
   if (joined) return;
-  const int rc = ipuma_gpu_join(engine, id, -1);
+  ipuma_stats st{};
+  const int rc = ipuma_gpu_join_stats(engine, id, -1, &st);
   joined = true;
   tick.tock();
-  ipuma_stats st{};
-  if (ipuma_gpu_last_stats(engine, &st) == IPUMA_OK) {
-    h2dCycles = static_cast<uint64_t>(st.total_ms * 1e6);
-    innerCycles = static_cast<uint64_t>(st.kernel_ms * 1e6);
-  }
   if (rc != IPUMA_OK) raise("batch failed");
+  h2dCycles = static_cast<uint64_t>(st.total_ms * 1e6);
+  innerCycles = static_cast<uint64_t>(st.kernel_ms * 1e6);
 }
 
 SWAlgorithm::SWAlgorithm(SWConfig config, IPUAlgoConfig algoconfig, int thread_id, size_t slotCap, size_t ipuCount,

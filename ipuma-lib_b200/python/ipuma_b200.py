@@ -41,7 +41,7 @@ EXPORTS = [
     "ipuma_gpu_autotune", "ipuma_gpu_tuning", "ipuma_server_create", "ipuma_server_submit",
     "ipuma_server_poll", "ipuma_server_wait", "ipuma_server_get_stats", "ipuma_server_close",
     "ipuma_server_destroy", "ipuma_server_add_sequences", "ipuma_server_submit_resident",
-    "ipuma_gpu_reserve",
+    "ipuma_gpu_reserve", "ipuma_gpu_join_stats", "ipuma_host_alloc", "ipuma_host_free",
 ]
 
 KERNEL_NAMES = {0: "k_batched<s32,L32,K16>", 1: "k_batched<s16x2,L16,K4>",
@@ -132,6 +132,7 @@ def lib():
         L.ipuma_gpu_submit_buffer.argtypes = [vp, vp, sz, vp, sz, ctypes.POINTER(ctypes.c_uint64)]
         L.ipuma_gpu_poll.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(i32)]
         L.ipuma_gpu_join.argtypes = [vp, ctypes.c_uint64, i64]
+        L.ipuma_gpu_join_stats.argtypes = [vp, ctypes.c_uint64, i64, ctypes.POINTER(Stats)]
         L.ipuma_gpu_compare.argtypes = [vp, vp, sz, vp, i32, vp, vp, vp]
         L.ipuma_gpu_compare_device.argtypes = [vp, vp, sz, vp, i32, i32, i32, vp, vp, vp, vp]
         L.ipuma_gpu_last_stats.argtypes = [vp, ctypes.POINTER(Stats)]
@@ -322,6 +323,12 @@ class Engine:
 
     def join(self, job: int, timeout_ms: int = -1):
         _check(lib().ipuma_gpu_join(self.h, job, timeout_ms))
+
+    def join_stats(self, job: int, timeout_ms: int = -1) -> "Stats":
+        """join() returning the job's own statistics."""
+        st = Stats()
+        _check(lib().ipuma_gpu_join_stats(self.h, job, timeout_ms, ctypes.byref(st)))
+        return st
 
 
 def compare_noalloc(sw: SwConfig, forward_only: bool, d_codes: int, n_codes: int, d_pairs: int,
