@@ -216,6 +216,7 @@ struct ipuma_engine {
   int timed_cls[kMaxTimed] = {};
 
   DevBuf d_sim, d_codes, d_pairs, d_list, d_res, d_scratch, d_cf, d_ovf, d_ctl, d_inputs, d_wres, d_flag;
+  DevBuf d_packed;  // 4-bit codes of ipuma_gpu_compare_packed before expansion
   // Second buffer set and streams of the chunked host-to-host path
   // (ipuma_gpu_compare): chunks alternate between `stream` and `stream2`
   // while `copy_stream` uploads the next chunks.
@@ -1275,6 +1276,33 @@ int ipuma_encode(int32_t datatype, const char* s, size_t n, uint8_t* out) {
   return IPUMA_OK;
 }
 
+int ipuma_pack_codes4(const uint8_t* codes, size_t n, uint8_t* out) {
+  if ((!codes || !out) && n) return fail(IPUMA_ERR_INVALID_ARG, "null pointer");
+  const size_t bytes = (n + 1) / 2;
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int nthr = (int)std::max<size_t>(1, std::min<size_t>({(size_t)16, (size_t)hw, bytes >> 22}));
+  std::vector<size_t> bad(nthr, SIZE_MAX);
+  auto work = [&](int t) {
+    const size_t b0 = bytes * t / nthr, b1 = bytes * (t + 1) / nthr;
+    for (size_t b = b0; b < b1; ++b) {
+      const uint8_t lo = codes[2 * b];
+      const uint8_t hi = (2 * b + 1 < n) ? codes[2 * b + 1] : 0;
+      if ((lo | hi) > 15) {
+        bad[t] = (lo > 15) ? 2 * b : 2 * b + 1;
+        return;
+      }
+      out[b] = (uint8_t)(lo | (hi << 4));
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nthr; ++t) pool.emplace_back(work, t);
+  work(0);
+  for (auto& th : pool) th.join();
+  for (size_t b : bad)
+    if (b != SIZE_MAX) return fail(IPUMA_ERR_BAD_SEQUENCE, "code %u at %zu does not fit 4 bits", codes[b], b);
+  return IPUMA_OK;
+}
+
 int ipuma_select_matrix(int32_t similarity, int32_t match, int32_t mismatch, int32_t ambiguity,
                         int8_t* out, size_t out_cap, int32_t* m, int32_t* n) {
   try {
@@ -1381,7 +1409,7 @@ void ipuma_gpu_destroy(ipuma_engine* e) {
   for (void* p : e->pinned_blocks) cudaFreeHost(p);
   if (e->stream2) cudaStreamSynchronize(e->stream2);
   if (e->copy_stream) cudaStreamSynchronize(e->copy_stream);
-  for (auto* b : {&e->d_sim, &e->d_codes, &e->d_pairs, &e->d_list, &e->d_res, &e->d_scratch, &e->d_cf,
+  for (auto* b : {&e->d_sim, &e->d_codes, &e->d_packed, &e->d_pairs, &e->d_list, &e->d_res, &e->d_scratch, &e->d_cf,
                   &e->d_ovf, &e->d_ctl, &e->d_inputs, &e->d_wres, &e->d_flag, &e->x_list, &e->x_scratch,
                   &e->x_ovf, &e->x_flag, &e->w1.inputs, &e->w1.results, &e->w1.pairs, &e->w1.ctl, &e->w1.list,
                   &e->w1.scratch, &e->w1.ovf, &e->w1.flag})
@@ -1562,8 +1590,11 @@ int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_c
   return IPUMA_OK;
 }
 
-int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes, const ipuma_pair* pairs,
-                      int32_t n, int32_t* score, int32_t* arange, int32_t* brange) {
+// Host-buffer compare of ipuma_gpu_compare (bits = 8: one byte per
+// residue) and ipuma_gpu_compare_packed (bits = 4: two residues per byte,
+// expanded on the device after each upload).
+static int compare_host(ipuma_engine* e, const uint8_t* codes, size_t n_codes, int bits, const ipuma_pair* pairs,
+                        int32_t n, int32_t* score, int32_t* arange, int32_t* brange) {
   if (!e) return fail(IPUMA_ERR_INVALID_ARG, "null engine");
   if (n < 0) return fail(IPUMA_ERR_INVALID_ARG, "negative pair count");
   if (n == 0) return IPUMA_OK;
@@ -1609,6 +1640,23 @@ int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes, con
   if ((rc = e->d_codes.ensure(std::max<size_t>(n_codes, 1), s))) return rc;
   if ((rc = e->d_pairs.ensure(sizeof(ipuma_pair) * (size_t)n, s))) return rc;
   if ((rc = e->d_res.ensure(sizeof(int32_t) * 3 * (size_t)n, s))) return rc;
+  // k_unpack4 reads whole 8-byte words around each range.
+  if (bits == 4 && (rc = e->d_packed.ensure(((n_codes + 1) / 2 + 31) & ~(size_t)15, s))) return rc;
+  // Puts residues [lo, hi) into d_codes on stream `us`.
+  auto upload = [&](size_t lo, size_t hi, cudaStream_t us) -> int {
+    if (lo >= hi) return IPUMA_OK;
+    if (bits == 8) {
+      CUDA_TRY(cudaMemcpyAsync(e->d_codes.as<uint8_t>() + lo, codes + lo, hi - lo, cudaMemcpyHostToDevice, us));
+      return IPUMA_OK;
+    }
+    const size_t blo = lo / 2, bhi = (hi + 1) / 2;
+    CUDA_TRY(cudaMemcpyAsync(e->d_packed.as<uint8_t>() + blo, codes + blo, bhi - blo, cudaMemcpyHostToDevice, us));
+    const size_t blocks16 = (hi - (lo & ~(size_t)15) + 15) / 16;
+    const int grid = (int)std::max<size_t>(1, std::min<size_t>((blocks16 + 255) / 256, (size_t)e->nsm * 8));
+    k_unpack4<<<grid, 256, 0, us>>>(e->d_packed.as<uint8_t>(), lo, hi, e->d_codes.as<uint8_t>());
+    CUDA_TRY(cudaGetLastError());
+    return IPUMA_OK;
+  };
   e->stats = ipuma_stats{};
   int launches = 0;
   int32_t* d_score = e->d_res.as<int32_t>();
@@ -1617,7 +1665,7 @@ int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes, con
   if (nch == 1) {
     if ((rc = reset_ctl(e, s))) return rc;
     CUDA_TRY(cudaEventRecord(e->ev[0], s));
-    CUDA_TRY(cudaMemcpyAsync(e->d_codes.p, codes, n_codes, cudaMemcpyHostToDevice, s));
+    if ((rc = upload(0, n_codes, s))) return rc;
     CUDA_TRY(cudaMemcpyAsync(e->d_pairs.p, pairs, sizeof(ipuma_pair) * (size_t)n, cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaEventRecord(e->ev[1], s));
     rc = run_batched(e, main_bufs(e), s, e->d_codes.as<uint8_t>(), e->d_pairs.as<PairDesc>(), n, maxA, maxB,
@@ -1661,8 +1709,7 @@ int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes, con
       for (int r = 0; r < 2; ++r)
         if (span[k].lo[r] < span[k].hi[r]) take_range(have, span[k].lo[r], span[k].hi[r], todo);
       for (const auto& r : todo)
-        CUDA_TRY(cudaMemcpyAsync(e->d_codes.as<uint8_t>() + r.first, codes + r.first, r.second - r.first,
-                                 cudaMemcpyHostToDevice, e->copy_stream));
+        if ((rc = upload(r.first, r.second, e->copy_stream))) return rc;
       CUDA_TRY(cudaMemcpyAsync(e->d_pairs.as<ipuma_pair>() + off, pairs + off, sizeof(ipuma_pair) * (size_t)nk,
                                cudaMemcpyHostToDevice, e->copy_stream));
       CUDA_TRY(cudaEventRecord(e->cev[k], e->copy_stream));
@@ -1700,6 +1747,18 @@ int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes, con
   e->stats.launches = launches;
   e->stats.chunks = nch;
   return IPUMA_OK;
+}
+
+int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes, const ipuma_pair* pairs,
+                      int32_t n, int32_t* score, int32_t* arange, int32_t* brange) {
+  return compare_host(e, codes, n_codes, 8, pairs, n, score, arange, brange);
+}
+
+int ipuma_gpu_compare_packed(ipuma_engine* e, const uint8_t* packed, size_t n_codes, const ipuma_pair* pairs,
+                             int32_t n, int32_t* score, int32_t* arange, int32_t* brange) {
+  if (!e) return fail(IPUMA_ERR_INVALID_ARG, "null engine");
+  if (e->M > 16) return fail(IPUMA_ERR_INVALID_ARG, "4-bit codes need an alphabet of at most 16 letters (this one has %d)", e->M);
+  return compare_host(e, packed, n_codes, 4, pairs, n, score, arange, brange);
 }
 
 // Launches the alignment work of a wire buffer already on the device

@@ -750,6 +750,35 @@ static __global__ void k_wire_check(const int* __restrict__ inputs, long metaOff
   }
 }
 
+// Expands 4-bit residue codes (two per byte, the lower-indexed residue in
+// the low nibble) of residues [lo, hi) into one byte per residue.  Writes
+// exactly that range: other ranges of `codes` may be read by kernels on
+// other streams meanwhile.  Reads whole 8-byte words of `packed` around the
+// range; the caller pads the packed buffer to cover them.
+static __global__ void k_unpack4(const uint8_t* __restrict__ packed, size_t lo, size_t hi,
+                                 uint8_t* __restrict__ codes) {
+  const size_t stride = (size_t)16 * gridDim.x * blockDim.x;
+  for (size_t blk = (lo & ~(size_t)15) + (size_t)16 * (blockIdx.x * blockDim.x + threadIdx.x); blk < hi;
+       blk += stride) {
+    const uint2 w = *reinterpret_cast<const uint2*>(packed + blk / 2);
+    // 16 packed bits (4 residues) -> 4 bytes.
+    auto spread = [](uint32_t v) -> uint32_t {
+      return (v & 0x000Fu) | ((v & 0x00F0u) << 4) | ((v & 0x0F00u) << 8) | ((v & 0xF000u) << 12);
+    };
+    const uint4 out = make_uint4(spread(w.x & 0xFFFFu), spread(w.x >> 16), spread(w.y & 0xFFFFu), spread(w.y >> 16));
+    if (blk >= lo && blk + 16 <= hi) {
+      *reinterpret_cast<uint4*>(codes + blk) = out;
+    } else {
+      const uint32_t o[4] = {out.x, out.y, out.z, out.w};
+#pragma unroll
+      for (int b = 0; b < 16; ++b) {
+        const size_t p = blk + b;
+        if (p >= lo && p < hi) codes[p] = (uint8_t)(o[b >> 2] >> (8 * (b & 3)));
+      }
+    }
+  }
+}
+
 // Wire buffer -> pair list: slot g of tile g / maxBatches, offsets made
 // absolute in bytes from the start of the input buffer.
 static __global__ void k_wire_to_pairs(const int* __restrict__ inputs, long seqWordsPerTile, long metaOffset,

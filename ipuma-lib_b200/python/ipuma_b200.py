@@ -42,6 +42,7 @@ EXPORTS = [
     "ipuma_server_poll", "ipuma_server_wait", "ipuma_server_get_stats", "ipuma_server_close",
     "ipuma_server_destroy", "ipuma_server_add_sequences", "ipuma_server_submit_resident",
     "ipuma_gpu_reserve", "ipuma_gpu_join_stats", "ipuma_host_alloc", "ipuma_host_free",
+    "ipuma_gpu_compare_packed", "ipuma_pack_codes4",
 ]
 
 KERNEL_NAMES = {0: "k_batched<s32,L32,K16>", 1: "k_batched<s16x2,L16,K4>",
@@ -134,6 +135,8 @@ def lib():
         L.ipuma_gpu_join.argtypes = [vp, ctypes.c_uint64, i64]
         L.ipuma_gpu_join_stats.argtypes = [vp, ctypes.c_uint64, i64, ctypes.POINTER(Stats)]
         L.ipuma_gpu_compare.argtypes = [vp, vp, sz, vp, i32, vp, vp, vp]
+        L.ipuma_gpu_compare_packed.argtypes = [vp, vp, sz, vp, i32, vp, vp, vp]
+        L.ipuma_pack_codes4.argtypes = [vp, sz, vp]
         L.ipuma_gpu_compare_device.argtypes = [vp, vp, sz, vp, i32, i32, i32, vp, vp, vp, vp]
         L.ipuma_gpu_last_stats.argtypes = [vp, ctypes.POINTER(Stats)]
         L.ipuma_gpu_run_buffer_device.argtypes = [vp, vp, sz, vp, sz, vp]
@@ -193,6 +196,19 @@ def encode(datatype: str, s: str) -> np.ndarray:
     b = s.encode("latin-1")
     out = np.zeros(len(b), dtype=np.uint8)
     _check(lib().ipuma_encode(DT[datatype], b, len(b), _ptr(out)))
+    return out
+
+
+def pack_codes4(codes: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
+    """Packs codes (each < 16) two per byte, residue 2k in the low nibble
+    of byte k (ipuma_pack_codes4); `out` may be a preallocated (e.g. pinned)
+    uint8 array of (n + 1) // 2 bytes."""
+    codes = np.ascontiguousarray(codes, dtype=np.uint8)
+    nb = (codes.size + 1) // 2
+    if out is None:
+        out = np.zeros(nb, dtype=np.uint8)
+    assert out.dtype == np.uint8 and out.size >= nb and out.flags.c_contiguous
+    _check(lib().ipuma_pack_codes4(_ptr(codes), codes.size, _ptr(out)))
     return out
 
 
@@ -287,6 +303,21 @@ class Engine:
         """Like compare() but into caller buffers (e.g. pinned host arrays)."""
         _check(lib().ipuma_gpu_compare(self.h, _ptr(codes), codes.size, _ptr(pairs),
                                        pairs.shape[0], _ptr(score), _ptr(ar), _ptr(br)))
+
+    def compare_packed(self, packed: np.ndarray, n_codes: int, pairs: np.ndarray):
+        """compare() on 4-bit packed codes (pack_codes4); n_codes residues."""
+        packed = np.ascontiguousarray(packed, dtype=np.uint8)
+        assert packed.size >= (n_codes + 1) // 2
+        pairs = np.ascontiguousarray(pairs, dtype=PAIR_DTYPE)
+        n = pairs.shape[0]
+        out = [np.zeros(n, dtype=np.int32) for _ in range(3)]
+        self.compare_packed_into(packed, n_codes, pairs, *out)
+        return tuple(out)
+
+    def compare_packed_into(self, packed: np.ndarray, n_codes: int, pairs: np.ndarray, score, ar, br):
+        """compare_packed() into caller buffers (e.g. pinned host arrays)."""
+        _check(lib().ipuma_gpu_compare_packed(self.h, _ptr(packed), n_codes, _ptr(pairs),
+                                              pairs.shape[0], _ptr(score), _ptr(ar), _ptr(br)))
 
     def compare_device(self, d_codes: int, n_codes: int, d_pairs: int, n: int, max_a: int,
                        max_b: int, d_score: int, d_ar: int, d_br: int, stream: int = 0):

@@ -68,3 +68,26 @@ def test_create_without_device_fails_cleanly():
     with pytest.raises(ib.IpumaError) as ei:
         ib.Engine(ib.sw_config())
     assert ei.value.code == ib.ERR_NO_DEVICE
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 7, 64, 100_001, (1 << 23) + 5])
+def test_pack_codes4_layout(n):
+    """Residue 2k in the low nibble of byte k, 2k+1 in the high nibble; an
+    odd count leaves the last high nibble 0 (large inputs pack on several
+    threads)."""
+    codes = np.random.default_rng(n).integers(0, 16, n).astype(np.uint8)
+    packed = ib.pack_codes4(codes)
+    assert packed.size == (n + 1) // 2
+    want = np.zeros((n + 1) // 2 * 2, np.uint8)
+    want[:n] = codes
+    np.testing.assert_array_equal(packed, want[0::2] | (want[1::2] << 4))
+
+
+def test_pack_codes4_rejects_codes_above_15():
+    codes = np.zeros(5_000_000, np.uint8)
+    codes[3_000_001] = 16
+    codes[4_000_000] = 200
+    with pytest.raises(ib.IpumaError) as ei:
+        ib.pack_codes4(codes)
+    assert ei.value.code == ib.ERR_BAD_SEQUENCE
+    assert "3000001" in str(ei.value)
