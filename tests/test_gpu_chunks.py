@@ -115,7 +115,8 @@ def test_chunked_into_pinned_buffers():
 
 def test_automatic_chunking_of_a_large_batch():
     """From 500,000 pairs and 32 MB of codes the call chunks by itself (one
-    chunk per 250,000 pairs); the pairs are checked on several host threads."""
+    chunk per 333,334 pairs, at least 2); the pairs are checked on several host
+    threads."""
     wl = workloads.dna_batched(n=520_000, seed=45)
     pairs = ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len)
     assert wl.codes.size >= 32 << 20
