@@ -505,9 +505,9 @@ def main():
         peng.close()
 
     # End to end through the host-buffer C ABI call, pinned host memory.
-    # Nucleic-acid codes (< 16) go through ipuma_gpu_compare_packed, two
-    # residues per byte (packed once, like the encoding, before timing);
-    # the one-byte path is timed beside it.
+    # Nucleic-acid codes go through ipuma_gpu_compare_packed, four (A/C/G/T
+    # only) or two residues per byte (packed once, like the encoding, before
+    # timing); the one-byte path is timed beside it.
     e2e = None
     if not args.no_e2e:
         h_codes = torch.from_numpy(wl.codes).pin_memory()
@@ -517,15 +517,19 @@ def main():
         pairs_view = h_pairs.numpy().view(ib.PAIR_DTYPE)
         out_np = h_out.numpy()
         packed_np = None
+        bits = 0
         if wl.datatype == "na":
-            h_packed = torch.empty((wl.codes.size + 1) // 2, dtype=torch.uint8).pin_memory()
-            packed_np = ib.pack_codes4(wl.codes, h_packed.numpy())
+            # 2 bits when every residue is A, C, G or T (codes 1..4), else 4.
+            bits = 2 if bool(((wl.codes >= 1) & (wl.codes <= 4)).all()) else 4
+            h_packed = torch.empty((wl.codes.size * bits + 7) // 8, dtype=torch.uint8).pin_memory()
+            packed_np = ib.pack_codes(wl.codes, bits, h_packed.numpy())
 
         def run_bytes():
             eng.compare_into(codes_np, pairs_view, out_np[0], out_np[1], out_np[2])
 
         def run_packed():
-            eng.compare_packed_into(packed_np, wl.codes.size, pairs_view, out_np[0], out_np[1], out_np[2])
+            eng.compare_packed_into(packed_np, wl.codes.size, pairs_view, out_np[0], out_np[1], out_np[2],
+                                    bits=bits)
 
         def time_call(call):
             for _ in range(max(1, args.warmup)):
@@ -550,7 +554,7 @@ def main():
                    "h2d_bytes_per_step": int(packed_np.nbytes + pairs_np.nbytes),
                    "d2h_bytes_per_step": int(3 * 4 * wl.n), "ms_per_step": wall * 1e3,
                    "bit_identical_to_device_run": same, "chunks": chunks,
-                   "call": "ipuma_gpu_compare_packed (4-bit codes, expanded on the device)",
+                   "call": "ipuma_gpu_compare_packed (%d-bit codes, expanded on the device)" % bits,
                    "bytes_path": bytes_path}
         else:
             e2e = {"value": bytes_path["value"], "unit": "GCUPS",

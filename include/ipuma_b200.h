@@ -23,7 +23,7 @@
  *   ipuma_gpu_poll          (non-blocking form of Job::join, :489-494)
  *   ipuma_gpu_compare       compare_local minus the host partitioning
  *                           (:564-663): pairs straight from a code array
- *   ipuma_gpu_compare_packed  the same with 4-bit packed codes
+ *   ipuma_gpu_compare_packed  the same with 2- or 4-bit packed codes
  *   ipuma_gpu_compare_device  the same with device-resident buffers
  *   ipuma_encode            swatlib::Encoding::encode  src/swatlib/encoding.cpp:38-60
  *   ipuma_select_matrix     swatlib::selectMatrix      src/swatlib/similarity.cpp:89-105
@@ -171,9 +171,10 @@ int ipuma_host_alloc(size_t bytes, void** out);
 void ipuma_host_free(void* p);
 
 /* Host-only helpers (no GPU needed). */
-/* Packs n codes (each < 16) two per byte into out[(n + 1) / 2] for
- * ipuma_gpu_compare_packed; a code >= 16 gives IPUMA_ERR_BAD_SEQUENCE. */
-int ipuma_pack_codes4(const uint8_t* codes, size_t n, uint8_t* out);
+/* Packs n codes for ipuma_gpu_compare_packed into out[ceil(n * bits / 8)]:
+ * bits = 4 takes codes < 16, bits = 2 takes A, T, C, G (codes 1..4); any
+ * other code gives IPUMA_ERR_BAD_SEQUENCE. */
+int ipuma_pack_codes(const uint8_t* codes, size_t n, int32_t bits, uint8_t* out);
 /* Encodes n chars into codes; unknown NA characters (code 16, which has no
  * row in the 16x16 NA matrix) are rejected with IPUMA_ERR_BAD_SEQUENCE. */
 int ipuma_encode(int32_t datatype, const char* s, size_t n, uint8_t* out);
@@ -260,12 +261,15 @@ int ipuma_gpu_join_stats(ipuma_engine* e, uint64_t job, int64_t timeout_ms, ipum
 int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes,
                       const ipuma_pair* pairs, int32_t n, int32_t* score, int32_t* arange,
                       int32_t* brange);
-/* ipuma_gpu_compare with the codes packed two per byte (residue 2k in the
- * low nibble of byte k, 2k+1 in the high nibble; ipuma_pack_codes4), for
- * alphabets of at most 16 codes (nucleic acids).  n_codes, offsets and
- * lengths count residues.  Halves the host-to-device bytes; each uploaded
- * range is expanded on the device before its pairs run. */
-int ipuma_gpu_compare_packed(ipuma_engine* e, const uint8_t* packed, size_t n_codes,
+/* ipuma_gpu_compare with packed codes (ipuma_pack_codes), for alphabets of
+ * at most 16 codes (nucleic acids):
+ *   bits = 4: two residues per byte, residue 2k in the low nibble of byte k;
+ *   bits = 2: four per byte, residue 4k+q in bits 2q..2q+1 of byte k holding
+ *             code - 1 (A, T, C, G only: codes 1..4).
+ * n_codes, offsets and lengths count residues.  Halves (quarters) the
+ * host-to-device bytes; each uploaded range is expanded on the device
+ * before its pairs run. */
+int ipuma_gpu_compare_packed(ipuma_engine* e, const uint8_t* packed, size_t n_codes, int32_t bits,
                              const ipuma_pair* pairs, int32_t n, int32_t* score, int32_t* arange,
                              int32_t* brange);
 /* Same with every buffer in device memory, enqueued on `stream`

@@ -1280,22 +1280,30 @@ int ipuma_encode(int32_t datatype, const char* s, size_t n, uint8_t* out) {
   return IPUMA_OK;
 }
 
-int ipuma_pack_codes4(const uint8_t* codes, size_t n, uint8_t* out) {
+int ipuma_pack_codes(const uint8_t* codes, size_t n, int32_t bits, uint8_t* out) {
   if ((!codes || !out) && n) return fail(IPUMA_ERR_INVALID_ARG, "null pointer");
-  const size_t bytes = (n + 1) / 2;
+  if (bits != 2 && bits != 4) return fail(IPUMA_ERR_INVALID_ARG, "bits must be 2 or 4, not %d", bits);
+  const size_t per = 8 / bits;
+  const size_t bytes = (n + per - 1) / per;
   const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
   const int nthr = (int)std::max<size_t>(1, std::min<size_t>({(size_t)16, (size_t)hw, bytes >> 22}));
   std::vector<size_t> bad(nthr, SIZE_MAX);
   auto work = [&](int t) {
     const size_t b0 = bytes * t / nthr, b1 = bytes * (t + 1) / nthr;
     for (size_t b = b0; b < b1; ++b) {
-      const uint8_t lo = codes[2 * b];
-      const uint8_t hi = (2 * b + 1 < n) ? codes[2 * b + 1] : 0;
-      if ((lo | hi) > 15) {
-        bad[t] = (lo > 15) ? 2 * b : 2 * b + 1;
-        return;
+      uint32_t v = 0;
+      for (size_t q = 0; q < per; ++q) {
+        const size_t i = per * b + q;
+        if (i >= n) break;
+        // 4 bits: the code; 2 bits: code - 1 for A, T, C, G (1..4).
+        const uint32_t x = (bits == 4) ? codes[i] : (uint32_t)codes[i] - 1u;
+        if (x >= (1u << bits)) {
+          bad[t] = i;
+          return;
+        }
+        v |= x << (bits * q);
       }
-      out[b] = (uint8_t)(lo | (hi << 4));
+      out[b] = (uint8_t)v;
     }
   };
   std::vector<std::thread> pool;
@@ -1303,7 +1311,8 @@ int ipuma_pack_codes4(const uint8_t* codes, size_t n, uint8_t* out) {
   work(0);
   for (auto& th : pool) th.join();
   for (size_t b : bad)
-    if (b != SIZE_MAX) return fail(IPUMA_ERR_BAD_SEQUENCE, "code %u at %zu does not fit 4 bits", codes[b], b);
+    if (b != SIZE_MAX)
+      return fail(IPUMA_ERR_BAD_SEQUENCE, "code %u at %zu does not fit %d bits", codes[b], b, bits);
   return IPUMA_OK;
 }
 
@@ -1595,8 +1604,8 @@ int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_c
 }
 
 // Host-buffer compare of ipuma_gpu_compare (bits = 8: one byte per
-// residue) and ipuma_gpu_compare_packed (bits = 4: two residues per byte,
-// expanded on the device after each upload).
+// residue) and ipuma_gpu_compare_packed (bits = 4 or 2: two or four
+// residues per byte, expanded on the device after each upload).
 static int compare_host(ipuma_engine* e, const uint8_t* codes, size_t n_codes, int bits, const ipuma_pair* pairs,
                         int32_t n, int32_t* score, int32_t* arange, int32_t* brange) {
   if (!e) return fail(IPUMA_ERR_INVALID_ARG, "null engine");
@@ -1644,8 +1653,10 @@ static int compare_host(ipuma_engine* e, const uint8_t* codes, size_t n_codes, i
   if ((rc = e->d_codes.ensure(std::max<size_t>(n_codes, 1), s))) return rc;
   if ((rc = e->d_pairs.ensure(sizeof(ipuma_pair) * (size_t)n, s))) return rc;
   if ((rc = e->d_res.ensure(sizeof(int32_t) * 3 * (size_t)n, s))) return rc;
-  // k_unpack4 reads whole 8-byte words around each range.
-  if (bits == 4 && (rc = e->d_packed.ensure(((n_codes + 1) / 2 + 31) & ~(size_t)15, s))) return rc;
+  // The expansion kernels read whole 8- or 4-byte words around each range.
+  const size_t perByte = 8 / bits;
+  if (bits < 8 && (rc = e->d_packed.ensure(((n_codes + perByte - 1) / perByte + 31) & ~(size_t)15, s)))
+    return rc;
   // Puts residues [lo, hi) into d_codes on stream `us`.
   auto upload = [&](size_t lo, size_t hi, cudaStream_t us) -> int {
     if (lo >= hi) return IPUMA_OK;
@@ -1653,11 +1664,14 @@ static int compare_host(ipuma_engine* e, const uint8_t* codes, size_t n_codes, i
       CUDA_TRY(cudaMemcpyAsync(e->d_codes.as<uint8_t>() + lo, codes + lo, hi - lo, cudaMemcpyHostToDevice, us));
       return IPUMA_OK;
     }
-    const size_t blo = lo / 2, bhi = (hi + 1) / 2;
+    const size_t blo = lo / perByte, bhi = (hi + perByte - 1) / perByte;
     CUDA_TRY(cudaMemcpyAsync(e->d_packed.as<uint8_t>() + blo, codes + blo, bhi - blo, cudaMemcpyHostToDevice, us));
     const size_t blocks16 = (hi - (lo & ~(size_t)15) + 15) / 16;
     const int grid = (int)std::max<size_t>(1, std::min<size_t>((blocks16 + 255) / 256, (size_t)e->nsm * 8));
-    k_unpack4<<<grid, 256, 0, us>>>(e->d_packed.as<uint8_t>(), lo, hi, e->d_codes.as<uint8_t>());
+    if (bits == 4)
+      k_unpack4<<<grid, 256, 0, us>>>(e->d_packed.as<uint8_t>(), lo, hi, e->d_codes.as<uint8_t>());
+    else
+      k_unpack2<<<grid, 256, 0, us>>>(e->d_packed.as<uint8_t>(), lo, hi, e->d_codes.as<uint8_t>());
     CUDA_TRY(cudaGetLastError());
     return IPUMA_OK;
   };
@@ -1758,11 +1772,17 @@ int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes, con
   return compare_host(e, codes, n_codes, 8, pairs, n, score, arange, brange);
 }
 
-int ipuma_gpu_compare_packed(ipuma_engine* e, const uint8_t* packed, size_t n_codes, const ipuma_pair* pairs,
-                             int32_t n, int32_t* score, int32_t* arange, int32_t* brange) {
+int ipuma_gpu_compare_packed(ipuma_engine* e, const uint8_t* packed, size_t n_codes, int32_t bits,
+                             const ipuma_pair* pairs, int32_t n, int32_t* score, int32_t* arange,
+                             int32_t* brange) {
   if (!e) return fail(IPUMA_ERR_INVALID_ARG, "null engine");
-  if (e->M > 16) return fail(IPUMA_ERR_INVALID_ARG, "4-bit codes need an alphabet of at most 16 letters (this one has %d)", e->M);
-  return compare_host(e, packed, n_codes, 4, pairs, n, score, arange, brange);
+  if (bits != 2 && bits != 4) return fail(IPUMA_ERR_INVALID_ARG, "bits must be 2 or 4, not %d", bits);
+  // 2-bit codes are A, T, C, G = nucleic-acid codes 1..4.
+  if (bits == 2 && e->sw.datatype != IPUMA_DT_NUCLEIC_ACID)
+    return fail(IPUMA_ERR_INVALID_ARG, "2-bit codes are nucleic-acid codes");
+  if (e->M > 16)
+    return fail(IPUMA_ERR_INVALID_ARG, "packed codes need an alphabet of at most 16 letters (this one has %d)", e->M);
+  return compare_host(e, packed, n_codes, bits, pairs, n, score, arange, brange);
 }
 
 // Launches the alignment work of a wire buffer already on the device

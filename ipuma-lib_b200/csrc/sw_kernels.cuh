@@ -779,6 +779,35 @@ static __global__ void k_unpack4(const uint8_t* __restrict__ packed, size_t lo, 
   }
 }
 
+// Expands 2-bit residue codes (four per byte, residue 4k+q in bits 2q and
+// 2q+1 of byte k, value = code - 1: A, T, C, G = codes 1..4) of residues
+// [lo, hi) into one byte per residue; as k_unpack4, it writes exactly that
+// range and reads whole 4-byte words of `packed` around it.
+static __global__ void k_unpack2(const uint8_t* __restrict__ packed, size_t lo, size_t hi,
+                                 uint8_t* __restrict__ codes) {
+  const size_t stride = (size_t)16 * gridDim.x * blockDim.x;
+  for (size_t blk = (lo & ~(size_t)15) + (size_t)16 * (blockIdx.x * blockDim.x + threadIdx.x); blk < hi;
+       blk += stride) {
+    const uint32_t w = *reinterpret_cast<const uint32_t*>(packed + blk / 4);
+    // 8 packed bits (4 residues) -> 4 bytes, plus 1 per byte.
+    auto spread = [](uint32_t v) -> uint32_t {
+      return ((v & 0x03u) | ((v & 0x0Cu) << 6) | ((v & 0x30u) << 12) | ((v & 0xC0u) << 18)) + 0x01010101u;
+    };
+    const uint4 out = make_uint4(spread(w & 0xFFu), spread((w >> 8) & 0xFFu), spread((w >> 16) & 0xFFu),
+                                 spread(w >> 24));
+    if (blk >= lo && blk + 16 <= hi) {
+      *reinterpret_cast<uint4*>(codes + blk) = out;
+    } else {
+      const uint32_t o[4] = {out.x, out.y, out.z, out.w};
+#pragma unroll
+      for (int b = 0; b < 16; ++b) {
+        const size_t p = blk + b;
+        if (p >= lo && p < hi) codes[p] = (uint8_t)(o[b >> 2] >> (8 * (b & 3)));
+      }
+    }
+  }
+}
+
 // Wire buffer -> pair list: slot g of tile g / maxBatches, offsets made
 // absolute in bytes from the start of the input buffer.
 static __global__ void k_wire_to_pairs(const int* __restrict__ inputs, long seqWordsPerTile, long metaOffset,

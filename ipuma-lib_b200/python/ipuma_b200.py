@@ -42,7 +42,7 @@ EXPORTS = [
     "ipuma_server_poll", "ipuma_server_wait", "ipuma_server_get_stats", "ipuma_server_close",
     "ipuma_server_destroy", "ipuma_server_add_sequences", "ipuma_server_submit_resident",
     "ipuma_gpu_reserve", "ipuma_gpu_join_stats", "ipuma_host_alloc", "ipuma_host_free",
-    "ipuma_gpu_compare_packed", "ipuma_pack_codes4",
+    "ipuma_gpu_compare_packed", "ipuma_pack_codes",
 ]
 
 KERNEL_NAMES = {0: "k_batched<s32,L32,K16>", 1: "k_batched<s16x2,L16,K4>",
@@ -135,8 +135,8 @@ def lib():
         L.ipuma_gpu_join.argtypes = [vp, ctypes.c_uint64, i64]
         L.ipuma_gpu_join_stats.argtypes = [vp, ctypes.c_uint64, i64, ctypes.POINTER(Stats)]
         L.ipuma_gpu_compare.argtypes = [vp, vp, sz, vp, i32, vp, vp, vp]
-        L.ipuma_gpu_compare_packed.argtypes = [vp, vp, sz, vp, i32, vp, vp, vp]
-        L.ipuma_pack_codes4.argtypes = [vp, sz, vp]
+        L.ipuma_gpu_compare_packed.argtypes = [vp, vp, sz, i32, vp, i32, vp, vp, vp]
+        L.ipuma_pack_codes.argtypes = [vp, sz, i32, vp]
         L.ipuma_gpu_compare_device.argtypes = [vp, vp, sz, vp, i32, i32, i32, vp, vp, vp, vp]
         L.ipuma_gpu_last_stats.argtypes = [vp, ctypes.POINTER(Stats)]
         L.ipuma_gpu_run_buffer_device.argtypes = [vp, vp, sz, vp, sz, vp]
@@ -199,17 +199,23 @@ def encode(datatype: str, s: str) -> np.ndarray:
     return out
 
 
-def pack_codes4(codes: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
-    """Packs codes (each < 16) two per byte, residue 2k in the low nibble
-    of byte k (ipuma_pack_codes4); `out` may be a preallocated (e.g. pinned)
-    uint8 array of (n + 1) // 2 bytes."""
+def pack_codes(codes: np.ndarray, bits: int = 4, out: np.ndarray | None = None) -> np.ndarray:
+    """Packs codes for compare_packed (ipuma_pack_codes): bits = 4 (codes
+    < 16, two per byte, low nibble first) or 2 (A, T, C, G = codes 1..4,
+    four per byte as code - 1).  `out` may be a preallocated (e.g. pinned)
+    uint8 array of ceil(n * bits / 8) bytes."""
     codes = np.ascontiguousarray(codes, dtype=np.uint8)
-    nb = (codes.size + 1) // 2
+    per = 8 // bits
+    nb = (codes.size + per - 1) // per
     if out is None:
         out = np.zeros(nb, dtype=np.uint8)
     assert out.dtype == np.uint8 and out.size >= nb and out.flags.c_contiguous
-    _check(lib().ipuma_pack_codes4(_ptr(codes), codes.size, _ptr(out)))
+    _check(lib().ipuma_pack_codes(_ptr(codes), codes.size, bits, _ptr(out)))
     return out
+
+
+def pack_codes4(codes: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
+    return pack_codes(codes, 4, out)
 
 
 def select_matrix(similarity: str, match=1, mismatch=-1, ambiguity=-1) -> np.ndarray:
@@ -304,19 +310,20 @@ class Engine:
         _check(lib().ipuma_gpu_compare(self.h, _ptr(codes), codes.size, _ptr(pairs),
                                        pairs.shape[0], _ptr(score), _ptr(ar), _ptr(br)))
 
-    def compare_packed(self, packed: np.ndarray, n_codes: int, pairs: np.ndarray):
-        """compare() on 4-bit packed codes (pack_codes4); n_codes residues."""
+    def compare_packed(self, packed: np.ndarray, n_codes: int, pairs: np.ndarray, bits: int = 4):
+        """compare() on packed codes (pack_codes); n_codes residues."""
         packed = np.ascontiguousarray(packed, dtype=np.uint8)
-        assert packed.size >= (n_codes + 1) // 2
+        assert packed.size >= (n_codes * bits + 7) // 8
         pairs = np.ascontiguousarray(pairs, dtype=PAIR_DTYPE)
         n = pairs.shape[0]
         out = [np.zeros(n, dtype=np.int32) for _ in range(3)]
-        self.compare_packed_into(packed, n_codes, pairs, *out)
+        self.compare_packed_into(packed, n_codes, pairs, *out, bits=bits)
         return tuple(out)
 
-    def compare_packed_into(self, packed: np.ndarray, n_codes: int, pairs: np.ndarray, score, ar, br):
+    def compare_packed_into(self, packed: np.ndarray, n_codes: int, pairs: np.ndarray, score, ar, br,
+                            bits: int = 4):
         """compare_packed() into caller buffers (e.g. pinned host arrays)."""
-        _check(lib().ipuma_gpu_compare_packed(self.h, _ptr(packed), n_codes, _ptr(pairs),
+        _check(lib().ipuma_gpu_compare_packed(self.h, _ptr(packed), n_codes, bits, _ptr(pairs),
                                               pairs.shape[0], _ptr(score), _ptr(ar), _ptr(br)))
 
     def compare_device(self, d_codes: int, n_codes: int, d_pairs: int, n: int, max_a: int,

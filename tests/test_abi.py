@@ -91,3 +91,28 @@ def test_pack_codes4_rejects_codes_above_15():
         ib.pack_codes4(codes)
     assert ei.value.code == ib.ERR_BAD_SEQUENCE
     assert "3000001" in str(ei.value)
+
+
+@pytest.mark.parametrize("n", [0, 1, 3, 4, 5, 64, 100_003, (1 << 24) + 7])
+def test_pack_codes2_layout(n):
+    """A, T, C, G (codes 1..4) four per byte as code - 1, residue 4k+q in
+    bits 2q..2q+1 of byte k; missing residues of the last byte are 0."""
+    codes = np.random.default_rng(n).integers(1, 5, n).astype(np.uint8)
+    packed = ib.pack_codes(codes, 2)
+    assert packed.size == (n + 3) // 4
+    v = np.zeros((n + 3) // 4 * 4, np.uint8)
+    v[:n] = codes - 1
+    want = v[0::4] | (v[1::4] << 2) | (v[2::4] << 4) | (v[3::4] << 6)
+    np.testing.assert_array_equal(packed, want)
+
+
+@pytest.mark.parametrize("bad", [0, 5, 15, 16])
+def test_pack_codes2_takes_only_acgt(bad):
+    """N (code 0) and the IUPAC codes 5..15 need the 4-bit path."""
+    codes = np.full(1_000, 2, np.uint8)
+    codes[777] = bad
+    with pytest.raises(ib.IpumaError) as ei:
+        ib.pack_codes(codes, 2)
+    assert ei.value.code == ib.ERR_BAD_SEQUENCE and "777" in str(ei.value)
+    with pytest.raises(ib.IpumaError):
+        ib.pack_codes(codes, 3)
