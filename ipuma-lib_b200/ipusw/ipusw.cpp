@@ -426,6 +426,7 @@ int run(int argc, char** argv) {
   {
     std::vector<ipu::batchaffine::Job*> jobs(nJobs, nullptr);
     std::vector<std::atomic<int>> ready(nJobs);
+    std::atomic<bool> submitFailed{false};  // receivers stop waiting for jobs that never come
     for (auto& r : ready) r.store(0);
     const int receivers = std::max(1, numThreads / 2);
     std::vector<std::string> errors(receivers);
@@ -434,7 +435,10 @@ int run(int argc, char** argv) {
       recv.emplace_back([&, w] {
         try {
           for (size_t i = w; i < nJobs; i += receivers) {
-            while (!ready[i].load(std::memory_order_acquire)) std::this_thread::yield();
+            while (!ready[i].load(std::memory_order_acquire)) {
+              if (submitFailed.load(std::memory_order_acquire)) return;
+              std::this_thread::yield();
+            }
             ipu::batchaffine::Job* job = jobs[i];
             Batch& b = batches[i % batches.size()];
             drivers[i % numDevices]->blocking_join_prepared_remote_compare(*job);
@@ -481,16 +485,24 @@ int run(int argc, char** argv) {
           errors[w] = ex.what();
         }
       });
-    for (size_t i = 0; i < nJobs; ++i) {
-      Batch& b = batches[i % batches.size()];
-      auto& r = results[i];
-      jobs[i] = drivers[i % numDevices]->async_submit_prepared_remote_compare(
-          b.inputBuffer->data(), b.inputBuffer->data() + b.inputBuffer->size(), r.data(), r.data() + r.size());
-      ready[i].store(1, std::memory_order_release);
-      cmpsSubmitted += b.numCmps;
-      batchesSubmitted++;
+    std::string submitError;
+    try {
+      for (size_t i = 0; i < nJobs; ++i) {
+        Batch& b = batches[i % batches.size()];
+        auto& r = results[i];
+        jobs[i] = drivers[i % numDevices]->async_submit_prepared_remote_compare(
+            b.inputBuffer->data(), b.inputBuffer->data() + b.inputBuffer->size(), r.data(), r.data() + r.size());
+        ready[i].store(1, std::memory_order_release);
+        cmpsSubmitted += b.numCmps;
+        batchesSubmitted++;
+      }
+    } catch (const std::exception& ex) {
+      // Jobs already submitted are still joined; the rest are not waited for.
+      submitError = ex.what();
+      submitFailed.store(true, std::memory_order_release);
     }
     for (auto& t : recv) t.join();
+    if (!submitError.empty()) throw std::runtime_error(submitError);
     for (const auto& e : errors)
       if (!e.empty()) throw std::runtime_error(e);
   }
