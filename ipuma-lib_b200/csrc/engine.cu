@@ -315,10 +315,12 @@ int smem_for(const ipuma_engine* e) {
   return SmemLayout<T, K, LANES>::total(e->M, kWarpsPerBlock);
 }
 
-// Grid of a k_batched<T, K, LANES, HYB> launch.
+// Grid of a k_batched<T, K, LANES, HYB> launch (the instantiation for the
+// engine's forwardOnly, which is fixed at creation).
 template <class T, int K, int LANES, bool HYB = false>
 int batched_grid(ipuma_engine* e) {
-  return occupancy_grid(e, k_batched<T, K, LANES, HYB>, smem_for<T, K, LANES>(e));
+  return e->sc.forwardOnly ? occupancy_grid(e, k_batched<T, K, LANES, HYB, true>, smem_for<T, K, LANES>(e))
+                           : occupancy_grid(e, k_batched<T, K, LANES, HYB, false>, smem_for<T, K, LANES>(e));
 }
 
 template <int K>
@@ -403,7 +405,8 @@ int launch_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uin
   auto* cells = reinterpret_cast<unsigned long long*>(ctl + CTL_CELLS);
   int rc;
   if ((rc = timed_begin(e, s, kind, cls))) return rc;
-  k_batched<T, K, LANES, HYB><<<grid, kThreads, smem, s>>>(
+  auto* kern = e->sc.forwardOnly ? k_batched<T, K, LANES, HYB, true> : k_batched<T, K, LANES, HYB, false>;
+  kern<<<grid, kThreads, smem, s>>>(
       e->sc, e->d_sim.as<int8_t>(), codes, pairs, list, range, head, rb.scratch->as<int2>(),
       rowsCap, score, arange, brange, rb.ovf->as<int>(), cells + CELLS_RERUN,
       reinterpret_cast<DevStatus*>(ctl + CTL_STATUS),

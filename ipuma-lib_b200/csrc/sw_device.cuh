@@ -79,6 +79,17 @@ struct PassCtl {
   int stoppedAt = -1;      // out (s16x2 pass): strip it stopped before, -1: none
 };
 
+// Early stop of a reverse pass (sw_pass with EARLY): the reverse maximum of
+// a pair equals its forward score, so a strip may end once every pair's
+// group has reached its target and all lanes have passed that row, and a
+// later strip (larger columns) can only win with a smaller row, so it runs
+// only the rows above the best row found so far.  Exact under the
+// first-strict-maximum tie-break.
+struct PassStop {
+  bool on = false;
+  int target[2] = {0, 0};  // per pair; 0 for a pair without a reverse pass
+};
+
 // -------------------------------------------------------------------------
 // Lane types
 // -------------------------------------------------------------------------
@@ -285,10 +296,11 @@ __device__ __forceinline__ uint32_t keep_mask(LaneS32, int rm, int b) {
 // it; an s32 pass with ctl->strip0 > 0 starts there from the packed
 // boundary half ctl->bndHalf in buffer ctl->scrBase, keeping `out` (the
 // best of the strips before) and using the two other buffers.
-template <class T, int K, int LANES, bool HYB = false>
+template <class T, int K, int LANES, bool HYB = false, bool EARLY = false>
 __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, const int8_t* s_simp,
                                         uint16_t* s_bring, const PassSeq (&ps)[T::NP], int2* scr,
-                                        long rowsCap, Best (&out)[T::NP], PassCtl* ctl = nullptr) {
+                                        long rowsCap, Best (&out)[T::NP], PassCtl* ctl = nullptr,
+                                        PassStop stop = PassStop{}) {
   using V = typename T::V;
   constexpr int SW = LANES * K;          // columns per strip
   constexpr int KP = ProfileWords<K>::KP;
@@ -310,9 +322,15 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
       out[h].j = 0;
     }
   }
-  const int rowsW = __reduce_max_sync(FULL, rowsG);
-  const int rowsMin = __reduce_min_sync(FULL, rowsG);
+  int rowsW = __reduce_max_sync(FULL, rowsG);
+  int rowsMin = __reduce_min_sync(FULL, rowsG);
   const int nstrips = (__reduce_max_sync(FULL, amax) + SW - 1) / SW;
+  // EARLY: rows each pair still needs (its best row once it reached its
+  // target), and this lane's group in the warp.
+  int capRows[NP];
+#pragma unroll
+  for (int h = 0; h < NP; ++h) capRows[h] = ps[h].blen;
+  const unsigned gmask = (LANES == 32) ? FULL : (0xFFFFu << (threadIdx.x & 16));
   const V vgE = T::splat(sc.gE);
   const V vgEp = T::splat(max(sc.gE, sc.gIgE));
   const V vgIgE = T::splat(sc.gIgE);
@@ -340,6 +358,16 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
   V bmax = vZero;
 
   for (int strip = strip0; strip < nstrips; ++strip) {
+    if constexpr (EARLY) {
+      if (stop.on && strip > strip0) {
+        rowsG = 0;
+#pragma unroll
+        for (int h = 0; h < NP; ++h) rowsG = max(rowsG, min(ps[h].blen, capRows[h]));
+        rowsW = __reduce_max_sync(FULL, rowsG);
+        rowsMin = __reduce_min_sync(FULL, rowsG);
+        if (rowsW == 0) break;  // caps only shrink: no later strip can win
+      }
+    }
     const int col0 = strip * SW;
     const bool hasIn = strip > 0;
     const bool hasOut = strip + 1 < nstrips;
@@ -491,7 +519,23 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
 
     const int nsteps = rowsW + LANES - 1;
     bool gaveUp = false;
+    int stopAt = nsteps;  // EARLY: end of the block after every pair is done
     for (int t0 = 0; t0 < nsteps; t0 += LANES) {
+      if constexpr (EARLY) {
+        if (t0 >= stopAt) break;
+        if (stop.on && stopAt == nsteps) {
+          // A pair is done once its group reached the target (before t0, so
+          // the slowest lane passes that row within this block) or all
+          // lanes are past its rows.  Warp-uniform.
+          bool done = true;
+#pragma unroll
+          for (int h = 0; h < NP; ++h) {
+            const bool found = (__ballot_sync(FULL, T::half(best, h) >= stop.target[h]) & gmask) != 0;
+            done = done && (found || t0 - (LANES - 1) >= min(ps[h].blen, capRows[h]));
+          }
+          if (__all_sync(FULL, done)) stopAt = t0 + LANES;
+        }
+      }
       if constexpr (NP == 2) {
         if ((t0 & 31) == 0) {
           // A cell above s16Limit could overflow the next additions.
@@ -544,6 +588,9 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
         out[h].s = s;
         out[h].i = ii;
         out[h].j = j;
+      }
+      if constexpr (EARLY) {
+        if (stop.on && out[h].s >= stop.target[h]) capRows[h] = min(capRows[h], out[h].i);
       }
     }
     if (hasOut) {

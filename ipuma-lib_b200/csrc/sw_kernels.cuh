@@ -82,7 +82,10 @@ __device__ __forceinline__ void load_simp(int8_t* s_simp, const int8_t* sim, con
 // by one lane group.  For s16x2 lanes a pair whose score exceeds
 // sc.s16Limit (or any pair of a warp that gave up) is flagged in `ovf` and
 // gets no reverse pass (the s32 rerun redoes it).
-template <class T, int K, int LANES>
+// MODE: 0 = by sc.forwardOnly at run time, 1 = forward only, 2 = with the
+// reverse pass (a kernel specialised for one mode holds only its code, so
+// the forward-only kernels keep their own register allocation).
+template <class T, int K, int LANES, int MODE = 0>
 __device__ __forceinline__ void align_pairs(const SwConst& sc, uint8_t* s_prof,
                                             const int8_t* s_simp, uint16_t* s_bring,
                                             const uint8_t* const (&a0)[T::NP],
@@ -99,19 +102,27 @@ __device__ __forceinline__ void align_pairs(const SwConst& sc, uint8_t* s_prof,
   }
 #pragma unroll
   for (int h = 0; h < NP; ++h) rv[h] = Best{0, 0, 0};
-  if (sc.forwardOnly) {
-    const bool done = sw_pass<T, K, LANES>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, fw);
+  if (MODE == 1 || (MODE == 0 && sc.forwardOnly)) {
+    if constexpr (MODE != 2) {
+      const bool done = sw_pass<T, K, LANES>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, fw);
 #pragma unroll
-    for (int h = 0; h < NP; ++h) ovf[h] = (NP == 2) && (!done || fw[h].s > sc.s16Limit);
+      for (int h = 0; h < NP; ++h) ovf[h] = (NP == 2) && (!done || fw[h].s > sc.s16Limit);
+    }
     return;
   }
+  if constexpr (MODE != 1) {
   // With start coordinates both passes run through one copy of sw_pass: two
   // inlined copies alternating in the instruction cache slowed both down.
-  // (A forward-only launch runs only the copy above.)
+  // (A forward-only launch runs only the copy above.)  The reverse pass
+  // stops early once every pair reached its forward score (PassStop).
+  // Only the kernels specialised for full alignments (MODE 2) take the
+  // early stop: it costs registers that the others keep.
+  PassStop stop;
 #pragma unroll 1
   for (int pass = 0; pass < 2; ++pass) {
     Best res[NP];
-    const bool done = sw_pass<T, K, LANES>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, res);
+    const bool done = sw_pass<T, K, LANES, false, MODE == 2>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, res,
+                                                              nullptr, stop);
     if (pass == 1) {
 #pragma unroll
       for (int h = 0; h < NP; ++h) rv[h] = res[h];
@@ -126,9 +137,12 @@ __device__ __forceinline__ void align_pairs(const SwConst& sc, uint8_t* s_prof,
       any |= run;
       ps[h] = run ? PassSeq{a0[h] + fw[h].j, b0[h] + fw[h].i, fw[h].j + 1, fw[h].i + 1, -1, -1}
                   : PassSeq{a0[h], b0[h], 0, 0, 1, 1};
+      stop.target[h] = run ? fw[h].s : 0;
     }
+    stop.on = true;
     // Uniform across the warp: every group takes part in the shuffles.
     if (!__any_sync(FULL, any)) break;
+  }
   }
 }
 
@@ -158,8 +172,8 @@ __device__ __forceinline__ bool hybrid_pass(const SwConst& sc, uint8_t* s_prof, 
   return true;
 }
 
-// Forward (+ reverse) pass of the hybrid class; as align_pairs.
-template <int K>
+// Forward (+ reverse) pass of the hybrid class; as align_pairs (MODE too).
+template <int K, int MODE = 0>
 __device__ __forceinline__ void align_pairs_hybrid(const SwConst& sc, uint8_t* s_prof, const int8_t* s_simp,
                                                    uint16_t* s_bring, const uint8_t* const (&a0)[2],
                                                    const uint8_t* const (&b0)[2], const int (&alen)[2],
@@ -173,11 +187,14 @@ __device__ __forceinline__ void align_pairs_hybrid(const SwConst& sc, uint8_t* s
   }
 #pragma unroll
   for (int h = 0; h < 2; ++h) rv[h] = Best{0, 0, 0};
-  if (sc.forwardOnly) {
-    const bool done = hybrid_pass<K>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, fw);
-    ovf[0] = ovf[1] = !done;
+  if (MODE == 1 || (MODE == 0 && sc.forwardOnly)) {
+    if constexpr (MODE != 2) {
+      const bool done = hybrid_pass<K>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, fw);
+      ovf[0] = ovf[1] = !done;
+    }
     return;
   }
+  if constexpr (MODE != 1) {
   // With start coordinates one copy of the hybrid pass serves both
   // directions (as align_pairs).
 #pragma unroll 1
@@ -202,6 +219,7 @@ __device__ __forceinline__ void align_pairs_hybrid(const SwConst& sc, uint8_t* s
     }
     if (!done) break;
   }
+  }
 }
 
 __device__ __forceinline__ void write_result(const SwConst& sc, const Best& fw, const Best& rv,
@@ -217,7 +235,7 @@ __device__ __forceinline__ void write_result(const SwConst& sc, const Best& fw, 
 // Persistent batched kernel.  `list` holds pair ids in processing order;
 // a warp takes items of 32 / LANES * NP consecutive entries (ids < 0 are
 // padding), lane group g aligning entries [g * NP, g * NP + NP).
-template <class T, int K, int LANES, bool HYB = false>
+template <class T, int K, int LANES, bool HYB = false, bool FWD = false>
 __global__ void __launch_bounds__(128) k_batched(SwConst sc, const int8_t* __restrict__ sim,
                                                  const uint8_t* __restrict__ codes,
                                                  const PairDesc* __restrict__ pairs,
@@ -283,9 +301,15 @@ __global__ void __launch_bounds__(128) k_batched(SwConst sc, const int8_t* __res
     bool ovf[NP];
     if constexpr (HYB) {
       static_assert(NP == 2 && LANES == 32, "the hybrid class pairs two s16x2 pairs per 32-lane warp");
-      align_pairs_hybrid<K>(sc, s_prof, s_simp, s_bring, a0, b0, alen, blen, scr, rowsCap, fw, rv, ovf);
+      // Mode chosen at run time: specialising the hybrid class made its
+      // forward-only kernel spill and slowed the heavy-tailed protein batch.
+      align_pairs_hybrid<K, 0>(sc, s_prof, s_simp, s_bring, a0, b0, alen, blen, scr, rowsCap, fw, rv, ovf);
     } else {
-      align_pairs<T, K, LANES>(sc, s_prof, s_simp, s_bring, a0, b0, alen, blen, scr, rowsCap, fw, rv, ovf);
+      // s16x2 classes: one kernel per mode (fewer registers, no spills for
+      // forward-only; the early reverse stop for full alignments); the s32
+      // class keeps the run-time choice for the same reason as the hybrid.
+      constexpr int MODE = (T::NP == 1) ? 0 : (FWD ? 1 : 2);
+      align_pairs<T, K, LANES, MODE>(sc, s_prof, s_simp, s_bring, a0, b0, alen, blen, scr, rowsCap, fw, rv, ovf);
     }
     if (glane == 0) {
 #pragma unroll
