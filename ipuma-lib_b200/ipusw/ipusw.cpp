@@ -142,6 +142,18 @@ struct IpuSwConfig {
   int repeat = 1;
 };
 
+int as_int(const std::string& v) {
+  size_t used = 0;
+  int x = 0;
+  try {
+    x = std::stoi(v, &used);
+  } catch (const std::exception&) {
+    used = 0;
+  }
+  if (used == 0 || used != v.size()) throw std::runtime_error("not an integer: " + v);
+  return x;
+}
+
 bool as_bool(const std::string& v) {
   if (v == "true" || v == "1") return true;
   if (v == "false" || v == "0") return false;
@@ -150,28 +162,28 @@ bool as_bool(const std::string& v) {
 
 // Sets one leaf key; false if the key is unknown.
 bool set_key(IpuSwConfig& c, const std::string& k, const std::string& v) {
-  if (k == "gapInit") c.sw.gapInit = std::stoi(v);
-  else if (k == "gapExtend") c.sw.gapExtend = std::stoi(v);
-  else if (k == "matchValue") c.sw.matchValue = std::stoi(v);
-  else if (k == "mismatchValue") c.sw.mismatchValue = std::stoi(v);
-  else if (k == "ambiguityValue") c.sw.ambiguityValue = std::stoi(v);
+  if (k == "gapInit") c.sw.gapInit = as_int(v);
+  else if (k == "gapExtend") c.sw.gapExtend = as_int(v);
+  else if (k == "matchValue") c.sw.matchValue = as_int(v);
+  else if (k == "mismatchValue") c.sw.mismatchValue = as_int(v);
+  else if (k == "ambiguityValue") c.sw.ambiguityValue = as_int(v);
   else if (k == "similarity") c.sw.similarity = swatlib::strToSimilarity(v);
   else if (k == "datatype") c.sw.datatype = swatlib::strToDataType(v);
-  else if (k == "tilesUsed") c.ipu.tilesUsed = std::stoi(v);
-  else if (k == "maxAB") c.ipu.maxAB = std::stoi(v);
-  else if (k == "maxBatches") c.ipu.maxBatches = std::stoi(v);
-  else if (k == "bufsize") c.ipu.bufsize = std::stoi(v);
+  else if (k == "tilesUsed") c.ipu.tilesUsed = as_int(v);
+  else if (k == "maxAB") c.ipu.maxAB = as_int(v);
+  else if (k == "maxBatches") c.ipu.maxBatches = as_int(v);
+  else if (k == "bufsize") c.ipu.bufsize = as_int(v);
   else if (k == "vtype") c.ipu.vtype = ipu::strToVertexType(v);
   else if (k == "fillAlgo") c.ipu.fillAlgo = ipu::strToAlgorithm(v);
   else if (k == "forwardOnly") c.ipu.forwardOnly = as_bool(v);
   else if (k == "useRemoteBuffer") c.ipu.useRemoteBuffer = as_bool(v);
-  else if (k == "transmissionPrograms") c.ipu.transmissionPrograms = std::stoi(v);
-  else if (k == "ioTiles") c.ipu.ioTiles = std::stoi(v);
-  else if (k == "numDevices") c.numDevices = std::stoi(v);
-  else if (k == "numThreads") c.numThreads = std::stoi(v);
+  else if (k == "transmissionPrograms") c.ipu.transmissionPrograms = as_int(v);
+  else if (k == "ioTiles") c.ipu.ioTiles = as_int(v);
+  else if (k == "numDevices") c.numDevices = as_int(v);
+  else if (k == "numThreads") c.numThreads = as_int(v);
   else if (k == "duplicateDatasets") c.duplicateDatasets = as_bool(v);
-  else if (k == "duplicationFactor") c.duplicationFactor = std::stoi(v);
-  else if (k == "repeat") c.repeat = std::stoi(v);
+  else if (k == "duplicationFactor") c.duplicationFactor = as_int(v);
+  else if (k == "repeat") c.repeat = as_int(v);
   else return false;
   return true;
 }

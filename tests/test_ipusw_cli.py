@@ -177,6 +177,8 @@ def test_defaults_without_a_config_file(exe, tmp_path):
     (["--bogus", "1"], "unknown option --bogus"),
     (["--forwardOnly", "maybe"], "not a boolean"),
     (["--similarity", "pam250"], "similarity"),
+    (["--maxAB", "300x"], "not an integer"),
+    (["--numThreads", ""], "not an integer"),
 ])
 def test_bad_options_are_reported(exe, tmp_path, args, message):
     _write_txt(tmp_path / "a.txt", ["ACGT"])
