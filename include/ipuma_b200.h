@@ -131,6 +131,15 @@ typedef struct ipuma_stats {
   /* ipuma_gpu_compare: chunks the batch was split into for upload/compute
    * overlap (1 = one upload, then the kernels). */
   int32_t chunks;
+  /* With option "trace" = 1: for each class launch of the batched pipeline
+   * that ran (concurrently, as in production), the device time of its
+   * first block's start and of its last warp's end, in ms from the call's
+   * first start, and its forward-pass cells. */
+  int32_t n_trace;
+  int32_t trace_kind[IPUMA_MAX_TIMED];   /* IPUMA_KERNEL_* */
+  double trace_start_ms[IPUMA_MAX_TIMED];
+  double trace_end_ms[IPUMA_MAX_TIMED];
+  int64_t trace_cells[IPUMA_MAX_TIMED];
 } ipuma_stats;
 
 /* Kernel kinds reported in ipuma_stats.timed_kind.  S16_L<lanes>_K<k>:
@@ -157,6 +166,7 @@ typedef struct ipuma_stats {
 #define IPUMA_KERNEL_S16_L16_K13 18
 #define IPUMA_KERNEL_S16_L16_K15 19
 #define IPUMA_KERNEL_S16_HYBRID 20 /* s16x2 strips while safe, then s32 (high scores) */
+#define IPUMA_KERNEL_PLAIN_S16 21  /* one-launch-per-batch wire kernel, s16x2 lanes */
 
 typedef struct ipuma_engine ipuma_engine;
 
@@ -190,9 +200,13 @@ int ipuma_gpu_create(const ipuma_sw_config* sw, const ipuma_algo_config* algo, i
                      ipuma_engine** out);
 void ipuma_gpu_destroy(ipuma_engine* e);
 
-/* Engine options (names and values documented in INTEGRATION.md):
+/* Engine options:
  *   "scheduler"   0 = persistent cost-binned engine (default), 1 = plain
  *                 one-launch-per-batch kernel (wire-buffer API only)
+ *   "plain_lanes" lanes of the plain kernel: 32 = one comparison slot per
+ *                 warp in s32 lanes (default), 16 = two consecutive slots
+ *                 per warp in s16x2 halves, a slot that could leave int16
+ *                 redone in s32 by the same warp (IPUMA_KERNEL_PLAIN_S16)
  *   "graphs"      1 = capture and replay CUDA graphs for repeated shapes
  *   "tile_k"      0 = kernel class by |A| (default); 1..6 = every pair
  *                 through s16x2 class IPUMA_KERNEL_S16_* (value = kind),
@@ -215,6 +229,9 @@ void ipuma_gpu_destroy(ipuma_engine* e);
  *                 chosen for pairs that are small relative to the batch,
  *                 0 = never (default) unless tile_k forces it
  *   "time_launches" 1 = time every alignment-kernel launch (ipuma_stats)
+ *   "trace"       1 = record when each class launch of the pipeline starts
+ *                 and ends on the device, launches running concurrently
+ *                 as usual (ipuma_stats trace_*)
  *   "autotune"    1 = measure the kernel-class rates before the first batch
  *                 (default), 0 = built-in rates unless ipuma_gpu_autotune
  *   "long_a"      |A| above which a pair takes the widest s16x2 class
@@ -274,7 +291,10 @@ int ipuma_gpu_compare_packed(ipuma_engine* e, const uint8_t* packed, size_t n_co
                              int32_t* brange);
 /* Same with every buffer in device memory, enqueued on `stream`
  * (cudaStream_t, NULL = the engine's stream); max_a_len / max_b_len bound
- * the pair lengths (checked on the device). */
+ * the pair lengths.  Every descriptor is checked on the device before any
+ * code is read: a length past those bounds gives IPUMA_ERR_TOO_LONG, a
+ * negative field or a sequence reaching past the n_codes residues of
+ * d_codes IPUMA_ERR_INVALID_ARG; those pairs get a zero result. */
 int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_codes,
                              const ipuma_pair* d_pairs, int32_t n, int32_t max_a_len,
                              int32_t max_b_len, int32_t* d_score, int32_t* d_arange,
@@ -305,21 +325,25 @@ int ipuma_gpu_autotune(ipuma_engine* e, const char* cache_path);
 /* Writes the rates in use as JSON text into buf. */
 int ipuma_gpu_tuning(ipuma_engine* e, char* buf, size_t cap);
 
-/* Allocation-free alignment, for callers that cannot call cudaMalloc (for
- * example code running while its stream is captured into a CUDA graph,
- * hosts that own all device memory through their own pool, or paths that
- * cannot afford the synchronisation cudaMalloc/cudaFree imply).  No
- * counterpart in the reference.  Aligns n pairs on the current device with
- * exact 32-bit lanes; codes, pairs and the three result arrays are device
- * memory owned by the caller; results as ipuma_gpu_compare.  Nothing is
- * allocated: the kernel's strip-boundary scratch is a 16 MiB file-scope
- * device array that every GPU loading the library holds until exit.
- * Limits: max_b_len (an upper bound of every b_len, checked on the device)
- * at most 65535; gap_init + gap_extend < 0 and gap_extend <= 0.  The first
- * call on a device looks up the array's device address, so make it before
- * any stream capture.  All calls share the array: calls that overlap on the
- * GPU race and must be serialised by the caller.  Blocks until the batch is
- * done; errors through ipuma_last_error(). */
+/* Allocation-free alignment, for callers that cannot call cudaMalloc: host
+ * programs whose own memory pool owns all device memory (for example a
+ * framework's caching allocator that reserved the GPU) and paths that
+ * cannot afford the device-wide synchronisation cudaMalloc/cudaFree imply.
+ * No counterpart in the reference.  Aligns n pairs on the current device
+ * with exact 32-bit lanes; codes (n_codes residues), pairs and the three
+ * result arrays are device memory owned by the caller; results as
+ * ipuma_gpu_compare.  Nothing is allocated: the kernel's strip-boundary
+ * scratch is a 16 MiB file-scope device array that every GPU loading the
+ * library holds until exit.  Limits: max_b_len (an upper bound of every
+ * b_len, checked on the device) at most 65535, every a_len at most 65535;
+ * gap_init + gap_extend < 0 and gap_extend <= 0.  Pairs are checked on the
+ * device before any code is read: a length beyond those limits gives
+ * IPUMA_ERR_TOO_LONG, a negative field or a sequence past n_codes
+ * IPUMA_ERR_INVALID_ARG (those pairs get a zero result).  The first call on
+ * a device looks up the array's device address, so make it before any
+ * stream capture.  All calls share the array: calls that overlap on the
+ * GPU race and must be serialised by the caller.  Blocks until the batch
+ * is done; errors through ipuma_last_error(). */
 int ipuma_gpu_compare_noalloc(const ipuma_sw_config* sw, int32_t forward_only, const uint8_t* d_codes,
                               size_t n_codes, const ipuma_pair* d_pairs, int32_t n, int32_t max_b_len,
                               int32_t* d_score, int32_t* d_arange, int32_t* d_brange, void* stream);

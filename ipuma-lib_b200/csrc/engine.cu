@@ -197,6 +197,8 @@ struct ipuma_engine {
 
   // options
   int scheduler = 0;
+  int plain_s16 = 0;  // option "plain_lanes" = 16: the plain kernel in s16x2 lanes (k_plain16)
+  int trace = 0;      // option "trace": first start / last end of every class launch
   int graphs = 0;
   int tile_k = 0;
   int time_launches = 0;
@@ -271,7 +273,9 @@ constexpr int NCELLS = NCLASS_MAX + 3;              // per class, rerun, wire ch
 constexpr int CTL_COST = CTL_CELLS + 2 * NCELLS;    // modelled cost per class (uint64, ps)
 constexpr int CTL_ALLOT = CTL_COST + 2 * NCLASS_MAX;  // ClassAllot per class + rerun (4 ints each)
 static_assert(CTL_COST % 2 == 0 && CTL_ALLOT % 2 == 0, "8-byte aligned control block fields");
-constexpr int CTL_HIST = CTL_ALLOT + 4 * (NCLASS_MAX + 1);  // NCLASS_MAX * NBUCKET
+constexpr int CTL_TRACE = CTL_ALLOT + 4 * (NCLASS_MAX + 1);  // {~start, end} ns per class + rerun (uint64)
+static_assert(CTL_TRACE % 2 == 0, "8-byte aligned trace");
+constexpr int CTL_HIST = CTL_TRACE + 4 * (NCLASS_MAX + 1);  // NCLASS_MAX * NBUCKET
 constexpr int CTL_OFFS = CTL_HIST + NCLASS_MAX * NBUCKET;
 constexpr int CTL_INTS = CTL_OFFS + NCLASS_MAX * NBUCKET;
 constexpr int CELLS_RERUN = NCLASS_MAX;             // index of the rerun cells
@@ -410,7 +414,8 @@ int launch_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uin
       e->sc, e->d_sim.as<int8_t>(), codes, pairs, list, range, head, rb.scratch->as<int2>(),
       rowsCap, score, arange, brange, rb.ovf->as<int>(), cells + CELLS_RERUN,
       reinterpret_cast<DevStatus*>(ctl + CTL_STATUS),
-      reinterpret_cast<const ClassAllot*>(ctl + CTL_ALLOT) + allot_idx);
+      reinterpret_cast<const ClassAllot*>(ctl + CTL_ALLOT) + allot_idx,
+      e->trace ? reinterpret_cast<unsigned long long*>(ctl + CTL_TRACE) + 2 * allot_idx : nullptr);
   CUDA_TRY(cudaGetLastError());
   return timed_end(e, s);
 }
@@ -517,7 +522,9 @@ int reserve_batched(ipuma_engine* e, cudaStream_t s, int n, int maxA, int maxB) 
 
 // Runs the persistent cost-binned pipeline over n device-resident pairs.
 // Results land at score[p], arange[p], brange[p].
-int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_t* codes,
+// n_codes = residues the code array holds: pairs reaching past it are
+// rejected on the device (status ERR_RANGE) before any code is read.
+int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_t* codes, size_t n_codes,
                 const PairDesc* pairs, int n, int maxA, int maxB, int* score, int* arange, int* brange,
                 int* launches) {
   int rc;
@@ -532,9 +539,9 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
     threads = ((threads + 127) / 128) * 128;
     if ((rc = e->d_cf.ensure(sizeof(int) * 2 * maxAcap * threads, s))) return rc;
     if ((rc = timed_begin(e, s, IPUMA_KERNEL_EXACT, -1))) return rc;
-    k_exact<<<(int)(threads / 128), 128, 0, s>>>(e->sc, e->d_sim.as<int8_t>(), codes, pairs, n,
-                                                  nullptr, 0, 0, 1, e->d_cf.as<int>(), maxAcap,
-                                                  score, arange, brange);
+    k_exact<<<(int)(threads / 128), 128, 0, s>>>(e->sc, e->d_sim.as<int8_t>(), codes, (long long)n_codes, pairs,
+                                                  n, nullptr, 0, 0, 1, e->d_cf.as<int>(), maxAcap, maxB,
+                                                  score, arange, brange, st);
     CUDA_TRY(cudaGetLastError());
     if ((rc = timed_end(e, s))) return rc;
     *launches += 1;
@@ -608,6 +615,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   bp.forced_class = e->tile_k > 0 ? e->tile_k - 1 : -1;
   bp.max_a = maxA;
   bp.max_b = maxB;
+  bp.n_codes = (long long)n_codes;
   bp.M = e->M;
   bp.s16_limit = e->sc.s16Limit;
   if ((rc = rb.flag->ensure((size_t)n + 64, s))) return rc;
@@ -717,6 +725,14 @@ int reset_ctl(ipuma_engine* e, cudaStream_t s) {
   return IPUMA_OK;
 }
 
+// Forward-pass cells counted for class c (or the rerun) over `nblk` runs.
+template <size_t N>
+unsigned long long cells_of(const unsigned long long (*cells)[N], int nblk, int c) {
+  unsigned long long v = 0;
+  for (int k = 0; k < nblk; ++k) v += cells[k][c];
+  return v;
+}
+
 // Waits for the stream and reads the status of the call's runs: `nblk`
 // consecutive control blocks at the start of d_ctl (one per run; errors,
 // overflow reruns and per-class cells are summed).
@@ -725,13 +741,41 @@ int check_status(ipuma_engine* e, cudaStream_t s, int nblk = 1) {
   unsigned long long cells[NCELLS] = {};
   DevStatus stk[kMaxChunks];
   unsigned long long cellsk[kMaxChunks][NCELLS];
+  unsigned long long tracek[kMaxChunks][2 * (NCLASS_MAX + 1)];
   nblk = std::max(1, std::min(nblk, kMaxChunks));
   for (int k = 0; k < nblk; ++k) {
     const int* ctl = e->d_ctl.as<int>() + (size_t)k * CTL_INTS;
     CUDA_TRY(cudaMemcpyAsync(&stk[k], ctl + CTL_STATUS, sizeof(DevStatus), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaMemcpyAsync(cellsk[k], ctl + CTL_CELLS, sizeof(cellsk[k]), cudaMemcpyDeviceToHost, s));
+    if (e->trace)
+      CUDA_TRY(cudaMemcpyAsync(tracek[k], ctl + CTL_TRACE, sizeof(tracek[k]), cudaMemcpyDeviceToHost, s));
   }
   CUDA_TRY(cudaStreamSynchronize(s));
+  e->stats.n_trace = 0;
+  if (e->trace) {
+    // Per class (and the rerun): earliest block start and latest warp end
+    // over the call's runs, in ms from the call's earliest start.
+    unsigned long long t0 = ~0ull;
+    unsigned long long st0[NCLASS_MAX + 1], en[NCLASS_MAX + 1];
+    for (int c = 0; c <= NCLASS_MAX; ++c) {
+      st0[c] = ~0ull;
+      en[c] = 0;
+      for (int k = 0; k < nblk; ++k) {
+        if (!tracek[k][2 * c + 1]) continue;
+        st0[c] = std::min(st0[c], ~tracek[k][2 * c]);
+        en[c] = std::max(en[c], tracek[k][2 * c + 1]);
+      }
+      if (en[c]) t0 = std::min(t0, st0[c]);
+    }
+    for (int c = 0; c <= NCLASS_MAX && e->stats.n_trace < IPUMA_MAX_TIMED; ++c) {
+      if (!en[c]) continue;
+      const int i = e->stats.n_trace++;
+      e->stats.trace_kind[i] = c < kNumClasses ? kClasses[c].kind : IPUMA_KERNEL_S32_RERUN;
+      e->stats.trace_start_ms[i] = (double)(st0[c] - t0) * 1e-6;
+      e->stats.trace_end_ms[i] = (double)(en[c] - t0) * 1e-6;
+      e->stats.trace_cells[i] = (int64_t)cells_of(cellsk, nblk, c < kNumClasses ? c : CELLS_RERUN);
+    }
+  }
   for (int k = 0; k < nblk; ++k) {
     if (!st.error) st.error = stk[k].error;
     st.overflow_count += stk[k].overflow_count;
@@ -749,6 +793,8 @@ int check_status(ipuma_engine* e, cudaStream_t s, int nblk = 1) {
   }
   e->n_timed = 0;
   if (st.error == ERR_LENGTH) return fail(IPUMA_ERR_TOO_LONG, "a pair exceeds the stated maximum length");
+  if (st.error == ERR_RANGE)
+    return fail(IPUMA_ERR_INVALID_ARG, "a pair lies outside the code array (negative or past n_codes)");
   if (st.error) return fail(IPUMA_ERR_DEVICE, "kernel status error %d", st.error);
   return IPUMA_OK;
 }
@@ -768,21 +814,28 @@ int run_plain_wire(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const int
   DevStatus* st = reinterpret_cast<DevStatus*>(ctl + CTL_STATUS);
   const long rowsCap = std::max(1, maxB);
   const int K = plain_k_for(e->algo.max_ab);
+  const bool s16 = e->plain_s16 && e->s16_ok;
   auto go = [&](auto kern, int smem) -> int {
     const int grid = occupancy_grid(e, kern, smem);
     const long warps = (long)grid * kWarpsPerBlock;
     int r;
     if ((r = rb.scratch->ensure(sizeof(int2) * 2 * rowsCap * warps, s))) return r;
-    if ((r = timed_begin(e, s, IPUMA_KERNEL_PLAIN, CELLS_WIRE))) return r;
+    if ((r = timed_begin(e, s, s16 ? IPUMA_KERNEL_PLAIN_S16 : IPUMA_KERNEL_PLAIN, CELLS_WIRE))) return r;
     kern<<<grid, kThreads, smem, s>>>(e->sc, e->d_sim.as<int8_t>(), d_inputs, seqWordsPerTile,
                                       metaOffset, maxBatches, totalSlots, rb.scratch->as<int2>(),
                                       rowsCap, d_results, st);
     CUDA_TRY(cudaGetLastError());
     return timed_end(e, s);
   };
-  if (K == 4) rc = go(k_plain<4>, smem_for<LaneS32, 4, 32>(e));
-  else if (K == 8) rc = go(k_plain<8>, smem_for<LaneS32, 8, 32>(e));
-  else rc = go(k_plain<16>, smem_for<LaneS32, 16, 32>(e));
+  if (s16) {
+    if (K == 4) rc = go(k_plain16<4>, smem_for<LaneS16x2, 4, 32>(e));
+    else if (K == 8) rc = go(k_plain16<8>, smem_for<LaneS16x2, 8, 32>(e));
+    else rc = go(k_plain16<16>, smem_for<LaneS16x2, 16, 32>(e));
+  } else {
+    if (K == 4) rc = go(k_plain<4>, smem_for<LaneS32, 4, 32>(e));
+    else if (K == 8) rc = go(k_plain<8>, smem_for<LaneS32, 8, 32>(e));
+    else rc = go(k_plain<16>, smem_for<LaneS32, 16, 32>(e));
+  }
   *launches += 1;
   return rc;
 }
@@ -919,7 +972,8 @@ int time_class(ipuma_engine* e, int cls, int n, int alen, int blen, const DevBuf
   for (int rep = 0; rep < 2 && rc == IPUMA_OK; ++rep) {
     int launches = 0;
     if ((rc = reset_ctl(e, s))) break;
-    if ((rc = run_batched(e, main_bufs(e), s, e->d_codes.as<uint8_t>(), e->d_pairs.as<PairDesc>(), n, alen, blen, out, out + n,
+    if ((rc = run_batched(e, main_bufs(e), s, e->d_codes.as<uint8_t>(), bytes, e->d_pairs.as<PairDesc>(), n, alen, blen,
+                          out, out + n,
                           out + 2 * n, &launches)))
       break;
     if ((rc = check_status(e, s))) break;
@@ -1457,6 +1511,11 @@ int ipuma_gpu_set_option(ipuma_engine* e, const char* name, int64_t value) {
   if (k == "scheduler") {
     if (value != 0 && value != 1) return fail(IPUMA_ERR_INVALID_ARG, "scheduler must be 0 or 1");
     e->scheduler = (int)value;
+  } else if (k == "plain_lanes") {
+    if (value != 16 && value != 32) return fail(IPUMA_ERR_INVALID_ARG, "plain_lanes must be 16 or 32");
+    e->plain_s16 = value == 16 ? 1 : 0;
+  } else if (k == "trace") {
+    e->trace = value ? 1 : 0;
   } else if (k == "graphs") {
     e->graphs = value ? 1 : 0;
   } else if (k == "long_a") {
@@ -1539,7 +1598,6 @@ int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_c
   if (n < 0) return fail(IPUMA_ERR_INVALID_ARG, "negative pair count");
   if (n > 0 && (!d_codes || !d_pairs || !d_score || !d_arange || !d_brange))
     return fail(IPUMA_ERR_INVALID_ARG, "null buffer");
-  (void)n_codes;
   std::lock_guard<std::mutex> lk(e->mu);
   CUDA_TRY(cudaSetDevice(e->device));
   cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : e->stream;
@@ -1550,14 +1608,15 @@ int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_c
   if (e->graphs && !e->time_launches && e->fast_ok && n > 0) {
     // Replay (or capture, then replay) the whole pipeline as one graph.
     if ((rc = reserve_batched(e, s, n, max_a_len, max_b_len))) return rc;
-    const std::vector<uint64_t> key = {(uint64_t)(uintptr_t)d_codes, (uint64_t)(uintptr_t)d_pairs, (uint64_t)n,
+    const std::vector<uint64_t> key = {(uint64_t)(uintptr_t)d_codes, (uint64_t)n_codes, (uint64_t)(uintptr_t)d_pairs,
+                                       (uint64_t)n,
                                        (uint64_t)max_a_len, (uint64_t)max_b_len, (uint64_t)(uintptr_t)d_score,
                                        (uint64_t)(uintptr_t)d_arange, (uint64_t)(uintptr_t)d_brange,
                                        (uint64_t)(uintptr_t)e->d_scratch.p, (uint64_t)e->d_scratch.cap,
                                        (uint64_t)(uintptr_t)e->d_list.p, (uint64_t)(uintptr_t)e->d_ctl.p,
                                        (uint64_t)(uintptr_t)e->d_ovf.p, (uint64_t)(uintptr_t)e->d_flag.p,
                                        (uint64_t)e->tile_k, (uint64_t)e->long_a, (uint64_t)e->thread_class,
-                                       (uint64_t)e->concurrent, (uint64_t)e->hybrid,
+                                       (uint64_t)e->concurrent, (uint64_t)e->hybrid, (uint64_t)e->trace,
                                        (uint64_t)(e->latency_share * 1e6f)};
     auto it = e->graphs_cache.find(key);
     if (it == e->graphs_cache.end()) {
@@ -1569,7 +1628,8 @@ int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_c
       CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       int crc = reset_ctl(e, s);
       if (!crc)
-        crc = run_batched(e, main_bufs(e), s, d_codes, reinterpret_cast<const PairDesc*>(d_pairs), n, max_a_len, max_b_len,
+        crc = run_batched(e, main_bufs(e), s, d_codes, n_codes, reinterpret_cast<const PairDesc*>(d_pairs), n,
+                          max_a_len, max_b_len,
                           d_score, d_arange, d_brange, &launches);
       cudaError_t ce = cudaStreamEndCapture(s, &g);
       if (crc) {
@@ -1591,7 +1651,7 @@ int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_c
   } else {
     if ((rc = reset_ctl(e, s))) return rc;
     CUDA_TRY(cudaEventRecord(e->ev[1], s));
-    rc = run_batched(e, main_bufs(e), s, d_codes, reinterpret_cast<const PairDesc*>(d_pairs), n, max_a_len,
+    rc = run_batched(e, main_bufs(e), s, d_codes, n_codes, reinterpret_cast<const PairDesc*>(d_pairs), n, max_a_len,
                      max_b_len, d_score, d_arange, d_brange, &launches);
     if (rc) return rc;
   }
@@ -1689,7 +1749,7 @@ static int compare_host(ipuma_engine* e, const uint8_t* codes, size_t n_codes, i
     if ((rc = upload(0, n_codes, s))) return rc;
     CUDA_TRY(cudaMemcpyAsync(e->d_pairs.p, pairs, sizeof(ipuma_pair) * (size_t)n, cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaEventRecord(e->ev[1], s));
-    rc = run_batched(e, main_bufs(e), s, e->d_codes.as<uint8_t>(), e->d_pairs.as<PairDesc>(), n, maxA, maxB,
+    rc = run_batched(e, main_bufs(e), s, e->d_codes.as<uint8_t>(), n_codes, e->d_pairs.as<PairDesc>(), n, maxA, maxB,
                      d_score, d_ar, d_br, &launches);
     if (rc) return rc;
     CUDA_TRY(cudaEventRecord(e->ev[2], s));
@@ -1738,7 +1798,8 @@ static int compare_host(ipuma_engine* e, const uint8_t* codes, size_t n_codes, i
       CUDA_TRY(cudaStreamWaitEvent(rs, e->cev[k], 0));
       RunBufs rb = (k & 1) ? rb1 : main_bufs(e);
       rb.ctl = e->d_ctl.as<int>() + (size_t)k * CTL_INTS;
-      if ((rc = run_batched(e, rb, rs, e->d_codes.as<uint8_t>(), e->d_pairs.as<PairDesc>() + off, nk, maxA, maxB,
+      if ((rc = run_batched(e, rb, rs, e->d_codes.as<uint8_t>(), n_codes, e->d_pairs.as<PairDesc>() + off, nk, maxA,
+                            maxB,
                             d_score + off, d_ar + off, d_br + off, &launches)))
         return rc;
       if (pinned_out) {
@@ -1808,7 +1869,9 @@ static int launch_wire(ipuma_engine* e, DevBuf* pairs, const RunBufs& rb, cudaSt
                                      pairs->as<PairDesc>());
   CUDA_TRY(cudaGetLastError());
   *launches += 1;
-  return run_batched(e, rb, s, reinterpret_cast<const uint8_t*>(d_in), pairs->as<PairDesc>(), (int)totalSlots,
+  // Pair offsets are absolute within the tiles' sequence words.
+  return run_batched(e, rb, s, reinterpret_cast<const uint8_t*>(d_in), (size_t)metaOffset * 4,
+                     pairs->as<PairDesc>(), (int)totalSlots,
                      maxA, maxB, d_res, d_res + totalSlots, d_res + 2 * totalSlots, launches);
 }
 

@@ -1,20 +1,19 @@
 // noalloc.cu -- ipuma_gpu_compare_noalloc, the entry point that allocates
 // no memory at all.
 //
-// Some callers cannot call cudaMalloc: code that runs while its stream is
-// being captured into a CUDA graph (allocation is not allowed during
-// capture), host programs that hand every byte of device memory to their
-// own pool and forbid other allocations, or latency-critical paths that
-// cannot afford the device-wide synchronisation cudaMalloc and cudaFree
-// imply.  For them this entry point aligns pairs whose inputs and outputs
-// the caller already holds in device memory, without an engine and without
-// any allocation.
+// Some callers cannot call cudaMalloc: host programs that hand every byte
+// of device memory to their own pool (a framework's caching allocator that
+// reserved the GPU up front) and forbid other allocations, or
+// latency-critical paths that cannot afford the device-wide
+// synchronisation cudaMalloc and cudaFree imply.  For them this entry point
+// aligns pairs whose inputs and outputs the caller already holds in device
+// memory, without an engine and without any allocation.
 //
 // It runs a variant of the s32 wavefront kernel (k_batched<LaneS32, 16, 32>):
 // the one scratch buffer that kernel needs -- the last column of a
 // 512-column strip, handed to the next strip for A longer than 512 -- lives
 // in the file-scope array g_noalloc_scratch (16 MiB, held by every GPU that
-// loads the library until the process exits), and the error word in
+// loads the library until the process exits), and the status word in
 // g_noalloc_status.  The substitution matrix travels in the kernel
 // parameters.  Pairs are taken in a static stride instead of from a queue.
 //
@@ -27,6 +26,11 @@
 // rows the next strip reads).  Calls that overlap on the GPU (different
 // streams, or host threads racing) share the scratch and race; issue them
 // one after another.
+//
+// Each pair descriptor is checked on the device before any code is read:
+// a negative offset or length, or a sequence reaching past n_codes, sets
+// the status to a range error; |A| > 65535 or |B| > max_b_len sets it to a
+// length error; such pairs and empty ones get a zero result.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -42,12 +46,12 @@ using namespace ipuma_dev;
 namespace {
 
 constexpr long kScratchInt2 = 2L << 20;  // 2 Mi int2 = 16 MiB
-constexpr int kMaxRows = 65535;          // ranges are uint16
+constexpr int kMaxLen = 65535;           // ranges are uint16
 constexpr int kWarps = 2;                // warps per block
 constexpr int kMaxDevices = 64;
 
 __device__ __align__(256) int2 g_noalloc_scratch[kScratchInt2];
-__device__ __align__(256) int g_noalloc_status[4];
+__device__ __align__(256) DevStatus g_noalloc_status;
 
 struct SimParam {
   int8_t v[32 * 32];
@@ -55,9 +59,9 @@ struct SimParam {
 
 template <int K>
 __global__ void __launch_bounds__(64) k_noalloc(SwConst sc, SimParam sim, const uint8_t* __restrict__ codes,
-                                                const PairDesc* __restrict__ pairs, int n, int2* scratch,
-                                                long rowsCap, int* status, int* score, int* arange,
-                                                int* brange) {
+                                                long long n_codes, const PairDesc* __restrict__ pairs, int n,
+                                                int2* scratch, long rowsCap, DevStatus* status, int* score,
+                                                int* arange, int* brange) {
   using T = LaneS32;
   using L = SmemLayout<T, K, 32>;
   extern __shared__ __align__(16) uint8_t smem[];
@@ -78,8 +82,14 @@ __global__ void __launch_bounds__(64) k_noalloc(SwConst sc, SimParam sim, const 
   int2* scr = scratch + gw * 2 * rowsCap;
   for (long p = gw; p < n; p += nw) {
     const PairDesc d = pairs[p];
-    if (d.b_len > rowsCap) {
-      if (lane == 0) atomicCAS(status, 0, ERR_LENGTH);
+    const int state = pair_state(d, n_codes, kMaxLen, (int)rowsCap);
+    if (state != PAIR_OK) {
+      if (lane == 0) {
+        report_pair(state, status);
+        score[p] = 0;
+        arange[p] = 0;
+        brange[p] = 0;
+      }
       continue;
     }
     const uint8_t* const a0[1] = {codes + d.a_off};
@@ -95,7 +105,7 @@ __global__ void __launch_bounds__(64) k_noalloc(SwConst sc, SimParam sim, const 
 struct DeviceSymbols {
   bool ready = false;
   int2* scratch = nullptr;
-  int* status = nullptr;
+  DevStatus* status = nullptr;
   int nsm = 0;
 };
 DeviceSymbols g_symbols[kMaxDevices];
@@ -109,13 +119,12 @@ extern "C" int ipuma_gpu_compare_noalloc(const ipuma_sw_config* sw, int32_t forw
                                          const uint8_t* d_codes, size_t n_codes, const ipuma_pair* d_pairs,
                                          int32_t n, int32_t max_b_len, int32_t* d_score, int32_t* d_arange,
                                          int32_t* d_brange, void* stream) {
-  (void)n_codes;
   if (!sw) return fail(IPUMA_ERR_INVALID_ARG, "null scoring configuration");
   if (n < 0) return fail(IPUMA_ERR_INVALID_ARG, "negative pair count");
   if (n == 0) return IPUMA_OK;
   if (!d_codes || !d_pairs || !d_score || !d_arange || !d_brange)
     return fail(IPUMA_ERR_INVALID_ARG, "null device buffer");
-  if (max_b_len < 1 || max_b_len > kMaxRows)
+  if (max_b_len < 1 || max_b_len > kMaxLen)
     return fail(IPUMA_ERR_TOO_LONG, "max_b_len must be 1..65535 for the allocation-free entry point");
   const int gI = sw->gap_init, gE = sw->gap_extend;
   if (!(gI + gE < 0 && gE <= 0))
@@ -142,7 +151,7 @@ extern "C" int ipuma_gpu_compare_noalloc(const ipuma_sw_config* sw, int32_t forw
       ds->scratch = static_cast<int2*>(p);
       if (cudaGetSymbolAddress(&p, g_noalloc_status) != cudaSuccess)
         return fail(IPUMA_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_status) failed");
-      ds->status = static_cast<int*>(p);
+      ds->status = static_cast<DevStatus*>(p);
       cudaDeviceProp prop;
       if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return fail(IPUMA_ERR_CUDA, "device query failed");
       ds->nsm = prop.multiProcessorCount;
@@ -166,16 +175,20 @@ extern "C" int ipuma_gpu_compare_noalloc(const ipuma_sw_config* sw, int32_t forw
   const int blocks = (int)(warps / kWarps);
   const int smem = SmemLayout<LaneS32, 16, 32>::total(m, kWarps);
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  if (cudaMemsetAsync(ds->status, 0, sizeof(int) * 4, s) != cudaSuccess)
+  if (cudaMemsetAsync(ds->status, 0, sizeof(DevStatus), s) != cudaSuccess)
     return fail(IPUMA_ERR_CUDA, "clearing the status word failed");
-  k_noalloc<16><<<blocks, 32 * kWarps, smem, s>>>(sc, sim, d_codes, reinterpret_cast<const PairDesc*>(d_pairs), n,
-                                                   ds->scratch, rowsCap, ds->status, d_score, d_arange, d_brange);
+  k_noalloc<16><<<blocks, 32 * kWarps, smem, s>>>(sc, sim, d_codes, (long long)n_codes,
+                                                   reinterpret_cast<const PairDesc*>(d_pairs), n, ds->scratch,
+                                                   rowsCap, ds->status, d_score, d_arange, d_brange);
   if (cudaGetLastError() != cudaSuccess) return fail(IPUMA_ERR_CUDA, "kernel launch failed");
   int status = 0;
   if (cudaMemcpyAsync(&status, ds->status, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
     return fail(IPUMA_ERR_CUDA, "reading the status word failed");
-  if (status == ERR_LENGTH) return fail(IPUMA_ERR_TOO_LONG, "a pair's b_len exceeds max_b_len");
+  if (status == ERR_LENGTH)
+    return fail(IPUMA_ERR_TOO_LONG, "a pair's b_len exceeds max_b_len or its a_len exceeds 65535");
+  if (status == ERR_RANGE)
+    return fail(IPUMA_ERR_INVALID_ARG, "a pair lies outside the code array (negative or past n_codes)");
   if (status) return fail(IPUMA_ERR_DEVICE, "kernel reported an error");
   return IPUMA_OK;
 }

@@ -51,8 +51,39 @@ struct ClassAllot {
   int pad;
 };
 
+// Device clock in nanoseconds (the trace of class launches).
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 constexpr int ERR_SCRATCH = 1;  // a pass needed more scratch rows than provided
 constexpr int ERR_LENGTH = 2;   // a pair exceeded the stated maximum lengths
+constexpr int ERR_RANGE = 3;    // a pair's offsets or lengths lie outside the code array
+
+// What a kernel does with one pair descriptor of a device-resident batch,
+// checked before any code is read (the same rules as the host-side check of
+// the host-buffer calls): PAIR_OUT for a negative offset or length or a
+// sequence reaching past the n_codes residues of the code array (error
+// status, zero result), PAIR_EMPTY for an empty sequence (zero result),
+// PAIR_LONG beyond the stated maxima (error status, zero result), PAIR_OK.
+constexpr int PAIR_OK = 0, PAIR_EMPTY = 1, PAIR_LONG = 2, PAIR_OUT = 3;
+__device__ __forceinline__ int pair_state(const PairDesc& d, long long n_codes, int max_a, int max_b) {
+  if (d.a_len < 0 || d.b_len < 0 || d.a_off < 0 || d.b_off < 0 || d.a_off > n_codes - d.a_len ||
+      d.b_off > n_codes - d.b_len)
+    return PAIR_OUT;
+  if (d.a_len == 0 || d.b_len == 0) return PAIR_EMPTY;
+  if (d.a_len > max_a || d.b_len > max_b) return PAIR_LONG;
+  return PAIR_OK;
+}
+
+// Records the error of a rejected pair (PAIR_LONG / PAIR_OUT) in the status
+// word; the caller writes its zero result.
+__device__ __forceinline__ void report_pair(int state, DevStatus* st) {
+  if (state == PAIR_LONG) atomicCAS(&st->error, 0, ERR_LENGTH);
+  if (state == PAIR_OUT) atomicCAS(&st->error, 0, ERR_RANGE);
+}
 
 // Shared-memory layout of the wavefront kernels.
 // Per warp: 32 / LANES groups, each with its profile and B-letter ring.
@@ -244,9 +275,12 @@ __global__ void __launch_bounds__(128) k_batched(SwConst sc, const int8_t* __res
                                                  int2* scratch, long rowsCap, int* score,
                                                  int* arange, int* brange, int* overflow_list,
                                                  unsigned long long* rerun_cells, DevStatus* st,
-                                                 const ClassAllot* __restrict__ allot) {
+                                                 const ClassAllot* __restrict__ allot,
+                                                 unsigned long long* trace) {
   if ((int)blockIdx.x >= allot->blocks) return;  // outside this launch's share
   scratch += allot->base;
+  // trace (option "trace"): {~first block start, last warp end} of the launch.
+  if (trace && threadIdx.x == 0) atomicMax(&trace[0], ~global_ns());
   using L = SmemLayout<T, K, LANES>;
   constexpr int NP = T::NP;
   constexpr int GROUPS = L::GROUPS;
@@ -326,6 +360,7 @@ __global__ void __launch_bounds__(128) k_batched(SwConst sc, const int8_t* __res
       }
     }
   }
+  if (trace && lane32 == 0) atomicMax(&trace[1], global_ns());
 }
 
 // One-launch-per-batch kernel over the reference wire buffer.
@@ -376,6 +411,76 @@ __global__ void __launch_bounds__(128) k_plain(SwConst sc, const int8_t* __restr
   }
 }
 
+// The one-launch-per-batch kernel with s16x2 lanes: the same wire buffer,
+// slot order and static stride as k_plain, but one warp aligns two
+// consecutive comparison slots (2g, 2g + 1) in the halves of s16x2 lanes,
+// whatever their lengths.  A slot whose score could have left int16 is
+// redone by the same warp in s32 lanes, so the batch still takes one
+// launch.  It isolates what the batched engine gains by sorting, binning
+// and packing pairs from what it gains by the lane width.
+template <int K>
+__global__ void __launch_bounds__(128) k_plain16(SwConst sc, const int8_t* __restrict__ sim,
+                                                 const int* __restrict__ inputs, long seqWordsPerTile,
+                                                 long metaOffset, int maxBatches, int totalSlots,
+                                                 int2* scratch, long rowsCap, int* results,
+                                                 DevStatus* st) {
+  using L = SmemLayout<LaneS16x2, K, 32>;
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int warps = blockDim.x >> 5;
+  const int wib = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  int8_t* s_simp = reinterpret_cast<int8_t*>(smem);
+  uint8_t* wbase = smem + L::simp_bytes(sc.M) + wib * L::warp_bytes(sc.M);
+  uint8_t* s_prof = wbase;  // the s32 redo uses the first half of it
+  uint16_t* s_bring = reinterpret_cast<uint16_t*>(wbase + L::prof_bytes(sc.M));
+  load_simp(s_simp, sim, sc);
+  __syncthreads();
+  const long gw = (long)blockIdx.x * warps + wib;
+  const long nw = (long)gridDim.x * warps;
+  int2* scr = scratch + gw * 2 * rowsCap;
+  const int* meta = inputs + metaOffset;
+  for (long g0 = 2 * gw; g0 < totalSlots; g0 += 2 * nw) {
+    const uint8_t* a0[2];
+    const uint8_t* b0[2];
+    int al[2], bl[2];
+    bool tooLong = false;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const long g = g0 + h;
+      const bool have = g < totalSlots;
+      const uint8_t* seqs = reinterpret_cast<const uint8_t*>(inputs + (have ? g / maxBatches : 0) * seqWordsPerTile);
+      al[h] = have ? meta[4 * g + 0] : 0;
+      bl[h] = have ? meta[4 * g + 2] : 0;
+      a0[h] = seqs + (have ? meta[4 * g + 1] : 0);
+      b0[h] = seqs + (have ? meta[4 * g + 3] : 0);
+      tooLong |= bl[h] > rowsCap;
+    }
+    if (tooLong) {  // warp-uniform: every lane read the same Meta words
+      if (lane == 0) atomicCAS(&st->error, 0, ERR_SCRATCH);
+      continue;
+    }
+    Best fw[2], rv[2];
+    bool ovf[2];
+    align_pairs<LaneS16x2, K, 32>(sc, s_prof, s_simp, s_bring, a0, b0, al, bl, scr, rowsCap, fw, rv, ovf);
+#pragma unroll 1
+    for (int h = 0; h < 2; ++h) {
+      if (g0 + h >= totalSlots) break;
+      if (ovf[h]) {  // uniform: the score is the 32-lane group's reduction
+        const uint8_t* const a1[1] = {a0[h]};
+        const uint8_t* const b1[1] = {b0[h]};
+        const int al1[1] = {al[h]}, bl1[1] = {bl[h]};
+        Best f1[1], r1[1];
+        bool o1[1];
+        align_pairs<LaneS32, K, 32>(sc, s_prof, s_simp, s_bring, a1, b1, al1, bl1, scr, rowsCap, f1, r1, o1);
+        fw[h] = f1[0];
+        rv[h] = r1[0];
+      }
+      if (lane == 0)
+        write_result(sc, fw[h], rv[h], results, results + totalSlots, results + 2L * totalSlots, g0 + h);
+    }
+  }
+}
+
 // Exact per-thread kernel: one thread per pair, the recurrence written out
 // cell by cell in int32 (codelet_batch_affine.cpp:65-115) with C and F rows
 // in global scratch (2 * maxA int per thread).  Covers every scoring
@@ -411,10 +516,14 @@ static __device__ void exact_pass(const uint8_t* a0, int alen, int da, const uin
   out = Best{s, bi, bj};
 }
 
+// Pairs from the list are checked with pair_state against n_codes and the
+// stated maxima (maxA, maxB); wire-buffer slots were validated before the
+// launch.
 static __global__ void k_exact(SwConst sc, const int8_t* __restrict__ sim, const uint8_t* __restrict__ codes,
-                        const PairDesc* __restrict__ pairs, int n, const int* __restrict__ inputs,
-                        long seqWordsPerTile, long metaOffset, int maxBatches, int* cf_scratch,
-                        long maxA, int* score, int* arange, int* brange) {
+                        long long n_codes, const PairDesc* __restrict__ pairs, int n,
+                        const int* __restrict__ inputs, long seqWordsPerTile, long metaOffset, int maxBatches,
+                        int* cf_scratch, long maxA, int maxB, int* score, int* arange, int* brange,
+                        DevStatus* st) {
   const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long nt = (long)gridDim.x * blockDim.x;
   int* C = cf_scratch + tid * 2 * maxA;
@@ -432,10 +541,12 @@ static __global__ void k_exact(SwConst sc, const int8_t* __restrict__ sim, const
       b = seqs + m[3];
     } else {
       const PairDesc d = pairs[p];
-      alen = d.a_len;
-      blen = d.b_len;
-      a = codes + d.a_off;
-      b = codes + d.b_off;
+      const int state = pair_state(d, n_codes, (int)maxA, maxB);
+      report_pair(state, st);
+      alen = state == PAIR_OK ? d.a_len : 0;
+      blen = state == PAIR_OK ? d.b_len : 0;
+      a = codes + (state == PAIR_OK ? d.a_off : 0);
+      b = codes + (state == PAIR_OK ? d.b_off : 0);
     }
     Best fw{0, 0, 0}, rv{0, 0, 0};
     if (alen > 0 && blen > 0 && alen <= maxA) {
@@ -496,6 +607,7 @@ struct BinParams {
   int forced_class;        // >= 0: every s16x2 pair goes to this class
   int n_s16_classes;
   int max_a, max_b;        // stated maxima (violations set ERR_LENGTH)
+  long long n_codes;       // residues in the code array (pairs past it set ERR_RANGE)
   int M;                   // alphabet size of `sim`
   int force_s32;           // 1: every pair goes to the s32 class
   // Per-thread class (k_thread): one thread per two pairs, so a pair's time
@@ -610,7 +722,7 @@ static __global__ void k_bin_total(BinParams bp, const PairDesc* __restrict__ pa
   unsigned long long local = 0;
   for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
     const PairDesc d = pairs[p];
-    if (d.a_len <= 0 || d.b_len <= 0 || d.a_len > bp.max_a || d.b_len > bp.max_b) continue;
+    if (pair_state(d, bp.n_codes, bp.max_a, bp.max_b) != PAIR_OK) continue;
     local += (unsigned long long)d.a_len * (unsigned long long)d.b_len;
   }
   for (int off = 16; off > 0; off >>= 1) local += __shfl_xor_sync(FULL, local, off);
@@ -623,14 +735,10 @@ static __global__ void k_bin_count(BinParams bp, const uint8_t* __restrict__ cod
                             int* score, int* arange, int* brange) {
   for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
     const PairDesc d = pairs[p];
-    if (d.a_len <= 0 || d.b_len <= 0) {
-      score[p] = 0;
-      arange[p] = 0;
-      brange[p] = 0;
-      continue;
-    }
-    if (d.a_len > bp.max_a || d.b_len > bp.max_b) {
-      atomicCAS(&st->error, 0, ERR_LENGTH);
+    const int state = pair_state(d, bp.n_codes, bp.max_a, bp.max_b);
+    if (state != PAIR_OK) {
+      // Empty, too long or outside the code array: zero result, not listed.
+      report_pair(state, st);
       score[p] = 0;
       arange[p] = 0;
       brange[p] = 0;
@@ -719,7 +827,7 @@ static __global__ void k_bin_scatter(BinParams bp, const PairDesc* __restrict__ 
                               const uint8_t* __restrict__ s32_flag, int* offs, int* list) {
   for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
     const PairDesc d = pairs[p];
-    if (d.a_len <= 0 || d.b_len <= 0 || d.a_len > bp.max_a || d.b_len > bp.max_b) continue;
+    if (pair_state(d, bp.n_codes, bp.max_a, bp.max_b) != PAIR_OK) continue;
     const int pos = atomicAdd(&offs[pair_key(bp, d.a_len, d.b_len, s32_flag[p] != 0, thread_cap(bp))], 1);
     list[pos] = (int)p;
   }

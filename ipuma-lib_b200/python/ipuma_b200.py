@@ -54,7 +54,8 @@ KERNEL_NAMES = {0: "k_batched<s32,L32,K16>", 1: "k_batched<s16x2,L16,K4>",
                 13: "k_batched<s16x2,L16,K14>", 14: "k_batched<s16x2,L16,K5>",
                 15: "k_batched<s16x2,L16,K7>", 16: "k_batched<s16x2,L16,K9>",
                 17: "k_batched<s16x2,L16,K11>", 18: "k_batched<s16x2,L16,K13>",
-                19: "k_batched<s16x2,L16,K15>", 20: "k_hybrid<s16x2->s32,L32,K16>"}
+                19: "k_batched<s16x2,L16,K15>", 20: "k_hybrid<s16x2->s32,L32,K16>",
+                21: "k_plain16<K>"}
 MAX_TIMED = 24  # IPUMA_MAX_TIMED
 
 
@@ -89,7 +90,11 @@ class Stats(ctypes.Structure):
                 ("launches", ctypes.c_int32), ("used_graph", ctypes.c_int32),
                 ("n_timed", ctypes.c_int32), ("timed_kind", ctypes.c_int32 * MAX_TIMED),
                 ("timed_ms", ctypes.c_double * MAX_TIMED), ("timed_cells", ctypes.c_int64 * MAX_TIMED),
-                ("chunks", ctypes.c_int32)]
+                ("chunks", ctypes.c_int32), ("n_trace", ctypes.c_int32),
+                ("trace_kind", ctypes.c_int32 * MAX_TIMED),
+                ("trace_start_ms", ctypes.c_double * MAX_TIMED),
+                ("trace_end_ms", ctypes.c_double * MAX_TIMED),
+                ("trace_cells", ctypes.c_int64 * MAX_TIMED)]
 
 
 class ServerConfig(ctypes.Structure):

@@ -1,9 +1,10 @@
 """Generates the golden fixtures in tests/golden/ from the reference tree.
 
-Run in a container that has the reference at /root/reference (read-only) and
-the reference libraries built by ``make -C oracle ref``:
+Run where the reference tree is available (read-only; its path in
+IPUMA_REF_DIR or --ref) and the reference libraries are built by
+``make -C oracle ref``:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    IPUMA_REF_DIR=<reference tree> python tests/golden/make_golden.py [--ref DIR]
 
 Outputs (committed; nothing at test time reads the reference tree):
 
@@ -205,8 +206,11 @@ def random_cases(rng, oracle):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("IPUMA_REF_DIR"),
+                    help="reference tree (default: $IPUMA_REF_DIR)")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("pass --ref or set IPUMA_REF_DIR to the reference tree")
     ref = args.ref
     rd = lambda p: open(os.path.join(ref, p)).read()
 

@@ -406,6 +406,79 @@ def test_rejects_pairs_outside_code_array():
         assert s[0] == 4
 
 
+@pytest.mark.parametrize("graphs", [0, 1])
+def test_device_call_rejects_pairs_outside_code_array(graphs):
+    # Device-resident descriptors are checked on the device before any code
+    # is read.  The codes live in a valid, larger allocation; the pairs reach
+    # past the n_codes residues the caller declares, or carry a negative
+    # field.  The rejected pairs get a zero result, the others their real
+    # one, and the call reports IPUMA_ERR_INVALID_ARG.
+    import torch
+    wl = workloads.dna_batched(n=300, seed=71)
+    case = _wl_case(wl)
+    pairs = ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len)
+    last = int(np.argmax(pairs["b_off"] + pairs["b_len"]))
+    declared = int(pairs["b_off"][last] + pairs["b_len"][last]) - 1
+    bad = pairs.copy()
+    bad["a_len"][7] = -3
+    bad["b_off"][11] = -1
+    sim = oracle.select_matrix(wl.similarity, wl.match, wl.mismatch, wl.ambiguity)
+    want = oracle.sw_batch(wl.codes, wl.a_off, wl.a_len, wl.b_off, wl.b_len, sim, wl.gap_init,
+                           wl.gap_extend, forward_only=True)
+    d_codes = torch.from_numpy(wl.codes).cuda()
+    with _engine(case, True, graphs=graphs) as e:
+        for desc, n_codes, rejected in ((pairs, declared, [last]), (bad, wl.codes.size, [7, 11])):
+            d_pairs = torch.from_numpy(desc.view(np.uint8)).cuda()
+            out = torch.full((3, wl.n), -7, dtype=torch.int32, device="cuda")
+            with pytest.raises(ib.IpumaError) as ei:
+                e.compare_device(d_codes.data_ptr(), n_codes, d_pairs.data_ptr(), wl.n,
+                                 int(wl.a_len.max()), int(wl.b_len.max()), out[0].data_ptr(),
+                                 out[1].data_ptr(), out[2].data_ptr())
+            assert ei.value.code == ib.ERR_INVALID_ARG and "outside" in str(ei.value)
+            got = out.cpu().numpy()
+            keep = np.setdiff1d(np.arange(wl.n), rejected)
+            assert (got[:, rejected] == 0).all()
+            for k in range(3):
+                assert np.array_equal(got[k][keep], want[k][keep])
+        # and a valid call on the same engine is exact
+        d_pairs = torch.from_numpy(pairs.view(np.uint8)).cuda()
+        out = torch.zeros((3, wl.n), dtype=torch.int32, device="cuda")
+        e.compare_device(d_codes.data_ptr(), wl.codes.size, d_pairs.data_ptr(), wl.n,
+                         int(wl.a_len.max()), int(wl.b_len.max()), out[0].data_ptr(),
+                         out[1].data_ptr(), out[2].data_ptr())
+        _assert_same(out.cpu().numpy(), want, "device call after rejections")
+
+
+@pytest.mark.parametrize("tile_k", [1, 4])
+def test_reverse_early_stop_over_several_strips(tile_k):
+    # Full alignments whose A spans several strips of a narrow class (64 or
+    # 256 columns): the reverse pass of each pair runs over [0..Aend] x
+    # [0..Bend], so the two pairs of a 16-lane group get very different
+    # reverse lengths; one finds its target (the forward score) and stops
+    # early while the other runs out of rows.  Mixed related and unrelated
+    # pairs, local alignments anywhere in the matrix.
+    rng = np.random.default_rng(72 + tile_k)
+    A, B = [], []
+    for _ in range(600):
+        a = "".join(rng.choice(list("ACGT"), int(rng.integers(100, 700))))
+        if rng.random() < 0.7:
+            lo = int(rng.integers(0, len(a) - 50))
+            hi = int(rng.integers(lo + 30, min(len(a), lo + 400)))
+            core = list(a[lo:hi])
+            for k in range(len(core)):
+                if rng.random() < 0.08:
+                    core[k] = rng.choice(list("ACGT"))
+            b = ("".join(rng.choice(list("ACGT"), int(rng.integers(0, 300)))) + "".join(core) +
+                 "".join(rng.choice(list("ACGT"), int(rng.integers(0, 300)))))
+        else:
+            b = "".join(rng.choice(list("ACGT"), int(rng.integers(50, 900))))
+        A.append(a)
+        B.append(b)
+    case = {"similarity": "na", "match": 1, "mismatch": -1, "ambiguity": -1, "datatype": "na",
+            "gapInit": 0, "gapExtend": -1, "A": A, "B": B}
+    _assert_same(_gpu(case, forward_only=False, tile_k=tile_k), _oracle(case), "tile_k %d" % tile_k)
+
+
 # ------------------------------------------------------- wire buffer ---
 
 def _wire(wl, tiles, max_batches, bufsize):

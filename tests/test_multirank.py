@@ -86,3 +86,49 @@ def test_reference_arm_under_torchrun_prints_once():
     line = json.loads(lines[0])
     assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
     assert line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_gpus_flag_launches_ranks_without_torchrun():
+    # `bench.py --gpus 2` started as one process re-launches itself through
+    # torch.distributed.run (WORLD_SIZE unset): two ranks start, rank 0 alone
+    # prints the line and reports the real world size.  The reference arm
+    # needs no GPU, so the launch runs here on CPU.
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    if not oracle.have_ssw():
+        pytest.skip("reference SSW library not built")
+    cmd = [sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference", "--gpus", "2",
+           "--steps", "1", "--warmup", "1", "--pairs", "2000"]
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT")}
+    env["OMP_NUM_THREADS"] = "2"
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=300, env=env, cwd=REPO)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["n_gpus"] == 2
+    assert line["config"]["pairs_per_gpu"] == 2000
+
+
+def test_launcher_builds_a_torchrun_command(monkeypatch):
+    # The re-launch keeps every argument and rendezvouses on 127.0.0.1.
+    sys.path.insert(0, REPO)
+    import bench
+    seen = {}
+
+    class Done:
+        returncode = 0
+
+    def fake_run(cmd, timeout):
+        seen["cmd"] = cmd
+        return Done()
+
+    monkeypatch.setattr(bench.subprocess, "run", fake_run)
+    args = bench.parse(["--gpus", "4", "--steps", "7"])
+    assert bench.launch_ranks(args, ["--gpus", "4", "--steps", "7"]) == 0
+    cmd = seen["cmd"]
+    i = cmd.index("--nproc-per-node")
+    assert cmd[i + 1] == "4"
+    assert cmd[cmd.index("--master-addr") + 1] == "127.0.0.1"
+    assert cmd[-3:] == ["--gpus", "4", "--steps", "7"][-3:] and "torch.distributed.run" in cmd
