@@ -23,8 +23,11 @@
  *   ipuma_gpu_poll          (non-blocking form of Job::join, :489-494)
  *   ipuma_gpu_compare       compare_local minus the host partitioning
  *                           (:564-663): pairs straight from a code array
- *   ipuma_gpu_compare_packed  the same with 2- or 4-bit packed codes
+ *   ipuma_gpu_compare_packed  the same with 2-, 4- or 5-bit packed codes
  *   ipuma_gpu_compare_device  the same with device-resident buffers
+ *   ipuma_gpu_compare_device_packed  device-resident packed codes
+ *   ipuma_pack_codes        (no counterpart: the reference stores one byte
+ *                           per residue, fill_input_buffer :874-877)
  *   ipuma_encode            swatlib::Encoding::encode  src/swatlib/encoding.cpp:38-60
  *   ipuma_select_matrix     swatlib::selectMatrix      src/swatlib/similarity.cpp:89-105
  */
@@ -181,9 +184,11 @@ int ipuma_host_alloc(size_t bytes, void** out);
 void ipuma_host_free(void* p);
 
 /* Host-only helpers (no GPU needed). */
-/* Packs n codes for ipuma_gpu_compare_packed into out[ceil(n * bits / 8)]:
- * bits = 4 takes codes < 16, bits = 2 takes A, T, C, G (codes 1..4); any
- * other code gives IPUMA_ERR_BAD_SEQUENCE. */
+/* Packs n codes for the packed compare calls into out[ceil(n * bits / 8)],
+ * a little-endian bit stream: residue r in bits [bits*r, bits*r + bits).
+ * bits = 5 takes codes < 32 (every amino-acid code, 0..24), bits = 4 codes
+ * < 16 (nucleic acids with IUPAC codes), bits = 2 A, T, C, G (codes 1..4,
+ * stored as code - 1); any other code gives IPUMA_ERR_BAD_SEQUENCE. */
 int ipuma_pack_codes(const uint8_t* codes, size_t n, int32_t bits, uint8_t* out);
 /* Encodes n chars into codes; unknown NA characters (code 16, which has no
  * row in the 16x16 NA matrix) are rejected with IPUMA_ERR_BAD_SEQUENCE. */
@@ -278,14 +283,13 @@ int ipuma_gpu_join_stats(ipuma_engine* e, uint64_t job, int64_t timeout_ms, ipum
 int ipuma_gpu_compare(ipuma_engine* e, const uint8_t* codes, size_t n_codes,
                       const ipuma_pair* pairs, int32_t n, int32_t* score, int32_t* arange,
                       int32_t* brange);
-/* ipuma_gpu_compare with packed codes (ipuma_pack_codes), for alphabets of
- * at most 16 codes (nucleic acids):
- *   bits = 4: two residues per byte, residue 2k in the low nibble of byte k;
- *   bits = 2: four per byte, residue 4k+q in bits 2q..2q+1 of byte k holding
- *             code - 1 (A, T, C, G only: codes 1..4).
- * n_codes, offsets and lengths count residues.  Halves (quarters) the
- * host-to-device bytes; each uploaded range is expanded on the device
- * before its pairs run. */
+/* ipuma_gpu_compare with packed codes (ipuma_pack_codes):
+ *   bits = 5: amino acids (or any alphabet of at most 32 codes);
+ *   bits = 4: alphabets of at most 16 codes (nucleic acids with IUPAC);
+ *   bits = 2: A, T, C, G only (nucleic acids, codes 1..4).
+ * n_codes, offsets and lengths count residues.  The codes travel and stay
+ * packed: the kernels read the bit stream themselves, so the upload and
+ * the device copy are bits/8 of the one-byte form. */
 int ipuma_gpu_compare_packed(ipuma_engine* e, const uint8_t* packed, size_t n_codes, int32_t bits,
                              const ipuma_pair* pairs, int32_t n, int32_t* score, int32_t* arange,
                              int32_t* brange);
@@ -299,6 +303,14 @@ int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_c
                              const ipuma_pair* d_pairs, int32_t n, int32_t max_a_len,
                              int32_t max_b_len, int32_t* d_score, int32_t* d_arange,
                              int32_t* d_brange, void* stream);
+/* ipuma_gpu_compare_device on packed codes (ipuma_pack_codes layout, bits =
+ * 2, 4 or 5) that the kernels read directly.  d_packed starts 4-byte
+ * aligned and is readable for ceil(n_codes * bits / 8) bytes rounded up to
+ * a multiple of 4, plus 4 more bytes (the word after the last residue's). */
+int ipuma_gpu_compare_device_packed(ipuma_engine* e, const uint8_t* d_packed, size_t n_codes, int32_t bits,
+                                    const ipuma_pair* d_pairs, int32_t n, int32_t max_a_len,
+                                    int32_t max_b_len, int32_t* d_score, int32_t* d_arange,
+                                    int32_t* d_brange, void* stream);
 
 /* Grows every device buffer that ipuma_gpu_compare_device needs for up to
  * n pairs with |A| <= max_a_len and |B| <= max_b_len, so that such calls

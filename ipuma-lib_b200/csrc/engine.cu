@@ -400,7 +400,7 @@ int timed_end(ipuma_engine* e, cudaStream_t s) {
 // allot_idx = entry of the control block's ClassAllot table (the class, or
 // NCLASS_MAX for the s32 rerun).
 template <class T, int K, int LANES, bool HYB = false>
-int launch_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_t* codes,
+int launch_batched(ipuma_engine* e, const SwConst& sc, const RunBufs& rb, cudaStream_t s, const uint8_t* codes,
                    const PairDesc* pairs, const int* list, const int* range, int* head, long rowsCap,
                    int* score, int* arange, int* brange, int kind, int cls, int allot_idx) {
   const int smem = smem_for<T, K, LANES>(e);
@@ -411,7 +411,7 @@ int launch_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uin
   if ((rc = timed_begin(e, s, kind, cls))) return rc;
   auto* kern = e->sc.forwardOnly ? k_batched<T, K, LANES, HYB, true> : k_batched<T, K, LANES, HYB, false>;
   kern<<<grid, kThreads, smem, s>>>(
-      e->sc, e->d_sim.as<int8_t>(), codes, pairs, list, range, head, rb.scratch->as<int2>(),
+      sc, e->d_sim.as<int8_t>(), codes, pairs, list, range, head, rb.scratch->as<int2>(),
       rowsCap, score, arange, brange, rb.ovf->as<int>(), cells + CELLS_RERUN,
       reinterpret_cast<DevStatus*>(ctl + CTL_STATUS),
       reinterpret_cast<const ClassAllot*>(ctl + CTL_ALLOT) + allot_idx,
@@ -524,13 +524,16 @@ int reserve_batched(ipuma_engine* e, cudaStream_t s, int n, int maxA, int maxB) 
 // Results land at score[p], arange[p], brange[p].
 // n_codes = residues the code array holds: pairs reaching past it are
 // rejected on the device (status ERR_RANGE) before any code is read.
+// bits = bits per residue of `codes` (8: bytes; 2, 4, 5: packed, code_at).
 int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_t* codes, size_t n_codes,
-                const PairDesc* pairs, int n, int maxA, int maxB, int* score, int* arange, int* brange,
-                int* launches) {
+                int bits, const PairDesc* pairs, int n, int maxA, int maxB, int* score, int* arange,
+                int* brange, int* launches) {
   int rc;
   if (n <= 0) return IPUMA_OK;
   int* ctl = rb.ctl;
   DevStatus* st = reinterpret_cast<DevStatus*>(ctl + CTL_STATUS);
+  SwConst sc = e->sc;
+  sc.bits = bits;
 
   if (!e->fast_ok) {
     // Exact per-thread kernel; C and F rows in global scratch.
@@ -539,9 +542,8 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
     threads = ((threads + 127) / 128) * 128;
     if ((rc = e->d_cf.ensure(sizeof(int) * 2 * maxAcap * threads, s))) return rc;
     if ((rc = timed_begin(e, s, IPUMA_KERNEL_EXACT, -1))) return rc;
-    k_exact<<<(int)(threads / 128), 128, 0, s>>>(e->sc, e->d_sim.as<int8_t>(), codes, (long long)n_codes, pairs,
-                                                  n, nullptr, 0, 0, 1, e->d_cf.as<int>(), maxAcap, maxB,
-                                                  score, arange, brange, st);
+    k_exact<<<(int)(threads / 128), 128, 0, s>>>(sc, e->d_sim.as<int8_t>(), codes, (long long)n_codes, pairs, n,
+                                                  e->d_cf.as<int>(), maxAcap, maxB, score, arange, brange, st);
     CUDA_TRY(cudaGetLastError());
     if ((rc = timed_end(e, s))) return rc;
     *launches += 1;
@@ -570,7 +572,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   bp.widest = kClsWidest;
   const long thrThreads = thread_threads<16>(e);
   bp.thr_cls = kClsThread;
-  bp.thr_on = e->thread_class;
+  bp.thr_on = e->thread_class && bits == 8;
   bp.thr_k = kClasses[kClsThread].width;
   bp.thr_max_rows = kThrMaxRows;
   bp.thr_cap_scale = kThrLatencyShare / (2.0f * (float)thrThreads);
@@ -585,7 +587,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   unsigned enabled = kCoarseClasses | (1u << kClsS32);
   if (e->hybrid) enabled |= 1u << kClsHi;
   if (n >= kFineClassMinPairs) enabled |= kFineClasses;
-  if (e->thread_class) enabled |= 1u << kClsThread;
+  if (e->thread_class && bits == 8) enabled |= 1u << kClsThread;  // k_thread reads bytes only
   if (e->tile_k > 0) enabled |= 1u << (e->tile_k - 1);
   bp.enabled = enabled;
   class_grids(e, maxA, maxB, bp.grid, bp.scr_per_block);
@@ -616,6 +618,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   bp.max_a = maxA;
   bp.max_b = maxB;
   bp.n_codes = (long long)n_codes;
+  bp.bits = bits;
   bp.M = e->M;
   bp.s16_limit = e->sc.s16Limit;
   if ((rc = rb.flag->ensure((size_t)n + 64, s))) return rc;
@@ -666,7 +669,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
 #define IPUMA_LAUNCH(T, K, L, cls)                                                                     \
   if ((enabled >> (cls)) & 1u) {                                                                       \
     cudaStream_t cs = on(cls);                                                                         \
-    if ((rc = launch_batched<T, K, L>(e, rb, cs, codes, pairs, list, R + 2 * (cls), heads + (cls),     \
+    if ((rc = launch_batched<T, K, L>(e, sc, rb, cs, codes, pairs, list, R + 2 * (cls), heads + (cls), \
                                       rowsCap, score, arange, brange, kClasses[cls].kind, cls, cls)))  \
       return rc;                                                                                       \
     if ((rc = done(cls))) return rc;                                                                   \
@@ -674,7 +677,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   }
   if ((enabled >> kClsHi) & 1u) {
     cudaStream_t cs = on(kClsHi);
-    if ((rc = launch_batched<LaneS16x2, 16, 32, true>(e, rb, cs, codes, pairs, list, R + 2 * kClsHi,
+    if ((rc = launch_batched<LaneS16x2, 16, 32, true>(e, sc, rb, cs, codes, pairs, list, R + 2 * kClsHi,
                                                       heads + kClsHi, rowsCap, score, arange, brange,
                                                       kClasses[kClsHi].kind, kClsHi, kClsHi)))
       return rc;
@@ -708,7 +711,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
 #undef IPUMA_LAUNCH
   // Exact 32-bit rerun of the s16x2 pairs whose score may have overflowed
   // (after every class: it reads their overflow list).
-  if ((rc = launch_batched<LaneS32, 16, 32>(e, rb, s, codes, pairs, rb.ovf->as<int>(), ctl + CTL_STATUS + 1,
+  if ((rc = launch_batched<LaneS32, 16, 32>(e, sc, rb, s, codes, pairs, rb.ovf->as<int>(), ctl + CTL_STATUS + 1,
                                             heads + NCLASS_MAX, rowsCap, score, arange, brange,
                                             IPUMA_KERNEL_S32_RERUN, CELLS_RERUN, NCLASS_MAX)))
     return rc;
@@ -972,7 +975,8 @@ int time_class(ipuma_engine* e, int cls, int n, int alen, int blen, const DevBuf
   for (int rep = 0; rep < 2 && rc == IPUMA_OK; ++rep) {
     int launches = 0;
     if ((rc = reset_ctl(e, s))) break;
-    if ((rc = run_batched(e, main_bufs(e), s, e->d_codes.as<uint8_t>(), bytes, e->d_pairs.as<PairDesc>(), n, alen, blen,
+    if ((rc = run_batched(e, main_bufs(e), s, e->d_codes.as<uint8_t>(), bytes, 8, e->d_pairs.as<PairDesc>(), n, alen,
+                          blen,
                           out, out + n,
                           out + 2 * n, &launches)))
       break;
@@ -1339,28 +1343,31 @@ int ipuma_encode(int32_t datatype, const char* s, size_t n, uint8_t* out) {
 
 int ipuma_pack_codes(const uint8_t* codes, size_t n, int32_t bits, uint8_t* out) {
   if ((!codes || !out) && n) return fail(IPUMA_ERR_INVALID_ARG, "null pointer");
-  if (bits != 2 && bits != 4) return fail(IPUMA_ERR_INVALID_ARG, "bits must be 2 or 4, not %d", bits);
-  const size_t per = 8 / bits;
-  const size_t bytes = (n + per - 1) / per;
+  if (bits != 2 && bits != 4 && bits != 5) return fail(IPUMA_ERR_INVALID_ARG, "bits must be 2, 4 or 5, not %d", bits);
+  // Groups of 8 residues fill `bits` whole bytes of the little-endian bit
+  // stream; the last group writes only the bytes its residues reach.
+  const size_t groups = (n + 7) / 8;
+  const size_t bytes = (n * (size_t)bits + 7) / 8;
   const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
-  const int nthr = (int)std::max<size_t>(1, std::min<size_t>({(size_t)16, (size_t)hw, bytes >> 22}));
+  const int nthr = (int)std::max<size_t>(1, std::min<size_t>({(size_t)16, (size_t)hw, groups >> 20}));
   std::vector<size_t> bad(nthr, SIZE_MAX);
   auto work = [&](int t) {
-    const size_t b0 = bytes * t / nthr, b1 = bytes * (t + 1) / nthr;
-    for (size_t b = b0; b < b1; ++b) {
-      uint32_t v = 0;
-      for (size_t q = 0; q < per; ++q) {
-        const size_t i = per * b + q;
+    const size_t g0 = groups * t / nthr, g1 = groups * (t + 1) / nthr;
+    for (size_t g = g0; g < g1; ++g) {
+      uint64_t v = 0;
+      for (size_t q = 0; q < 8; ++q) {
+        const size_t i = 8 * g + q;
         if (i >= n) break;
-        // 4 bits: the code; 2 bits: code - 1 for A, T, C, G (1..4).
-        const uint32_t x = (bits == 4) ? codes[i] : (uint32_t)codes[i] - 1u;
+        // 2 bits: code - 1 for A, T, C, G (1..4); 4 and 5 bits: the code.
+        const uint32_t x = (bits == 2) ? (uint32_t)codes[i] - 1u : codes[i];
         if (x >= (1u << bits)) {
           bad[t] = i;
           return;
         }
-        v |= x << (bits * q);
+        v |= (uint64_t)x << (bits * q);
       }
-      out[b] = (uint8_t)v;
+      for (size_t k = 0; k < (size_t)bits && (size_t)bits * g + k < bytes; ++k)
+        out[(size_t)bits * g + k] = (uint8_t)(v >> (8 * k));
     }
   };
   std::vector<std::thread> pool;
@@ -1459,6 +1466,7 @@ int ipuma_gpu_create(const ipuma_sw_config* sw, const ipuma_algo_config* algo, i
   // s16x2 lanes: H <= 32767 - maxSub guarantees no halfword overflow.
   e->sc.s16Limit = 32767 - std::max(0, e->maxSub);
   e->sc.maxSub = std::max(0, e->maxSub);
+  e->sc.bits = 8;
   e->s16_ok = e->fast_ok;
   e->s16_max_len = e->maxSub > 0 ? (e->sc.s16Limit / e->maxSub) : (1 << 30);
   set_default_rates(e.get());
@@ -1590,14 +1598,36 @@ int ipuma_gpu_reserve(ipuma_engine* e, int32_t n, int32_t max_a_len, int32_t max
   return IPUMA_OK;
 }
 
-int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_codes,
-                             const ipuma_pair* d_pairs, int32_t n, int32_t max_a_len,
-                             int32_t max_b_len, int32_t* d_score, int32_t* d_arange,
-                             int32_t* d_brange, void* stream) {
+// Checks a packed-code request: the width fits the engine's alphabet and
+// the per-thread class (byte codes only) is not forced.
+static int check_bits(const ipuma_engine* e, int bits) {
+  if (bits != 2 && bits != 4 && bits != 5) return fail(IPUMA_ERR_INVALID_ARG, "bits must be 2, 4 or 5, not %d", bits);
+  // 2-bit codes are A, T, C, G = nucleic-acid codes 1..4.
+  if (bits == 2 && e->sw.datatype != IPUMA_DT_NUCLEIC_ACID)
+    return fail(IPUMA_ERR_INVALID_ARG, "2-bit codes are nucleic-acid codes");
+  if (e->M > (1 << bits))
+    return fail(IPUMA_ERR_INVALID_ARG, "%d-bit codes hold at most %d letters (this alphabet has %d)", bits, 1 << bits,
+                e->M);
+  if (e->tile_k == kClsThread + 1)
+    return fail(IPUMA_ERR_INVALID_ARG, "the per-thread class (tile_k %d) reads one byte per residue", e->tile_k);
+  return IPUMA_OK;
+}
+
+// Body of ipuma_gpu_compare_device (bits = 8) and
+// ipuma_gpu_compare_device_packed (bits = 2, 4, 5).
+static int compare_dev(ipuma_engine* e, const uint8_t* d_codes, size_t n_codes, int bits,
+                       const ipuma_pair* d_pairs, int32_t n, int32_t max_a_len, int32_t max_b_len,
+                       int32_t* d_score, int32_t* d_arange, int32_t* d_brange, void* stream) {
   if (!e) return fail(IPUMA_ERR_INVALID_ARG, "null engine");
   if (n < 0) return fail(IPUMA_ERR_INVALID_ARG, "negative pair count");
   if (n > 0 && (!d_codes || !d_pairs || !d_score || !d_arange || !d_brange))
     return fail(IPUMA_ERR_INVALID_ARG, "null buffer");
+  if (bits != 8) {
+    int rcb = check_bits(e, bits);
+    if (rcb) return rcb;
+    if (reinterpret_cast<uintptr_t>(d_codes) & 3)
+      return fail(IPUMA_ERR_INVALID_ARG, "packed codes must start 4-byte aligned");
+  }
   std::lock_guard<std::mutex> lk(e->mu);
   CUDA_TRY(cudaSetDevice(e->device));
   cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : e->stream;
@@ -1608,7 +1638,8 @@ int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_c
   if (e->graphs && !e->time_launches && e->fast_ok && n > 0) {
     // Replay (or capture, then replay) the whole pipeline as one graph.
     if ((rc = reserve_batched(e, s, n, max_a_len, max_b_len))) return rc;
-    const std::vector<uint64_t> key = {(uint64_t)(uintptr_t)d_codes, (uint64_t)n_codes, (uint64_t)(uintptr_t)d_pairs,
+    const std::vector<uint64_t> key = {(uint64_t)(uintptr_t)d_codes, (uint64_t)n_codes, (uint64_t)bits,
+                                       (uint64_t)(uintptr_t)d_pairs,
                                        (uint64_t)n,
                                        (uint64_t)max_a_len, (uint64_t)max_b_len, (uint64_t)(uintptr_t)d_score,
                                        (uint64_t)(uintptr_t)d_arange, (uint64_t)(uintptr_t)d_brange,
@@ -1628,7 +1659,7 @@ int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_c
       CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       int crc = reset_ctl(e, s);
       if (!crc)
-        crc = run_batched(e, main_bufs(e), s, d_codes, n_codes, reinterpret_cast<const PairDesc*>(d_pairs), n,
+        crc = run_batched(e, main_bufs(e), s, d_codes, n_codes, bits, reinterpret_cast<const PairDesc*>(d_pairs), n,
                           max_a_len, max_b_len,
                           d_score, d_arange, d_brange, &launches);
       cudaError_t ce = cudaStreamEndCapture(s, &g);
@@ -1651,7 +1682,8 @@ int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_c
   } else {
     if ((rc = reset_ctl(e, s))) return rc;
     CUDA_TRY(cudaEventRecord(e->ev[1], s));
-    rc = run_batched(e, main_bufs(e), s, d_codes, n_codes, reinterpret_cast<const PairDesc*>(d_pairs), n, max_a_len,
+    rc = run_batched(e, main_bufs(e), s, d_codes, n_codes, bits, reinterpret_cast<const PairDesc*>(d_pairs), n,
+                     max_a_len,
                      max_b_len, d_score, d_arange, d_brange, &launches);
     if (rc) return rc;
   }
@@ -1713,29 +1745,18 @@ static int compare_host(ipuma_engine* e, const uint8_t* codes, size_t n_codes, i
   cudaStream_t s = e->stream;
   int rc;
   if ((rc = maybe_autotune(e))) return rc;
-  if ((rc = e->d_codes.ensure(std::max<size_t>(n_codes, 1), s))) return rc;
+  // Packed codes stay packed on the device (the kernels decode them, code_at):
+  // the buffer covers the host's bytes rounded up to a word plus one word.
+  const size_t hostBytes = bits == 8 ? n_codes : (n_codes * (size_t)bits + 7) / 8;
+  DevBuf& dcodes = bits == 8 ? e->d_codes : e->d_packed;
+  if ((rc = dcodes.ensure(std::max<size_t>(((hostBytes + 3) & ~(size_t)3) + 8, 16), s))) return rc;
   if ((rc = e->d_pairs.ensure(sizeof(ipuma_pair) * (size_t)n, s))) return rc;
   if ((rc = e->d_res.ensure(sizeof(int32_t) * 3 * (size_t)n, s))) return rc;
-  // The expansion kernels read whole 8- or 4-byte words around each range.
-  const size_t perByte = 8 / bits;
-  if (bits < 8 && (rc = e->d_packed.ensure(((n_codes + perByte - 1) / perByte + 31) & ~(size_t)15, s)))
-    return rc;
-  // Puts residues [lo, hi) into d_codes on stream `us`.
+  // Puts the bytes holding residues [lo, hi) on the device, on stream `us`.
   auto upload = [&](size_t lo, size_t hi, cudaStream_t us) -> int {
     if (lo >= hi) return IPUMA_OK;
-    if (bits == 8) {
-      CUDA_TRY(cudaMemcpyAsync(e->d_codes.as<uint8_t>() + lo, codes + lo, hi - lo, cudaMemcpyHostToDevice, us));
-      return IPUMA_OK;
-    }
-    const size_t blo = lo / perByte, bhi = (hi + perByte - 1) / perByte;
-    CUDA_TRY(cudaMemcpyAsync(e->d_packed.as<uint8_t>() + blo, codes + blo, bhi - blo, cudaMemcpyHostToDevice, us));
-    const size_t blocks16 = (hi - (lo & ~(size_t)15) + 15) / 16;
-    const int grid = (int)std::max<size_t>(1, std::min<size_t>((blocks16 + 255) / 256, (size_t)e->nsm * 8));
-    if (bits == 4)
-      k_unpack4<<<grid, 256, 0, us>>>(e->d_packed.as<uint8_t>(), lo, hi, e->d_codes.as<uint8_t>());
-    else
-      k_unpack2<<<grid, 256, 0, us>>>(e->d_packed.as<uint8_t>(), lo, hi, e->d_codes.as<uint8_t>());
-    CUDA_TRY(cudaGetLastError());
+    const size_t blo = lo * (size_t)bits / 8, bhi = std::min(hostBytes, (hi * (size_t)bits + 7) / 8);
+    CUDA_TRY(cudaMemcpyAsync(dcodes.as<uint8_t>() + blo, codes + blo, bhi - blo, cudaMemcpyHostToDevice, us));
     return IPUMA_OK;
   };
   e->stats = ipuma_stats{};
@@ -1749,7 +1770,7 @@ static int compare_host(ipuma_engine* e, const uint8_t* codes, size_t n_codes, i
     if ((rc = upload(0, n_codes, s))) return rc;
     CUDA_TRY(cudaMemcpyAsync(e->d_pairs.p, pairs, sizeof(ipuma_pair) * (size_t)n, cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaEventRecord(e->ev[1], s));
-    rc = run_batched(e, main_bufs(e), s, e->d_codes.as<uint8_t>(), n_codes, e->d_pairs.as<PairDesc>(), n, maxA, maxB,
+    rc = run_batched(e, main_bufs(e), s, dcodes.as<uint8_t>(), n_codes, bits, e->d_pairs.as<PairDesc>(), n, maxA, maxB,
                      d_score, d_ar, d_br, &launches);
     if (rc) return rc;
     CUDA_TRY(cudaEventRecord(e->ev[2], s));
@@ -1798,7 +1819,7 @@ static int compare_host(ipuma_engine* e, const uint8_t* codes, size_t n_codes, i
       CUDA_TRY(cudaStreamWaitEvent(rs, e->cev[k], 0));
       RunBufs rb = (k & 1) ? rb1 : main_bufs(e);
       rb.ctl = e->d_ctl.as<int>() + (size_t)k * CTL_INTS;
-      if ((rc = run_batched(e, rb, rs, e->d_codes.as<uint8_t>(), n_codes, e->d_pairs.as<PairDesc>() + off, nk, maxA,
+      if ((rc = run_batched(e, rb, rs, dcodes.as<uint8_t>(), n_codes, bits, e->d_pairs.as<PairDesc>() + off, nk, maxA,
                             maxB,
                             d_score + off, d_ar + off, d_br + off, &launches)))
         return rc;
@@ -1840,13 +1861,22 @@ int ipuma_gpu_compare_packed(ipuma_engine* e, const uint8_t* packed, size_t n_co
                              const ipuma_pair* pairs, int32_t n, int32_t* score, int32_t* arange,
                              int32_t* brange) {
   if (!e) return fail(IPUMA_ERR_INVALID_ARG, "null engine");
-  if (bits != 2 && bits != 4) return fail(IPUMA_ERR_INVALID_ARG, "bits must be 2 or 4, not %d", bits);
-  // 2-bit codes are A, T, C, G = nucleic-acid codes 1..4.
-  if (bits == 2 && e->sw.datatype != IPUMA_DT_NUCLEIC_ACID)
-    return fail(IPUMA_ERR_INVALID_ARG, "2-bit codes are nucleic-acid codes");
-  if (e->M > 16)
-    return fail(IPUMA_ERR_INVALID_ARG, "packed codes need an alphabet of at most 16 letters (this one has %d)", e->M);
+  int rc = check_bits(e, bits);
+  if (rc) return rc;
   return compare_host(e, packed, n_codes, bits, pairs, n, score, arange, brange);
+}
+
+int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_codes, const ipuma_pair* d_pairs,
+                             int32_t n, int32_t max_a_len, int32_t max_b_len, int32_t* d_score, int32_t* d_arange,
+                             int32_t* d_brange, void* stream) {
+  return compare_dev(e, d_codes, n_codes, 8, d_pairs, n, max_a_len, max_b_len, d_score, d_arange, d_brange, stream);
+}
+
+int ipuma_gpu_compare_device_packed(ipuma_engine* e, const uint8_t* d_packed, size_t n_codes, int32_t bits,
+                                    const ipuma_pair* d_pairs, int32_t n, int32_t max_a_len, int32_t max_b_len,
+                                    int32_t* d_score, int32_t* d_arange, int32_t* d_brange, void* stream) {
+  return compare_dev(e, d_packed, n_codes, bits, d_pairs, n, max_a_len, max_b_len, d_score, d_arange, d_brange,
+                     stream);
 }
 
 // Launches the alignment work of a wire buffer already on the device
@@ -1870,7 +1900,7 @@ static int launch_wire(ipuma_engine* e, DevBuf* pairs, const RunBufs& rb, cudaSt
   CUDA_TRY(cudaGetLastError());
   *launches += 1;
   // Pair offsets are absolute within the tiles' sequence words.
-  return run_batched(e, rb, s, reinterpret_cast<const uint8_t*>(d_in), (size_t)metaOffset * 4,
+  return run_batched(e, rb, s, reinterpret_cast<const uint8_t*>(d_in), (size_t)metaOffset * 4, 8,
                      pairs->as<PairDesc>(), (int)totalSlots,
                      maxA, maxB, d_res, d_res + totalSlots, d_res + 2 * totalSlots, launches);
 }

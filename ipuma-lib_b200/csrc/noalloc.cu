@@ -92,12 +92,12 @@ __global__ void __launch_bounds__(64) k_noalloc(SwConst sc, SimParam sim, const 
       }
       continue;
     }
-    const uint8_t* const a0[1] = {codes + d.a_off};
-    const uint8_t* const b0[1] = {codes + d.b_off};
+    const long long a0[1] = {d.a_off};
+    const long long b0[1] = {d.b_off};
     const int al[1] = {d.a_len}, bl[1] = {d.b_len};
     Best fw[1], rv[1];
     bool ovf[1];
-    align_pairs<T, K, 32>(sc, s_prof, s_simp, s_bring, a0, b0, al, bl, scr, rowsCap, fw, rv, ovf);
+    align_pairs<T, K, 32>(sc, s_prof, s_simp, s_bring, codes, a0, b0, al, bl, scr, rowsCap, fw, rv, ovf);
     if (lane == 0) write_result(sc, fw[0], rv[0], score, arange, brange, p);
   }
 }
@@ -166,6 +166,7 @@ extern "C" int ipuma_gpu_compare_noalloc(const ipuma_sw_config* sw, int32_t forw
   sc.M = m;
   sc.forwardOnly = forward_only ? 1 : 0;
   sc.s16Limit = 32767;
+  sc.bits = 8;  // one byte per residue
   // Warps that fit the static scratch at this row count (2 rows per B row).
   const long rowsCap = max_b_len;
   const long warpsFit = kScratchInt2 / (2 * rowsCap);

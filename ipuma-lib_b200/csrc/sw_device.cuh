@@ -63,6 +63,7 @@ struct SwConst {
   int forwardOnly;
   int s16Limit; // a pair whose score exceeds this is rerun in s32
   int maxSub;   // largest substitution score (strip bound of the hybrid pass)
+  int bits;     // bits per residue of the code array (8, or packed 2/4/5: code_at)
 };
 
 // Control of a hybrid pass (sw_pass with HYB): an s16x2 pass that stops
@@ -158,11 +159,29 @@ struct LaneS16x2 {
 // Pair views
 // -------------------------------------------------------------------------
 
-// One sequence pair as seen by a pass: A[j] = a[j * da], B[i] = b[i * db].
-// The reverse pass reads a[Aend..0] and b[Bend..0] with da = db = -1.
+// Residue codes in device memory.  bits = 8: one byte per residue.  bits =
+// 2, 4 or 5: a little-endian bit stream of fields, residue r in bits
+// [bits * r, bits * r + bits), read through the two 32-bit words around it
+// (one funnel shift); 2-bit fields hold code - 1 (A, T, C, G = codes 1..4),
+// wider ones the code itself.  A packed array starts 4-byte aligned and is
+// readable one word past the word of its last field.
+__device__ __forceinline__ int code_at(const uint8_t* base, long long idx, int bits) {
+  if (bits == 8) return base[idx];
+  const long long bit = idx * bits;
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(base) + (bit >> 5);
+  const uint32_t v = __funnelshift_r(__ldg(w), __ldg(w + 1), (uint32_t)bit & 31u);
+  const int x = (int)(v & ((1u << bits) - 1u));
+  return bits == 2 ? x + 1 : x;
+}
+
+// One sequence pair as seen by a pass: A[j] = residue a + j * da and
+// B[i] = residue b + i * db of the code array at `base` (bits per residue
+// in SwConst).  The reverse pass reads A[Aend..0] and B[Bend..0] with
+// da = db = -1.
 struct PassSeq {
-  const uint8_t* a;
-  const uint8_t* b;
+  const uint8_t* base;
+  long long a;
+  long long b;
   int alen;
   int blen;
   int da;
@@ -192,7 +211,7 @@ struct ProfileWords {
 };
 
 template <int K, int LANES>
-__device__ __forceinline__ void build_profile(uint8_t* prof, const int8_t* s_simp, int M,
+__device__ __forceinline__ void build_profile(uint8_t* prof, const int8_t* s_simp, int M, int bits,
                                               const PassSeq& ps, int col0, int lane) {
   // s_simp[a * (M + 1) + x] = sim[a][x] and SUB_PAD for x == M.
   constexpr int KP = ProfileWords<K>::KP;
@@ -201,7 +220,7 @@ __device__ __forceinline__ void build_profile(uint8_t* prof, const int8_t* s_sim
 #pragma unroll
   for (int c = 0; c < KP; ++c) {
     const int col = col0 + lane * K + c;
-    acode[c] = (c < K && col < ps.alen) ? (int)ps.a[(long)col * ps.da] : -1;
+    acode[c] = (c < K && col < ps.alen) ? code_at(ps.base, ps.a + (long long)col * ps.da, bits) : -1;
   }
   for (int x = 0; x <= M; ++x) {
 #pragma unroll
@@ -400,7 +419,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
     __syncwarp();
 #pragma unroll
     for (int h = 0; h < NP; ++h)
-      build_profile<K, LANES>(s_prof + h * profStride, s_simp, M, ps[h], col0, lane);
+      build_profile<K, LANES>(s_prof + h * profStride, s_simp, M, sc.bits, ps[h], col0, lane);
     __threadfence_block();
     __syncwarp();
 
@@ -431,7 +450,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
       uint32_t v = 0;
 #pragma unroll
       for (int h = 0; h < NP; ++h) {
-        const int x = (r < ps[h].blen) ? (int)ps[h].b[(long)r * ps[h].db] : M;
+        const int x = (r < ps[h].blen) ? code_at(ps[h].base, ps[h].b + (long long)r * ps[h].db, sc.bits) : M;
         v |= (uint32_t)x << (8 * h);
       }
       return v;

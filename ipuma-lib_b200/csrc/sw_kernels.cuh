@@ -118,9 +118,8 @@ __device__ __forceinline__ void load_simp(int8_t* s_simp, const int8_t* sim, con
 // the forward-only kernels keep their own register allocation).
 template <class T, int K, int LANES, int MODE = 0>
 __device__ __forceinline__ void align_pairs(const SwConst& sc, uint8_t* s_prof,
-                                            const int8_t* s_simp, uint16_t* s_bring,
-                                            const uint8_t* const (&a0)[T::NP],
-                                            const uint8_t* const (&b0)[T::NP],
+                                            const int8_t* s_simp, uint16_t* s_bring, const uint8_t* codes,
+                                            const long long (&a0)[T::NP], const long long (&b0)[T::NP],
                                             const int (&alen)[T::NP], const int (&blen)[T::NP],
                                             int2* scr, long rowsCap, Best (&fw)[T::NP],
                                             Best (&rv)[T::NP], bool (&ovf)[T::NP]) {
@@ -129,7 +128,7 @@ __device__ __forceinline__ void align_pairs(const SwConst& sc, uint8_t* s_prof,
 #pragma unroll
   for (int h = 0; h < NP; ++h) {
     const bool empty = alen[h] <= 0 || blen[h] <= 0;
-    ps[h] = PassSeq{a0[h], b0[h], empty ? 0 : alen[h], empty ? 0 : blen[h], 1, 1};
+    ps[h] = PassSeq{codes, a0[h], b0[h], empty ? 0 : alen[h], empty ? 0 : blen[h], 1, 1};
   }
 #pragma unroll
   for (int h = 0; h < NP; ++h) rv[h] = Best{0, 0, 0};
@@ -166,8 +165,8 @@ __device__ __forceinline__ void align_pairs(const SwConst& sc, uint8_t* s_prof,
       ovf[h] = (NP == 2) && (!done || fw[h].s > sc.s16Limit);
       const bool run = !ovf[h] && fw[h].s > 0;
       any |= run;
-      ps[h] = run ? PassSeq{a0[h] + fw[h].j, b0[h] + fw[h].i, fw[h].j + 1, fw[h].i + 1, -1, -1}
-                  : PassSeq{a0[h], b0[h], 0, 0, 1, 1};
+      ps[h] = run ? PassSeq{codes, a0[h] + fw[h].j, b0[h] + fw[h].i, fw[h].j + 1, fw[h].i + 1, -1, -1}
+                  : PassSeq{codes, a0[h], b0[h], 0, 0, 1, 1};
       stop.target[h] = run ? fw[h].s : 0;
     }
     stop.on = true;
@@ -206,15 +205,15 @@ __device__ __forceinline__ bool hybrid_pass(const SwConst& sc, uint8_t* s_prof, 
 // Forward (+ reverse) pass of the hybrid class; as align_pairs (MODE too).
 template <int K, int MODE = 0>
 __device__ __forceinline__ void align_pairs_hybrid(const SwConst& sc, uint8_t* s_prof, const int8_t* s_simp,
-                                                   uint16_t* s_bring, const uint8_t* const (&a0)[2],
-                                                   const uint8_t* const (&b0)[2], const int (&alen)[2],
-                                                   const int (&blen)[2], int2* scr, long rowsCap,
-                                                   Best (&fw)[2], Best (&rv)[2], bool (&ovf)[2]) {
+                                                   uint16_t* s_bring, const uint8_t* codes,
+                                                   const long long (&a0)[2], const long long (&b0)[2],
+                                                   const int (&alen)[2], const int (&blen)[2], int2* scr,
+                                                   long rowsCap, Best (&fw)[2], Best (&rv)[2], bool (&ovf)[2]) {
   PassSeq ps[2];
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     const bool empty = alen[h] <= 0 || blen[h] <= 0;
-    ps[h] = PassSeq{a0[h], b0[h], empty ? 0 : alen[h], empty ? 0 : blen[h], 1, 1};
+    ps[h] = PassSeq{codes, a0[h], b0[h], empty ? 0 : alen[h], empty ? 0 : blen[h], 1, 1};
   }
 #pragma unroll
   for (int h = 0; h < 2; ++h) rv[h] = Best{0, 0, 0};
@@ -245,8 +244,8 @@ __device__ __forceinline__ void align_pairs_hybrid(const SwConst& sc, uint8_t* s
     for (int h = 0; h < 2; ++h) {
       fw[h] = res[h];
       ovf[h] = !done;
-      ps[h] = fw[h].s > 0 ? PassSeq{a0[h] + fw[h].j, b0[h] + fw[h].i, fw[h].j + 1, fw[h].i + 1, -1, -1}
-                          : PassSeq{a0[h], b0[h], 0, 0, 1, 1};
+      ps[h] = fw[h].s > 0 ? PassSeq{codes, a0[h] + fw[h].j, b0[h] + fw[h].i, fw[h].j + 1, fw[h].i + 1, -1, -1}
+                          : PassSeq{codes, a0[h], b0[h], 0, 0, 1, 1};
     }
     if (!done) break;
   }
@@ -266,8 +265,13 @@ __device__ __forceinline__ void write_result(const SwConst& sc, const Best& fw, 
 // Persistent batched kernel.  `list` holds pair ids in processing order;
 // a warp takes items of 32 / LANES * NP consecutive entries (ids < 0 are
 // padding), lane group g aligning entries [g * NP, g * NP + NP).
+// Register budget: the forward-only kernels get at most 128 registers (4
+// blocks of 128 threads per SM when the profile is small); the kernels
+// with a reverse pass or a run-time mode (FWD false, or the hybrid class)
+// up to 170 (3 blocks per SM, which their shared memory allows anyway), as
+// at 128 they spilled.
 template <class T, int K, int LANES, bool HYB = false, bool FWD = false>
-__global__ void __launch_bounds__(128) k_batched(SwConst sc, const int8_t* __restrict__ sim,
+__global__ void __launch_bounds__(128, (FWD && !HYB) ? 4 : 3) k_batched(SwConst sc, const int8_t* __restrict__ sim,
                                                  const uint8_t* __restrict__ codes,
                                                  const PairDesc* __restrict__ pairs,
                                                  const int* __restrict__ list,
@@ -312,8 +316,7 @@ __global__ void __launch_bounds__(128) k_batched(SwConst sc, const int8_t* __res
     item = __shfl_sync(FULL, item, 0);
     if (item >= items) break;
     int pid[NP], alen[NP], blen[NP];
-    const uint8_t* a0[NP];
-    const uint8_t* b0[NP];
+    long long a0[NP], b0[NP];
     bool tooLong = false;
 #pragma unroll
     for (int h = 0; h < NP; ++h) {
@@ -322,8 +325,8 @@ __global__ void __launch_bounds__(128) k_batched(SwConst sc, const int8_t* __res
       PairDesc d = (pid[h] >= 0) ? pairs[pid[h]] : PairDesc{0, 0, 0, 0};
       alen[h] = d.a_len;
       blen[h] = d.b_len;
-      a0[h] = codes + d.a_off;
-      b0[h] = codes + d.b_off;
+      a0[h] = d.a_off;
+      b0[h] = d.b_off;
       tooLong |= d.b_len > rowsCap;
     }
     if (__any_sync(FULL, tooLong)) {
@@ -337,13 +340,15 @@ __global__ void __launch_bounds__(128) k_batched(SwConst sc, const int8_t* __res
       static_assert(NP == 2 && LANES == 32, "the hybrid class pairs two s16x2 pairs per 32-lane warp");
       // Mode chosen at run time: specialising the hybrid class made its
       // forward-only kernel spill and slowed the heavy-tailed protein batch.
-      align_pairs_hybrid<K, 0>(sc, s_prof, s_simp, s_bring, a0, b0, alen, blen, scr, rowsCap, fw, rv, ovf);
+      align_pairs_hybrid<K, 0>(sc, s_prof, s_simp, s_bring, codes, a0, b0, alen, blen, scr, rowsCap, fw, rv,
+                               ovf);
     } else {
       // s16x2 classes: one kernel per mode (fewer registers, no spills for
       // forward-only; the early reverse stop for full alignments); the s32
       // class keeps the run-time choice for the same reason as the hybrid.
       constexpr int MODE = (T::NP == 1) ? 0 : (FWD ? 1 : 2);
-      align_pairs<T, K, LANES, MODE>(sc, s_prof, s_simp, s_bring, a0, b0, alen, blen, scr, rowsCap, fw, rv, ovf);
+      align_pairs<T, K, LANES, MODE>(sc, s_prof, s_simp, s_bring, codes, a0, b0, alen, blen, scr, rowsCap, fw, rv,
+                                     ovf);
     }
     if (glane == 0) {
 #pragma unroll
@@ -391,21 +396,22 @@ __global__ void __launch_bounds__(128) k_plain(SwConst sc, const int8_t* __restr
   const long nw = (long)gridDim.x * warps;
   int2* scr = scratch + gw * 2 * rowsCap;
   const int* meta = inputs + metaOffset;
+  // Byte codes: residue offsets count bytes from the start of the buffer.
+  const uint8_t* bytes = reinterpret_cast<const uint8_t*>(inputs);
   for (long g = gw; g < totalSlots; g += nw) {
-    const long tile = g / maxBatches;
-    const uint8_t* seqs = reinterpret_cast<const uint8_t*>(inputs + tile * seqWordsPerTile);
+    const long long tileBase = (long long)(g / maxBatches) * seqWordsPerTile * 4;
     const int alen = meta[4 * g + 0], aoff = meta[4 * g + 1];
     const int blen = meta[4 * g + 2], boff = meta[4 * g + 3];
     if (blen > rowsCap) {
       if (lane == 0) atomicCAS(&st->error, 0, ERR_SCRATCH);
       continue;
     }
-    const uint8_t* const a0[1] = {seqs + aoff};
-    const uint8_t* const b0[1] = {seqs + boff};
+    const long long a0[1] = {tileBase + aoff};
+    const long long b0[1] = {tileBase + boff};
     const int al[1] = {alen}, bl[1] = {blen};
     Best fw[1], rv[1];
     bool ovf[1];
-    align_pairs<T, K, 32>(sc, s_prof, s_simp, s_bring, a0, b0, al, bl, scr, rowsCap, fw, rv, ovf);
+    align_pairs<T, K, 32>(sc, s_prof, s_simp, s_bring, bytes, a0, b0, al, bl, scr, rowsCap, fw, rv, ovf);
     if (lane == 0)
       write_result(sc, fw[0], rv[0], results, results + totalSlots, results + 2L * totalSlots, g);
   }
@@ -439,20 +445,20 @@ __global__ void __launch_bounds__(128) k_plain16(SwConst sc, const int8_t* __res
   const long nw = (long)gridDim.x * warps;
   int2* scr = scratch + gw * 2 * rowsCap;
   const int* meta = inputs + metaOffset;
+  const uint8_t* bytes = reinterpret_cast<const uint8_t*>(inputs);
   for (long g0 = 2 * gw; g0 < totalSlots; g0 += 2 * nw) {
-    const uint8_t* a0[2];
-    const uint8_t* b0[2];
+    long long a0[2], b0[2];
     int al[2], bl[2];
     bool tooLong = false;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const long g = g0 + h;
       const bool have = g < totalSlots;
-      const uint8_t* seqs = reinterpret_cast<const uint8_t*>(inputs + (have ? g / maxBatches : 0) * seqWordsPerTile);
+      const long long tileBase = have ? (long long)(g / maxBatches) * seqWordsPerTile * 4 : 0;
       al[h] = have ? meta[4 * g + 0] : 0;
       bl[h] = have ? meta[4 * g + 2] : 0;
-      a0[h] = seqs + (have ? meta[4 * g + 1] : 0);
-      b0[h] = seqs + (have ? meta[4 * g + 3] : 0);
+      a0[h] = tileBase + (have ? meta[4 * g + 1] : 0);
+      b0[h] = tileBase + (have ? meta[4 * g + 3] : 0);
       tooLong |= bl[h] > rowsCap;
     }
     if (tooLong) {  // warp-uniform: every lane read the same Meta words
@@ -461,17 +467,18 @@ __global__ void __launch_bounds__(128) k_plain16(SwConst sc, const int8_t* __res
     }
     Best fw[2], rv[2];
     bool ovf[2];
-    align_pairs<LaneS16x2, K, 32>(sc, s_prof, s_simp, s_bring, a0, b0, al, bl, scr, rowsCap, fw, rv, ovf);
+    align_pairs<LaneS16x2, K, 32>(sc, s_prof, s_simp, s_bring, bytes, a0, b0, al, bl, scr, rowsCap, fw, rv, ovf);
 #pragma unroll 1
     for (int h = 0; h < 2; ++h) {
       if (g0 + h >= totalSlots) break;
       if (ovf[h]) {  // uniform: the score is the 32-lane group's reduction
-        const uint8_t* const a1[1] = {a0[h]};
-        const uint8_t* const b1[1] = {b0[h]};
+        const long long a1[1] = {a0[h]};
+        const long long b1[1] = {b0[h]};
         const int al1[1] = {al[h]}, bl1[1] = {bl[h]};
         Best f1[1], r1[1];
         bool o1[1];
-        align_pairs<LaneS32, K, 32>(sc, s_prof, s_simp, s_bring, a1, b1, al1, bl1, scr, rowsCap, f1, r1, o1);
+        align_pairs<LaneS32, K, 32>(sc, s_prof, s_simp, s_bring, bytes, a1, b1, al1, bl1, scr, rowsCap, f1, r1,
+                                    o1);
         fw[h] = f1[0];
         rv[h] = r1[0];
       }
@@ -484,20 +491,21 @@ __global__ void __launch_bounds__(128) k_plain16(SwConst sc, const int8_t* __res
 // Exact per-thread kernel: one thread per pair, the recurrence written out
 // cell by cell in int32 (codelet_batch_affine.cpp:65-115) with C and F rows
 // in global scratch (2 * maxA int per thread).  Covers every scoring
-// configuration.  Pairs come either from a pair list or from the wire
-// buffer (inputs != nullptr).
-static __device__ void exact_pass(const uint8_t* a0, int alen, int da, const uint8_t* b0, int blen, int db,
-                           const int8_t* sim, int M, int gI, int gE, int* C, int* F, Best& out) {
+// configuration.  A[j] = residue a0 + j * da, B[i] = residue b0 + i * db of
+// `codes` (sc.bits per residue).
+static __device__ void exact_pass(const uint8_t* codes, int bits, long long a0, int alen, int da, long long b0,
+                                  int blen, int db, const int8_t* sim, int M, int gI, int gE, int* C, int* F,
+                                  Best& out) {
   int s = 0, bi = 0, bj = 0;
   for (int j = 0; j < alen; ++j) {
     C[j] = 0;
     F[j] = 0;
   }
   for (int i = 0; i < blen; ++i) {
-    const int bc = b0[(long)i * db];
+    const int bc = code_at(codes, b0 + (long long)i * db, bits);
     int e = gI, hl = 0, diag = 0;
     for (int j = 0; j < alen; ++j) {
-      const int ac = a0[(long)j * da];
+      const int ac = code_at(codes, a0 + (long long)j * da, bits);
       e = max(hl + gI + gE, e + gE);
       const int f = max(C[j] + gI + gE, F[j] + gE);
       F[j] = f;
@@ -516,43 +524,29 @@ static __device__ void exact_pass(const uint8_t* a0, int alen, int da, const uin
   out = Best{s, bi, bj};
 }
 
-// Pairs from the list are checked with pair_state against n_codes and the
-// stated maxima (maxA, maxB); wire-buffer slots were validated before the
-// launch.
+// Pairs are checked with pair_state against n_codes and the stated maxima
+// (maxA, maxB) before any code is read.
 static __global__ void k_exact(SwConst sc, const int8_t* __restrict__ sim, const uint8_t* __restrict__ codes,
-                        long long n_codes, const PairDesc* __restrict__ pairs, int n,
-                        const int* __restrict__ inputs, long seqWordsPerTile, long metaOffset, int maxBatches,
-                        int* cf_scratch, long maxA, int maxB, int* score, int* arange, int* brange,
-                        DevStatus* st) {
+                        long long n_codes, const PairDesc* __restrict__ pairs, int n, int* cf_scratch, long maxA,
+                        int maxB, int* score, int* arange, int* brange, DevStatus* st) {
   const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long nt = (long)gridDim.x * blockDim.x;
   int* C = cf_scratch + tid * 2 * maxA;
   int* F = C + maxA;
   for (long p = tid; p < n; p += nt) {
-    const uint8_t *a, *b;
-    int alen, blen;
-    if (inputs) {
-      const long tile = p / maxBatches;
-      const uint8_t* seqs = reinterpret_cast<const uint8_t*>(inputs + tile * seqWordsPerTile);
-      const int* m = inputs + metaOffset + 4 * p;
-      alen = m[0];
-      a = seqs + m[1];
-      blen = m[2];
-      b = seqs + m[3];
-    } else {
-      const PairDesc d = pairs[p];
-      const int state = pair_state(d, n_codes, (int)maxA, maxB);
-      report_pair(state, st);
-      alen = state == PAIR_OK ? d.a_len : 0;
-      blen = state == PAIR_OK ? d.b_len : 0;
-      a = codes + (state == PAIR_OK ? d.a_off : 0);
-      b = codes + (state == PAIR_OK ? d.b_off : 0);
-    }
+    const PairDesc d = pairs[p];
+    const int state = pair_state(d, n_codes, (int)maxA, maxB);
+    report_pair(state, st);
+    const int alen = state == PAIR_OK ? d.a_len : 0;
+    const int blen = state == PAIR_OK ? d.b_len : 0;
+    const long long a = state == PAIR_OK ? d.a_off : 0;
+    const long long b = state == PAIR_OK ? d.b_off : 0;
     Best fw{0, 0, 0}, rv{0, 0, 0};
     if (alen > 0 && blen > 0 && alen <= maxA) {
-      exact_pass(a, alen, 1, b, blen, 1, sim, sc.M, sc.gI, sc.gE, C, F, fw);
+      exact_pass(codes, sc.bits, a, alen, 1, b, blen, 1, sim, sc.M, sc.gI, sc.gE, C, F, fw);
       if (!sc.forwardOnly)
-        exact_pass(a + fw.j, fw.j + 1, -1, b + fw.i, fw.i + 1, -1, sim, sc.M, sc.gI, sc.gE, C, F, rv);
+        exact_pass(codes, sc.bits, a + fw.j, fw.j + 1, -1, b + fw.i, fw.i + 1, -1, sim, sc.M, sc.gI, sc.gE, C, F,
+                   rv);
     }
     write_result(sc, fw, rv, score, arange, brange, p);
   }
@@ -608,6 +602,7 @@ struct BinParams {
   int n_s16_classes;
   int max_a, max_b;        // stated maxima (violations set ERR_LENGTH)
   long long n_codes;       // residues in the code array (pairs past it set ERR_RANGE)
+  int bits;                // bits per residue of the code array (code_at)
   int M;                   // alphabet size of `sim`
   int force_s32;           // 1: every pair goes to the s32 class
   // Per-thread class (k_thread): one thread per two pairs, so a pair's time
@@ -643,10 +638,11 @@ static_assert(THR_NSB * THR_NRB <= NBUCKET, "per-thread buckets");
 // Best ungapped score along the main diagonal (a lower bound of the local
 // alignment score): pairs that surely pass the s16 limit go straight to
 // s32 lanes instead of giving up half way in s16x2.
-static __device__ int diagonal_bound(const uint8_t* a, const uint8_t* b, int n, const int8_t* sim, int M) {
+static __device__ int diagonal_bound(const uint8_t* codes, int bits, long long a, long long b, int n,
+                                     const int8_t* sim, int M) {
   int run = 0, best = 0;
   for (int k = 0; k < n; ++k) {
-    run = max(run + (int)sim[a[k] * M + b[k]], 0);
+    run = max(run + (int)sim[code_at(codes, a + k, bits) * M + code_at(codes, b + k, bits)], 0);
     best = max(best, run);
   }
   return best;
@@ -746,8 +742,7 @@ static __global__ void k_bin_count(BinParams bp, const uint8_t* __restrict__ cod
     }
     bool s32 = false;
     if (!bp.force_s32 && min(d.a_len, d.b_len) > bp.s16_max_len)
-      s32 = diagonal_bound(codes + d.a_off, codes + d.b_off, min(d.a_len, d.b_len), sim, bp.M) >
-            bp.s16_limit;
+      s32 = diagonal_bound(codes, bp.bits, d.a_off, d.b_off, min(d.a_len, d.b_len), sim, bp.M) > bp.s16_limit;
     s32_flag[p] = s32 ? 1 : 0;
     float cost = 0.f;
     const int key = pair_key(bp, d.a_len, d.b_len, s32, thread_cap(bp), &cost);
@@ -879,64 +874,6 @@ static __global__ void k_wire_check(const int* __restrict__ inputs, long metaOff
     atomicMax(&info[0], al);
     atomicMax(&info[1], bl);
     atomicAdd(cells, (unsigned long long)al * (unsigned long long)bl);
-  }
-}
-
-// Expands 4-bit residue codes (two per byte, the lower-indexed residue in
-// the low nibble) of residues [lo, hi) into one byte per residue.  Writes
-// exactly that range: other ranges of `codes` may be read by kernels on
-// other streams meanwhile.  Reads whole 8-byte words of `packed` around the
-// range; the caller pads the packed buffer to cover them.
-static __global__ void k_unpack4(const uint8_t* __restrict__ packed, size_t lo, size_t hi,
-                                 uint8_t* __restrict__ codes) {
-  const size_t stride = (size_t)16 * gridDim.x * blockDim.x;
-  for (size_t blk = (lo & ~(size_t)15) + (size_t)16 * (blockIdx.x * blockDim.x + threadIdx.x); blk < hi;
-       blk += stride) {
-    const uint2 w = *reinterpret_cast<const uint2*>(packed + blk / 2);
-    // 16 packed bits (4 residues) -> 4 bytes.
-    auto spread = [](uint32_t v) -> uint32_t {
-      return (v & 0x000Fu) | ((v & 0x00F0u) << 4) | ((v & 0x0F00u) << 8) | ((v & 0xF000u) << 12);
-    };
-    const uint4 out = make_uint4(spread(w.x & 0xFFFFu), spread(w.x >> 16), spread(w.y & 0xFFFFu), spread(w.y >> 16));
-    if (blk >= lo && blk + 16 <= hi) {
-      *reinterpret_cast<uint4*>(codes + blk) = out;
-    } else {
-      const uint32_t o[4] = {out.x, out.y, out.z, out.w};
-#pragma unroll
-      for (int b = 0; b < 16; ++b) {
-        const size_t p = blk + b;
-        if (p >= lo && p < hi) codes[p] = (uint8_t)(o[b >> 2] >> (8 * (b & 3)));
-      }
-    }
-  }
-}
-
-// Expands 2-bit residue codes (four per byte, residue 4k+q in bits 2q and
-// 2q+1 of byte k, value = code - 1: A, T, C, G = codes 1..4) of residues
-// [lo, hi) into one byte per residue; as k_unpack4, it writes exactly that
-// range and reads whole 4-byte words of `packed` around it.
-static __global__ void k_unpack2(const uint8_t* __restrict__ packed, size_t lo, size_t hi,
-                                 uint8_t* __restrict__ codes) {
-  const size_t stride = (size_t)16 * gridDim.x * blockDim.x;
-  for (size_t blk = (lo & ~(size_t)15) + (size_t)16 * (blockIdx.x * blockDim.x + threadIdx.x); blk < hi;
-       blk += stride) {
-    const uint32_t w = *reinterpret_cast<const uint32_t*>(packed + blk / 4);
-    // 8 packed bits (4 residues) -> 4 bytes, plus 1 per byte.
-    auto spread = [](uint32_t v) -> uint32_t {
-      return ((v & 0x03u) | ((v & 0x0Cu) << 6) | ((v & 0x30u) << 12) | ((v & 0xC0u) << 18)) + 0x01010101u;
-    };
-    const uint4 out = make_uint4(spread(w & 0xFFu), spread((w >> 8) & 0xFFu), spread((w >> 16) & 0xFFu),
-                                 spread(w >> 24));
-    if (blk >= lo && blk + 16 <= hi) {
-      *reinterpret_cast<uint4*>(codes + blk) = out;
-    } else {
-      const uint32_t o[4] = {out.x, out.y, out.z, out.w};
-#pragma unroll
-      for (int b = 0; b < 16; ++b) {
-        const size_t p = blk + b;
-        if (p >= lo && p < hi) codes[p] = (uint8_t)(o[b >> 2] >> (8 * (b & 3)));
-      }
-    }
   }
 }
 

@@ -1,7 +1,8 @@
 // sw_thread.cuh -- the per-thread kernel class k_thread<K>: one thread
 // aligns two pairs in s16x2 halves (pair P low, pair Q high) over the whole
 // matrix, column strip by column strip, with no communication between
-// threads.
+// threads.  It reads one byte per residue (the engine never launches it on
+// packed codes).
 //
 // Same recurrence, frames and tie-break as the wavefront kernels
 // (sw_device.cuh, after src/codelets/codelet_batch_affine.cpp:65-85): per
@@ -51,7 +52,7 @@ __device__ __forceinline__ void thread_profile(uint8_t* s_warp, const int8_t* s_
 #pragma unroll
     for (int c = 0; c < K; ++c) {
       const int col = col0 + c;
-      acode[c] = (col < ps[h].alen) ? (int)ps[h].a[(long)col * ps[h].da] * (M + 1) : -1;
+      acode[c] = (col < ps[h].alen) ? (int)ps[h].base[ps[h].a + (long long)col * ps[h].da] * (M + 1) : -1;
     }
     uint8_t* dst = s_warp + (h * 32 + t) * K;
     for (int x = 0; x <= M; ++x) {
@@ -120,7 +121,8 @@ __device__ __forceinline__ void thread_pass(const SwConst& sc, uint8_t* s_warp, 
   int wstep[2], wshift[2], wfirst[2];
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
-    const uintptr_t p = (ps[h].db > 0) ? (uintptr_t)ps[h].b : (uintptr_t)ps[h].b - 3;
+    const uintptr_t bp = (uintptr_t)(ps[h].base + ps[h].b);
+    const uintptr_t p = (ps[h].db > 0) ? bp : bp - 3;
     wshift[h] = 8 * (int)(p & 3);
     wbase[h] = reinterpret_cast<const uint32_t*>(p & ~(uintptr_t)3) + (ps[h].db > 0 ? 0 : 1);
     wstep[h] = ps[h].db > 0 ? 1 : -1;
@@ -310,7 +312,7 @@ __global__ void __launch_bounds__(128, 3) k_thread(SwConst sc, const int8_t* __r
       pid[h] = (k < n) ? list[k] : -1;
       const PairDesc d = (pid[h] >= 0) ? pairs[pid[h]] : PairDesc{0, 0, 0, 0};
       const bool empty = d.a_len <= 0 || d.b_len <= 0;
-      ps[h] = PassSeq{codes + d.a_off, codes + d.b_off, empty ? 0 : d.a_len, empty ? 0 : d.b_len, 1, 1};
+      ps[h] = PassSeq{codes, d.a_off, d.b_off, empty ? 0 : d.a_len, empty ? 0 : d.b_len, 1, 1};
     }
     // Only a thread with more than one strip touches the boundary scratch,
     // for all of its rows.
@@ -330,8 +332,8 @@ __global__ void __launch_bounds__(128, 3) k_thread(SwConst sc, const int8_t* __r
       for (int h = 0; h < 2; ++h) {
         const bool run = !over[h] && fw[h].s > 0;
         any |= run;
-        rs[h] = run ? PassSeq{ps[h].a + fw[h].j, ps[h].b + fw[h].i, fw[h].j + 1, fw[h].i + 1, -1, -1}
-                    : PassSeq{ps[h].a, ps[h].b, 0, 0, 1, 1};
+        rs[h] = run ? PassSeq{codes, ps[h].a + fw[h].j, ps[h].b + fw[h].i, fw[h].j + 1, fw[h].i + 1, -1, -1}
+                    : PassSeq{codes, ps[h].a, ps[h].b, 0, 0, 1, 1};
       }
       bool dummy[2];
       if (any) thread_pass<K>(sc, s_warp, s_simp, rs, scr, stride, t, rv, dummy);

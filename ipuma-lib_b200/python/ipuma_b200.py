@@ -42,7 +42,7 @@ EXPORTS = [
     "ipuma_server_poll", "ipuma_server_wait", "ipuma_server_get_stats", "ipuma_server_close",
     "ipuma_server_destroy", "ipuma_server_add_sequences", "ipuma_server_submit_resident",
     "ipuma_gpu_reserve", "ipuma_gpu_join_stats", "ipuma_host_alloc", "ipuma_host_free",
-    "ipuma_gpu_compare_packed", "ipuma_pack_codes",
+    "ipuma_gpu_compare_packed", "ipuma_pack_codes", "ipuma_gpu_compare_device_packed",
 ]
 
 KERNEL_NAMES = {0: "k_batched<s32,L32,K16>", 1: "k_batched<s16x2,L16,K4>",
@@ -143,6 +143,7 @@ def lib():
         L.ipuma_gpu_compare_packed.argtypes = [vp, vp, sz, i32, vp, i32, vp, vp, vp]
         L.ipuma_pack_codes.argtypes = [vp, sz, i32, vp]
         L.ipuma_gpu_compare_device.argtypes = [vp, vp, sz, vp, i32, i32, i32, vp, vp, vp, vp]
+        L.ipuma_gpu_compare_device_packed.argtypes = [vp, vp, sz, i32, vp, i32, i32, i32, vp, vp, vp, vp]
         L.ipuma_gpu_last_stats.argtypes = [vp, ctypes.POINTER(Stats)]
         L.ipuma_gpu_run_buffer_device.argtypes = [vp, vp, sz, vp, sz, vp]
         L.ipuma_measure_int_peak.argtypes = [i32, ctypes.POINTER(ctypes.c_double)]
@@ -204,14 +205,25 @@ def encode(datatype: str, s: str) -> np.ndarray:
     return out
 
 
+def packed_bytes(n_codes: int, bits: int) -> int:
+    """Bytes of n_codes residues packed at `bits` per residue."""
+    return (n_codes * bits + 7) // 8
+
+
+def device_packed_bytes(n_codes: int, bits: int) -> int:
+    """Bytes a device copy of packed codes must hold for
+    compare_device_packed: rounded up to a word, plus one word."""
+    return ((packed_bytes(n_codes, bits) + 3) // 4) * 4 + 4
+
+
 def pack_codes(codes: np.ndarray, bits: int = 4, out: np.ndarray | None = None) -> np.ndarray:
-    """Packs codes for compare_packed (ipuma_pack_codes): bits = 4 (codes
-    < 16, two per byte, low nibble first) or 2 (A, T, C, G = codes 1..4,
-    four per byte as code - 1).  `out` may be a preallocated (e.g. pinned)
-    uint8 array of ceil(n * bits / 8) bytes."""
+    """Packs codes for the packed compare calls (ipuma_pack_codes): a
+    little-endian bit stream, residue r in bits [bits*r, bits*r + bits);
+    bits = 5 (codes < 32), 4 (codes < 16) or 2 (A, T, C, G = codes 1..4 as
+    code - 1).  `out` may be a preallocated (e.g. pinned) uint8 array of at
+    least ceil(n * bits / 8) bytes."""
     codes = np.ascontiguousarray(codes, dtype=np.uint8)
-    per = 8 // bits
-    nb = (codes.size + per - 1) // per
+    nb = packed_bytes(codes.size, bits)
     if out is None:
         out = np.zeros(nb, dtype=np.uint8)
     assert out.dtype == np.uint8 and out.size >= nb and out.flags.c_contiguous
@@ -338,6 +350,16 @@ class Engine:
                                               ctypes.c_void_p(d_pairs), n, max_a, max_b,
                                               ctypes.c_void_p(d_score), ctypes.c_void_p(d_ar),
                                               ctypes.c_void_p(d_br), ctypes.c_void_p(stream)))
+
+    def compare_device_packed(self, d_packed: int, n_codes: int, bits: int, d_pairs: int, n: int,
+                              max_a: int, max_b: int, d_score: int, d_ar: int, d_br: int,
+                              stream: int = 0):
+        """compare_device on packed codes the kernels read directly
+        (device_packed_bytes(n_codes, bits) bytes at d_packed)."""
+        _check(lib().ipuma_gpu_compare_device_packed(self.h, ctypes.c_void_p(d_packed), n_codes, bits,
+                                                     ctypes.c_void_p(d_pairs), n, max_a, max_b,
+                                                     ctypes.c_void_p(d_score), ctypes.c_void_p(d_ar),
+                                                     ctypes.c_void_p(d_br), ctypes.c_void_p(stream)))
 
     def run_buffer(self, inputs: np.ndarray) -> np.ndarray:
         inputs = np.ascontiguousarray(inputs, dtype=np.int32)

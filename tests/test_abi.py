@@ -116,3 +116,41 @@ def test_pack_codes2_takes_only_acgt(bad):
     assert ei.value.code == ib.ERR_BAD_SEQUENCE and "777" in str(ei.value)
     with pytest.raises(ib.IpumaError):
         ib.pack_codes(codes, 3)
+
+
+def _bitstream(values, bits):
+    """Little-endian bit stream of `bits`-bit fields (the restatement the
+    packer is checked against): field r in bits [bits*r, bits*r + bits)."""
+    n = values.size
+    nbytes = (n * bits + 7) // 8
+    bitpos = np.arange(n, dtype=np.int64)[:, None] * bits + np.arange(bits)[None, :]
+    bitval = (values.astype(np.int64)[:, None] >> np.arange(bits)[None, :]) & 1
+    flat = np.zeros(nbytes * 8, np.uint8)
+    flat[bitpos.ravel()] = bitval.ravel()
+    return np.packbits(flat.reshape(-1, 8)[:, ::-1], axis=1).ravel()
+
+
+@pytest.mark.parametrize("n", [0, 1, 7, 8, 9, 63, 64, 100_003, (1 << 23) + 5])
+def test_pack_codes5_layout(n):
+    """Amino-acid codes 0..24 as a little-endian bit stream of 5-bit fields;
+    the last byte's missing bits are 0 (large inputs pack on several
+    threads)."""
+    codes = np.random.default_rng(n).integers(0, 25, n).astype(np.uint8)
+    packed = ib.pack_codes(codes, 5)
+    assert packed.size == (5 * n + 7) // 8
+    np.testing.assert_array_equal(packed, _bitstream(codes, 5))
+
+
+@pytest.mark.parametrize("bits", [2, 4])
+def test_pack_codes_2_and_4_are_the_same_bit_stream(bits):
+    codes = np.random.default_rng(bits).integers(1, 5, 1001).astype(np.uint8)
+    packed = ib.pack_codes(codes, bits)
+    np.testing.assert_array_equal(packed, _bitstream(codes - 1 if bits == 2 else codes, bits))
+
+
+def test_pack_codes5_rejects_codes_above_31():
+    codes = np.full(500, 3, np.uint8)
+    codes[321] = 32
+    with pytest.raises(ib.IpumaError) as ei:
+        ib.pack_codes(codes, 5)
+    assert ei.value.code == ib.ERR_BAD_SEQUENCE and "321" in str(ei.value)

@@ -1,9 +1,11 @@
-"""GPU parity of ipuma_gpu_compare_packed: codes packed two (4-bit) or
-four (2-bit, A/C/G/T) per byte are uploaded (whole, or per chunk of pairs)
-and expanded on the device; every result must equal ipuma_gpu_compare on
-the byte codes and the oracle, for sequences starting inside a byte,
-ranges ending mid-byte, empty pairs, and chunks whose code ranges
-overlap."""
+"""GPU parity of the packed-code calls: codes packed as a bit stream of 2-bit
+(A/C/G/T), 4-bit or 5-bit (amino acid) fields are uploaded (whole, or per
+chunk of pairs) and read packed by the kernels; device-resident packed
+codes go straight to ipuma_gpu_compare_device_packed.  Every result must
+equal the byte-code call and the oracle, for sequences starting inside a
+byte, ranges ending mid-byte, empty pairs, chunks whose code ranges
+overlap, reverse passes, and every kernel class (wavefront classes, the
+hybrid and s32 classes with their diagonal bound, the exact kernel)."""
 import numpy as np
 import pytest
 
@@ -112,6 +114,7 @@ def test_packed_automatic_chunks_into_pinned_buffers(bits):
 
 
 def test_packed_needs_a_small_alphabet():
+    # 25 amino-acid codes need 5 bits: 4, 2 (and 3) are refused.
     wl = workloads.protein(n=100, seed=74)
     pairs = ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len)
     with _engine(wl, True) as e:
@@ -120,3 +123,104 @@ def test_packed_needs_a_small_alphabet():
                 e.compare_packed(np.zeros(wl.codes.size, np.uint8), wl.codes.size, pairs, bits=bits)
             assert ei.value.code == ib.ERR_INVALID_ARG
         _same(e.compare(wl.codes, pairs), _oracle(wl, wl.codes, pairs, True), "after rejection")
+
+
+@pytest.mark.parametrize("forward_only", [True, False])
+def test_protein_5bit_host_call_equals_bytes_and_oracle(forward_only):
+    wl = workloads.protein(n=3_000, seed=75)
+    codes = np.concatenate([[7], wl.codes, [1, 2, 3]]).astype(np.uint8)
+    pairs = ib.make_pairs(wl.a_off + 1, wl.a_len, wl.b_off + 1, wl.b_len)
+    pairs["a_len"][17] = 0
+    packed = ib.pack_codes(codes, 5)
+    want = _oracle(wl, codes, pairs, forward_only)
+    for chunks in (1, 3):
+        with _engine(wl, forward_only, chunks=chunks) as e:
+            got = e.compare_packed(packed, codes.size, pairs, bits=5)
+        _same(got, want, "5-bit chunks=%d" % chunks)
+
+
+def _device_packed(wl, codes, pairs, bits, forward_only, graphs=0, **opts):
+    """compare_device_packed on a device copy of the packed codes (padded as
+    the call requires) and compare_device on the byte codes."""
+    torch = pytest.importorskip("torch")
+    packed = ib.pack_codes(codes, bits)
+    buf = np.zeros(ib.device_packed_bytes(codes.size, bits), np.uint8)
+    buf[:packed.size] = packed
+    d_packed = torch.from_numpy(buf).cuda()
+    d_bytes = torch.from_numpy(codes).cuda()
+    d_pairs = torch.from_numpy(pairs.view(np.uint8)).cuda()
+    n = pairs.shape[0]
+    outs = []
+    with _engine(wl, forward_only, graphs=graphs, **opts) as e:
+        for call in ("packed", "bytes"):
+            out = torch.full((3, n), -7, dtype=torch.int32, device="cuda")
+            args = (pairs.shape[0], int(pairs["a_len"].max()), int(pairs["b_len"].max()),
+                    out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr())
+            if call == "packed":
+                e.compare_device_packed(d_packed.data_ptr(), codes.size, bits, d_pairs.data_ptr(), *args)
+            else:
+                e.compare_device(d_bytes.data_ptr(), codes.size, d_pairs.data_ptr(), *args)
+            torch.cuda.synchronize()
+            outs.append(tuple(out.cpu().numpy()))
+    return outs
+
+
+@pytest.mark.parametrize("bits,kind", [(2, "dna"), (4, "dna"), (5, "protein")])
+@pytest.mark.parametrize("forward_only", [True, False])
+def test_device_packed_equals_bytes_and_oracle(bits, kind, forward_only):
+    wl = workloads.dna_batched(n=6_000, seed=76) if kind == "dna" else workloads.protein(n=2_000, seed=76)
+    codes, pairs = (_odd_layout(wl) if kind == "dna" else
+                    (np.concatenate([[5], wl.codes]).astype(np.uint8),
+                     ib.make_pairs(wl.a_off + 1, wl.a_len, wl.b_off + 1, wl.b_len)))
+    pairs["b_len"][3] = 0
+    want = _oracle(wl, codes, pairs, forward_only)
+    for graphs in (0, 1):
+        got_p, got_b = _device_packed(wl, codes, pairs, bits, forward_only, graphs=graphs)
+        _same(got_p, want, "device %d-bit graphs=%d" % (bits, graphs))
+        _same(got_b, want, "device bytes graphs=%d" % graphs)
+
+
+def test_device_packed_high_scores_hybrid_and_s32():
+    # Near-identical long protein pairs: the diagonal bound (read packed)
+    # sends them to the hybrid class, which switches to s32 strips; with
+    # option hybrid 0 they run in the s32 class.
+    wl = workloads.protein_mixed(n=1_200, seed=77, long_identical_frac=0.01)
+    assert (wl.a_len >= 7000).sum() >= 8
+    pairs = ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len)
+    want = _oracle(wl, wl.codes, pairs, True)
+    assert want[0].max() > 32767
+    for hybrid in (1, 0):
+        got_p, _ = _device_packed(wl, wl.codes, pairs, 5, True, hybrid=hybrid)
+        _same(got_p, want, "5-bit high scores hybrid=%d" % hybrid)
+
+
+def test_device_packed_exact_kernel_for_unusual_gaps():
+    # gap extend > 0 runs the exact per-thread kernel, which reads packed
+    # codes through the same accessor.
+    wl = workloads.dna_batched(n=400, seed=78)
+    wl.gap_init, wl.gap_extend = -1, 1
+    pairs = ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len)
+    for fwd in (True, False):
+        got_p, got_b = _device_packed(wl, wl.codes, pairs, 2, fwd)
+        want = _oracle(wl, wl.codes, pairs, fwd)
+        _same(got_p, want, "exact packed fwd=%s" % fwd)
+        _same(got_b, want, "exact bytes fwd=%s" % fwd)
+
+
+def test_device_packed_rejects_bad_requests():
+    torch = pytest.importorskip("torch")
+    wl = workloads.dna_batched(n=50, seed=79)
+    pairs = ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len)
+    d = torch.zeros(ib.device_packed_bytes(wl.codes.size, 2) + 8, dtype=torch.uint8, device="cuda")
+    d_pairs = torch.from_numpy(pairs.view(np.uint8)).cuda()
+    out = torch.zeros((3, wl.n), dtype=torch.int32, device="cuda")
+    args = (d_pairs.data_ptr(), wl.n, 250, 1000, out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr())
+    with _engine(wl, True) as e:
+        for bits, ptr in ((3, d.data_ptr()), (8, d.data_ptr()), (2, d.data_ptr() + 1)):
+            with pytest.raises(ib.IpumaError) as ei:
+                e.compare_device_packed(ptr, wl.codes.size, bits, *args)
+            assert ei.value.code == ib.ERR_INVALID_ARG
+        # the per-thread class reads bytes only
+        e.set_option("tile_k", 7)
+        with pytest.raises(ib.IpumaError):
+            e.compare_device_packed(d.data_ptr(), wl.codes.size, 2, *args)
