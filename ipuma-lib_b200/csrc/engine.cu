@@ -1605,7 +1605,9 @@ static int check_bits(const ipuma_engine* e, int bits) {
   // 2-bit codes are A, T, C, G = nucleic-acid codes 1..4.
   if (bits == 2 && e->sw.datatype != IPUMA_DT_NUCLEIC_ACID)
     return fail(IPUMA_ERR_INVALID_ARG, "2-bit codes are nucleic-acid codes");
-  if (e->M > (1 << bits))
+  // 4 and 5 bits hold codes 0 .. 2^bits - 1: the alphabet must fit (2 bits
+  // hold A, C, G, T of the nucleic-acid alphabet).
+  if (bits != 2 && e->M > (1 << bits))
     return fail(IPUMA_ERR_INVALID_ARG, "%d-bit codes hold at most %d letters (this alphabet has %d)", bits, 1 << bits,
                 e->M);
   if (e->tile_k == kClsThread + 1)
