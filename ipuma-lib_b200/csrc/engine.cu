@@ -341,23 +341,23 @@ long thread_threads(ipuma_engine* e) {
 // Lane groups (one scratch slice each) of the widest batched launch.
 int max_batched_groups(ipuma_engine* e) {
   int g = 0;
-  g = std::max(g, batched_grid<LaneS16x2, 4, 16>(e) * 2);
-  g = std::max(g, batched_grid<LaneS16x2, 8, 16>(e) * 2);
-  g = std::max(g, batched_grid<LaneS16x2, 12, 16>(e) * 2);
-  g = std::max(g, batched_grid<LaneS16x2, 16, 16>(e) * 2);
-  g = std::max(g, batched_grid<LaneS16x2, 6, 16>(e) * 2);
-  g = std::max(g, batched_grid<LaneS16x2, 10, 16>(e) * 2);
-  g = std::max(g, batched_grid<LaneS16x2, 14, 16>(e) * 2);
-  g = std::max(g, batched_grid<LaneS16x2, 5, 16>(e) * 2);
-  g = std::max(g, batched_grid<LaneS16x2, 7, 16>(e) * 2);
-  g = std::max(g, batched_grid<LaneS16x2, 9, 16>(e) * 2);
-  g = std::max(g, batched_grid<LaneS16x2, 11, 16>(e) * 2);
-  g = std::max(g, batched_grid<LaneS16x2, 13, 16>(e) * 2);
-  g = std::max(g, batched_grid<LaneS16x2, 15, 16>(e) * 2);
-  g = std::max(g, batched_grid<LaneS16x2, 12, 32>(e));
-  g = std::max(g, batched_grid<LaneS16x2, 16, 32>(e));
+  g = std::max(g, batched_grid<Lane16, 4, 16>(e) * 2);
+  g = std::max(g, batched_grid<Lane16, 8, 16>(e) * 2);
+  g = std::max(g, batched_grid<Lane16, 12, 16>(e) * 2);
+  g = std::max(g, batched_grid<Lane16, 16, 16>(e) * 2);
+  g = std::max(g, batched_grid<Lane16, 6, 16>(e) * 2);
+  g = std::max(g, batched_grid<Lane16, 10, 16>(e) * 2);
+  g = std::max(g, batched_grid<Lane16, 14, 16>(e) * 2);
+  g = std::max(g, batched_grid<Lane16, 5, 16>(e) * 2);
+  g = std::max(g, batched_grid<Lane16, 7, 16>(e) * 2);
+  g = std::max(g, batched_grid<Lane16, 9, 16>(e) * 2);
+  g = std::max(g, batched_grid<Lane16, 11, 16>(e) * 2);
+  g = std::max(g, batched_grid<Lane16, 13, 16>(e) * 2);
+  g = std::max(g, batched_grid<Lane16, 15, 16>(e) * 2);
+  g = std::max(g, batched_grid<Lane16, 12, 32>(e));
+  g = std::max(g, batched_grid<Lane16, 16, 32>(e));
   g = std::max(g, batched_grid<LaneS32, 16, 32>(e));
-  g = std::max(g, batched_grid<LaneS16x2, 16, 32, true>(e));
+  g = std::max(g, batched_grid<Lane16, 16, 32, true>(e));
   return g * kWarpsPerBlock;
 }
 
@@ -459,23 +459,23 @@ void class_grids(ipuma_engine* e, int maxA, int maxB, int* grid, long long* spb)
   const long long rowsCap = std::max(1, maxB);
   for (int c = 0; c < kNumClasses; ++c) {
     switch (c) {
-      case kClsHi: grid[c] = batched_grid<LaneS16x2, 16, 32, true>(e); break;
-      case 0: grid[c] = batched_grid<LaneS16x2, 4, 16>(e); break;
-      case 1: grid[c] = batched_grid<LaneS16x2, 8, 16>(e); break;
-      case 2: grid[c] = batched_grid<LaneS16x2, 12, 16>(e); break;
-      case 3: grid[c] = batched_grid<LaneS16x2, 16, 16>(e); break;
-      case 4: grid[c] = batched_grid<LaneS16x2, 12, 32>(e); break;
-      case 5: grid[c] = batched_grid<LaneS16x2, 16, 32>(e); break;
+      case kClsHi: grid[c] = batched_grid<Lane16, 16, 32, true>(e); break;
+      case 0: grid[c] = batched_grid<Lane16, 4, 16>(e); break;
+      case 1: grid[c] = batched_grid<Lane16, 8, 16>(e); break;
+      case 2: grid[c] = batched_grid<Lane16, 12, 16>(e); break;
+      case 3: grid[c] = batched_grid<Lane16, 16, 16>(e); break;
+      case 4: grid[c] = batched_grid<Lane16, 12, 32>(e); break;
+      case 5: grid[c] = batched_grid<Lane16, 16, 32>(e); break;
       case kClsThread: grid[c] = (int)(thread_threads<16>(e) / kThreads); break;
-      case 7: grid[c] = batched_grid<LaneS16x2, 6, 16>(e); break;
-      case 8: grid[c] = batched_grid<LaneS16x2, 10, 16>(e); break;
-      case 9: grid[c] = batched_grid<LaneS16x2, 14, 16>(e); break;
-      case 10: grid[c] = batched_grid<LaneS16x2, 5, 16>(e); break;
-      case 11: grid[c] = batched_grid<LaneS16x2, 7, 16>(e); break;
-      case 12: grid[c] = batched_grid<LaneS16x2, 9, 16>(e); break;
-      case 13: grid[c] = batched_grid<LaneS16x2, 11, 16>(e); break;
-      case 14: grid[c] = batched_grid<LaneS16x2, 13, 16>(e); break;
-      case 15: grid[c] = batched_grid<LaneS16x2, 15, 16>(e); break;
+      case 7: grid[c] = batched_grid<Lane16, 6, 16>(e); break;
+      case 8: grid[c] = batched_grid<Lane16, 10, 16>(e); break;
+      case 9: grid[c] = batched_grid<Lane16, 14, 16>(e); break;
+      case 10: grid[c] = batched_grid<Lane16, 5, 16>(e); break;
+      case 11: grid[c] = batched_grid<Lane16, 7, 16>(e); break;
+      case 12: grid[c] = batched_grid<Lane16, 9, 16>(e); break;
+      case 13: grid[c] = batched_grid<Lane16, 11, 16>(e); break;
+      case 14: grid[c] = batched_grid<Lane16, 13, 16>(e); break;
+      case 15: grid[c] = batched_grid<Lane16, 15, 16>(e); break;
       default: grid[c] = batched_grid<LaneS32, 16, 32>(e); break;
     }
     if (c == kClsThread)
@@ -620,7 +620,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   bp.n_codes = (long long)n_codes;
   bp.bits = bits;
   bp.M = e->M;
-  bp.s16_limit = e->sc.s16Limit;
+  bp.s16_limit = e->sc.u16Limit;
   if ((rc = rb.flag->ensure((size_t)n + 64, s))) return rc;
   const int nkeys = bp.nclass * NBUCKET;
   const int tb = 256;
@@ -677,7 +677,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   }
   if ((enabled >> kClsHi) & 1u) {
     cudaStream_t cs = on(kClsHi);
-    if ((rc = launch_batched<LaneS16x2, 16, 32, true>(e, sc, rb, cs, codes, pairs, list, R + 2 * kClsHi,
+    if ((rc = launch_batched<Lane16, 16, 32, true>(e, sc, rb, cs, codes, pairs, list, R + 2 * kClsHi,
                                                       heads + kClsHi, rowsCap, score, arange, brange,
                                                       kClasses[kClsHi].kind, kClsHi, kClsHi)))
       return rc;
@@ -685,8 +685,8 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
     ++*launches;
   }
   IPUMA_LAUNCH(LaneS32, 16, 32, 16)
-  IPUMA_LAUNCH(LaneS16x2, 16, 32, 5)
-  IPUMA_LAUNCH(LaneS16x2, 12, 32, 4)
+  IPUMA_LAUNCH(Lane16, 16, 32, 5)
+  IPUMA_LAUNCH(Lane16, 12, 32, 4)
   if ((enabled >> kClsThread) & 1u) {
     cudaStream_t cs = on(kClsThread);
     if ((rc = launch_thread<16>(e, rb, cs, codes, pairs, list, R + 2 * kClsThread, heads + kClsThread,
@@ -695,19 +695,19 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
     if ((rc = done(kClsThread))) return rc;
     ++*launches;
   }
-  IPUMA_LAUNCH(LaneS16x2, 16, 16, 3)
-  IPUMA_LAUNCH(LaneS16x2, 15, 16, 15)
-  IPUMA_LAUNCH(LaneS16x2, 14, 16, 9)
-  IPUMA_LAUNCH(LaneS16x2, 13, 16, 14)
-  IPUMA_LAUNCH(LaneS16x2, 12, 16, 2)
-  IPUMA_LAUNCH(LaneS16x2, 11, 16, 13)
-  IPUMA_LAUNCH(LaneS16x2, 10, 16, 8)
-  IPUMA_LAUNCH(LaneS16x2, 9, 16, 12)
-  IPUMA_LAUNCH(LaneS16x2, 8, 16, 1)
-  IPUMA_LAUNCH(LaneS16x2, 7, 16, 11)
-  IPUMA_LAUNCH(LaneS16x2, 6, 16, 7)
-  IPUMA_LAUNCH(LaneS16x2, 5, 16, 10)
-  IPUMA_LAUNCH(LaneS16x2, 4, 16, 0)
+  IPUMA_LAUNCH(Lane16, 16, 16, 3)
+  IPUMA_LAUNCH(Lane16, 15, 16, 15)
+  IPUMA_LAUNCH(Lane16, 14, 16, 9)
+  IPUMA_LAUNCH(Lane16, 13, 16, 14)
+  IPUMA_LAUNCH(Lane16, 12, 16, 2)
+  IPUMA_LAUNCH(Lane16, 11, 16, 13)
+  IPUMA_LAUNCH(Lane16, 10, 16, 8)
+  IPUMA_LAUNCH(Lane16, 9, 16, 12)
+  IPUMA_LAUNCH(Lane16, 8, 16, 1)
+  IPUMA_LAUNCH(Lane16, 7, 16, 11)
+  IPUMA_LAUNCH(Lane16, 6, 16, 7)
+  IPUMA_LAUNCH(Lane16, 5, 16, 10)
+  IPUMA_LAUNCH(Lane16, 4, 16, 0)
 #undef IPUMA_LAUNCH
   // Exact 32-bit rerun of the s16x2 pairs whose score may have overflowed
   // (after every class: it reads their overflow list).
@@ -831,9 +831,9 @@ int run_plain_wire(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const int
     return timed_end(e, s);
   };
   if (s16) {
-    if (K == 4) rc = go(k_plain16<4>, smem_for<LaneS16x2, 4, 32>(e));
-    else if (K == 8) rc = go(k_plain16<8>, smem_for<LaneS16x2, 8, 32>(e));
-    else rc = go(k_plain16<16>, smem_for<LaneS16x2, 16, 32>(e));
+    if (K == 4) rc = go(k_plain16<4>, smem_for<Lane16, 4, 32>(e));
+    else if (K == 8) rc = go(k_plain16<8>, smem_for<Lane16, 8, 32>(e));
+    else rc = go(k_plain16<16>, smem_for<Lane16, 16, 32>(e));
   } else {
     if (K == 4) rc = go(k_plain<4>, smem_for<LaneS32, 4, 32>(e));
     else if (K == 8) rc = go(k_plain<8>, smem_for<LaneS32, 8, 32>(e));
@@ -1027,21 +1027,21 @@ int run_autotune(ipuma_engine* e, const char* cache_path) {
     const int rounds = L > 0 ? 6 : 2;
     int grid = 1;
     switch (c) {
-      case 0: grid = batched_grid<LaneS16x2, 4, 16>(e); break;
-      case 1: grid = batched_grid<LaneS16x2, 8, 16>(e); break;
-      case 2: grid = batched_grid<LaneS16x2, 12, 16>(e); break;
-      case 3: grid = batched_grid<LaneS16x2, 16, 16>(e); break;
-      case 4: grid = batched_grid<LaneS16x2, 12, 32>(e); break;
-      case 5: grid = batched_grid<LaneS16x2, 16, 32>(e); break;
-      case 7: grid = batched_grid<LaneS16x2, 6, 16>(e); break;
-      case 8: grid = batched_grid<LaneS16x2, 10, 16>(e); break;
-      case 9: grid = batched_grid<LaneS16x2, 14, 16>(e); break;
-      case 10: grid = batched_grid<LaneS16x2, 5, 16>(e); break;
-      case 11: grid = batched_grid<LaneS16x2, 7, 16>(e); break;
-      case 12: grid = batched_grid<LaneS16x2, 9, 16>(e); break;
-      case 13: grid = batched_grid<LaneS16x2, 11, 16>(e); break;
-      case 14: grid = batched_grid<LaneS16x2, 13, 16>(e); break;
-      case 15: grid = batched_grid<LaneS16x2, 15, 16>(e); break;
+      case 0: grid = batched_grid<Lane16, 4, 16>(e); break;
+      case 1: grid = batched_grid<Lane16, 8, 16>(e); break;
+      case 2: grid = batched_grid<Lane16, 12, 16>(e); break;
+      case 3: grid = batched_grid<Lane16, 16, 16>(e); break;
+      case 4: grid = batched_grid<Lane16, 12, 32>(e); break;
+      case 5: grid = batched_grid<Lane16, 16, 32>(e); break;
+      case 7: grid = batched_grid<Lane16, 6, 16>(e); break;
+      case 8: grid = batched_grid<Lane16, 10, 16>(e); break;
+      case 9: grid = batched_grid<Lane16, 14, 16>(e); break;
+      case 10: grid = batched_grid<Lane16, 5, 16>(e); break;
+      case 11: grid = batched_grid<Lane16, 7, 16>(e); break;
+      case 12: grid = batched_grid<Lane16, 9, 16>(e); break;
+      case 13: grid = batched_grid<Lane16, 11, 16>(e); break;
+      case 14: grid = batched_grid<Lane16, 13, 16>(e); break;
+      case 15: grid = batched_grid<Lane16, 15, 16>(e); break;
       default: grid = (int)(thread_threads<16>(e) / kThreads); break;
     }
     const int minPairs = grid * kWarpsPerBlock * perItem * rounds;
@@ -1463,12 +1463,16 @@ int ipuma_gpu_create(const ipuma_sw_config* sw, const ipuma_algo_config* algo, i
   // gE <= 0) and profile entries sim - (gI+gE) must fit int8.
   e->fast_ok = (gI + gE < 0) && (gE <= 0) && (e->maxSub - (gI + gE) <= 127) &&
                (minSub - (gI + gE) >= -128) && (gI + gE > -1000) && (gE > -1000);
-  // s16x2 lanes: H <= 32767 - maxSub guarantees no halfword overflow.
+  // 16-bit lanes: H <= limit guarantees no halfword leaves its range (signed
+  // halves of the per-thread class: 32767 - maxSub; the biased unsigned
+  // halves of the wavefront classes: 65535 - bias - maxSub).  Pairs that
+  // may pass the wavefront classes' limit are checked by the binning pass.
   e->sc.s16Limit = 32767 - std::max(0, e->maxSub);
+  e->sc.u16Limit = 65535 - Lane16::BIAS - std::max(0, e->maxSub);
   e->sc.maxSub = std::max(0, e->maxSub);
   e->sc.bits = 8;
   e->s16_ok = e->fast_ok;
-  e->s16_max_len = e->maxSub > 0 ? (e->sc.s16Limit / e->maxSub) : (1 << 30);
+  e->s16_max_len = e->maxSub > 0 ? (e->sc.u16Limit / e->maxSub) : (1 << 30);
   set_default_rates(e.get());
   max_batched_groups(e.get());  // warm the grid cache
   thread_threads<16>(e.get());

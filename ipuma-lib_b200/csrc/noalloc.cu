@@ -165,7 +165,8 @@ extern "C" int ipuma_gpu_compare_noalloc(const ipuma_sw_config* sw, int32_t forw
   sc.gIgE = gI + gE;
   sc.M = m;
   sc.forwardOnly = forward_only ? 1 : 0;
-  sc.s16Limit = 32767;
+  sc.s16Limit = 32767;  // (16-bit lanes are not used here)
+  sc.u16Limit = 32767;
   sc.bits = 8;  // one byte per residue
   // Warps that fit the static scratch at this row count (2 rows per B row).
   const long rowsCap = max_b_len;

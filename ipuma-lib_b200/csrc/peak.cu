@@ -1,6 +1,8 @@
 // peak.cu -- measures the integer/DPX issue peak that bounds the alignment
-// kernels: the instruction mix of one s16x2 cell update
-//   3 x add.s16x2, 2 x viaddmax.s16x2, 1 x vimax3.relu.s16x2, 1 x max.s16x2
+// kernels: the instruction mix of one cell update of the wavefront classes
+// (biased unsigned 16-bit halves, two cells per instruction)
+//   1 x prmt (substitution bytes), 5 x viaddmax.u16x2 (F, F term of Y, Y,
+//   E, H), 1 x max.u16x2 (row maximum)
 // (7 instructions = 14 lane-ops, two cells), run as independent chains by
 // every thread of a full-occupancy grid.  Reported as lane-ops per second.
 #include <cuda_runtime.h>
@@ -16,26 +18,27 @@ constexpr int kChains = 8;
 constexpr int kIters = 4096;
 
 __global__ void __launch_bounds__(256) k_int_peak(uint32_t seed, uint32_t* sink) {
-  using T = ipuma_dev::LaneS16x2;
-  uint32_t e[kChains], f[kChains], h[kChains];
-  const uint32_t g = T::splat(-1), go = T::splat(-2);
+  using T = ipuma_dev::LaneU16x2;
+  uint32_t e[kChains], f[kChains], h[kChains], w[kChains];
+  const uint32_t g = T::delta(-1), go = T::delta(-2), floor0 = T::splat(0);
 #pragma unroll
   for (int c = 0; c < kChains; ++c) {
     e[c] = seed ^ (threadIdx.x * 2654435761u) ^ c;
     f[c] = e[c] * 3u;
     h[c] = e[c] * 7u;
+    w[c] = e[c] * 13u;
   }
   uint32_t rm = 0;
   for (int it = 0; it < kIters; ++it) {
 #pragma unroll
     for (int c = 0; c < kChains; ++c) {
-      const uint32_t hg = T::add(h[c], go);                 // add
-      e[c] = T::addmax(e[c], g, hg);                        // viaddmax
-      f[c] = T::addmax(f[c], g, hg);                        // viaddmax
-      const uint32_t t = T::add(h[c], f[c]);                // add
-      h[c] = T::max3relu(t, e[c], f[c]);                    // vimax3.relu
-      h[c] = T::add(h[c], go);                              // add
-      rm = T::max2(rm, h[c]);                               // max
+      const uint32_t sb = T::sub<1>(w[c], h[c]);          // prmt
+      f[c] = T::addmax(f[c], g, h[c]);                    // F
+      const uint32_t ft = T::addmax(f[c], go, floor0);    // F term of Y
+      const uint32_t y = T::addmax(h[c], sb, ft);         // Y
+      e[c] = T::addmax(e[c], g, y);                       // E
+      h[c] = T::addmax(e[c], go, y);                      // H
+      rm = T::max2(rm, h[c]);                             // row maximum
     }
   }
   uint32_t acc = rm;

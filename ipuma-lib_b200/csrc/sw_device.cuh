@@ -61,13 +61,14 @@ struct SwConst {
   int gIgE;     // gI + gE
   int M;        // alphabet size (rows/cols of the substitution matrix)
   int forwardOnly;
-  int s16Limit; // a pair whose score exceeds this is rerun in s32
+  int s16Limit; // a pair whose score exceeds this is rerun in s32 (signed halves)
+  int u16Limit; // the same for the biased unsigned halves (LaneU16x2)
   int maxSub;   // largest substitution score (strip bound of the hybrid pass)
   int bits;     // bits per residue of the code array (8, or packed 2/4/5: code_at)
 };
 
 // Control of a hybrid pass (sw_pass with HYB): an s16x2 pass that stops
-// before the first strip whose values could pass sc.s16Limit, and the s32
+// before the first strip whose values could pass the 16-bit lanes' limit, and the s32
 // pass that continues one of its pairs from there.  A strip's H values are
 // at most max(0, H of the boundary column entering it) + maxSub * strip
 // width: a path enters from that column or starts inside the strip, and
@@ -153,6 +154,81 @@ struct LaneS16x2 {
     return h == 0 ? (int)(int16_t)(v & 0xffff) : (int)(int16_t)(v >> 16);
   }
   __device__ __forceinline__ static V shfl_up(V v) { return __shfl_up_sync(FULL, v, 1); }
+};
+
+// Two pairs per warp in biased unsigned 16-bit halves (pair P low, pair Q
+// high): a score v is held as v + BIAS in [0, 65535], so one lane covers
+// scores up to 65535 - BIAS - max(sim) -- twice the signed halfword's range
+// -- with the same instructions per cell.  Every stored value (H, Y, and E,
+// F shifted by -(gI + gE)) is >= 0, so it is >= BIAS when biased; a sum
+// with a profile byte (>= -128), gI + gE or gE (> -1000 on this path)
+// stays >= 0 and no halfword wraps below zero.  The floor 0 of the
+// recurrence is BIAS here: it is folded into the F term of Y (Cell::fterm),
+// so Y needs no relu.  The running best goes through the unsigned DPX max
+// with predicates (update_best).
+struct LaneU16x2 {
+  using V = uint32_t;
+  static constexpr int NP = 2;
+  static constexpr int BIAS = 1024;
+  __device__ __forceinline__ static V splat(int x) {  // a score
+    const uint32_t v = (uint32_t)(x + BIAS) & 0xffffu;
+    return v | (v << 16);
+  }
+  __device__ __forceinline__ static V delta(int x) {  // an addend
+    const uint32_t v = (uint32_t)x & 0xffffu;
+    return v | (v << 16);
+  }
+  __device__ __forceinline__ static V add(V a, V b) {  // mod 2^16 per half
+    V d;
+    asm("add.s16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+  }
+  __device__ __forceinline__ static V addmax(V a, V b, V c) { return __viaddmax_u16x2(a, b, c); }
+  __device__ __forceinline__ static V max2(V a, V b) {
+    V d;
+    asm("max.u16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+  }
+  template <int C>
+  __device__ __forceinline__ static V sub(uint32_t wp, uint32_t wq) {
+    return prmt(wp, wq, (uint32_t)(C | ((C | 8) << 4) | ((4 + C) << 8) | (((4 + C) | 8) << 12)));
+  }
+  __device__ __forceinline__ static int half(V v, int h) {
+    return (int)((h == 0) ? (v & 0xffffu) : (v >> 16)) - BIAS;
+  }
+  __device__ __forceinline__ static V shfl_up(V v) { return __shfl_up_sync(FULL, v, 1); }
+};
+
+// The 16-bit lane type of the engine's wavefront classes.
+using Lane16 = LaneU16x2;
+
+// The pieces of one cell that differ between lane types.
+//   fterm(F̂, gI+gE)    the F term of Y: F̂ + gI + gE (with the floor 0 of
+//                      the recurrence for biased lanes)
+//   ymax(Hdiag, s, f)  Y = max(Hdiag + s, f, 0)
+//   delta(x)           an addend (gap penalties) in the lane's format
+//   limit(sc)          largest score a lane may hold before the next cells
+//                      could leave its range (checked every 32 steps)
+template <class T>
+struct Cell {
+  __device__ __forceinline__ static typename T::V fterm(typename T::V f, typename T::V gIgE) {
+    return T::add(f, gIgE);
+  }
+  __device__ __forceinline__ static typename T::V ymax(typename T::V d, typename T::V s, typename T::V f) {
+    return T::addmax_relu(d, s, f);
+  }
+  __device__ __forceinline__ static typename T::V delta(int x) { return T::splat(x); }
+  __device__ __forceinline__ static int limit(const SwConst& sc) { return sc.s16Limit; }
+};
+template <>
+struct Cell<LaneU16x2> {
+  using V = LaneU16x2::V;
+  __device__ __forceinline__ static V fterm(V f, V gIgE) {
+    return LaneU16x2::addmax(f, gIgE, LaneU16x2::splat(0));
+  }
+  __device__ __forceinline__ static V ymax(V d, V s, V f) { return LaneU16x2::addmax(d, s, f); }
+  __device__ __forceinline__ static V delta(int x) { return LaneU16x2::delta(x); }
+  __device__ __forceinline__ static int limit(const SwConst& sc) { return sc.u16Limit; }
 };
 
 // -------------------------------------------------------------------------
@@ -289,6 +365,23 @@ __device__ __forceinline__ uint32_t keep_mask(LaneS32, int rm, int b) {
   return (uint32_t)((rm + ~b) >> 31);
 }
 
+// Raises the running best `b` to the row maximum `rm` and returns the keep
+// mask of the halves (or word) that did not improve.
+template <class T>
+__device__ __forceinline__ uint32_t update_best(T, typename T::V& b, typename T::V rm) {
+  const uint32_t keep = keep_mask(T{}, rm, b);
+  b = T::max2(b, rm);
+  return keep;
+}
+// Biased unsigned halves differ by up to 65535, so the signed-difference
+// trick does not apply: the DPX max with predicates (b >= rm per half)
+// gives the new best and the keep mask in one instruction.
+__device__ __forceinline__ uint32_t update_best(LaneU16x2, uint32_t& b, uint32_t rm) {
+  bool hi, lo;
+  b = __vibmax_u16x2(b, rm, &hi, &lo);
+  return (lo ? 0x0000ffffu : 0u) | (hi ? 0xffff0000u : 0u);
+}
+
 // -------------------------------------------------------------------------
 // One full pass (forward or reverse) of one warp.
 //
@@ -300,7 +393,7 @@ __device__ __forceinline__ uint32_t keep_mask(LaneS32, int rm, int b) {
 // take an unrolled path without per-step activity checks.
 //
 // Returns false when s16x2 lanes gave up because a running best passed
-// sc.s16Limit (checked every 32 steps, warp-uniformly); the caller reruns
+// the lane's limit (Cell::limit, checked every 32 steps, warp-uniformly); the caller reruns
 // the warp's pairs in s32 lanes.
 //
 //   s_prof   : this group's profile area, NP * (M + 1) * LANES * K bytes
@@ -350,15 +443,16 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
 #pragma unroll
   for (int h = 0; h < NP; ++h) capRows[h] = ps[h].blen;
   const unsigned gmask = (LANES == 32) ? FULL : (0xFFFFu << (threadIdx.x & 16));
-  const V vgE = T::splat(sc.gE);
-  const V vgEp = T::splat(max(sc.gE, sc.gIgE));
-  const V vgIgE = T::splat(sc.gIgE);
+  using C = Cell<T>;
+  const V vgE = C::delta(sc.gE);
+  const V vgEp = C::delta(max(sc.gE, sc.gIgE));
+  const V vgIgE = C::delta(sc.gIgE);
   // Ê handed to column 0 (and the initial hand-over value): -gE' makes the
   // first column's Ê come out as the reference's E = max(gI, H - gI) + gE.
   const V vE0 = T::splat(-max(sc.gE, sc.gIgE));
   const V vF0 = T::splat(-sc.gIgE);   // F̂ where F = 0 (pass start)
   const V vZero = T::splat(0);
-  const int lim = sc.s16Limit;
+  const int lim = C::limit(sc);
   // Steps unrolled in a check-free block: the block's code has to stay in
   // the instruction cache next to the checked path.
   // (Measured on B200: 8 steps for K <= 12, 4 for K = 16; the full LANES
@@ -410,8 +504,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
     auto bnd = [&](int r) -> int2 {
       const int2 v = scrIn[r];
       if (HYB && NP == 1 && packedIn) {
-        const int sh = 16 * ctl->bndHalf;
-        return make_int2((int)(int16_t)((uint32_t)v.x >> sh), (int)(int16_t)((uint32_t)v.y >> sh));
+        return make_int2(Lane16::half((uint32_t)v.x, ctl->bndHalf), Lane16::half((uint32_t)v.y, ctl->bndHalf));
       }
       return v;
     };
@@ -502,7 +595,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
             default: sb = T::template sub<3>(wp[c >> 2], wq[c >> 2]); break;
           }
           const V f = T::addmax(Fh[c], vgE, H[c]);                   // F̂
-          const V y = T::addmax_relu(diag, sb, T::add(f, vgIgE));    // Y
+          const V y = C::ymax(diag, sb, C::fterm(f, vgIgE));         // Y
           e = T::addmax(e, vgEp, yl);                                // Ê
           const V hv = T::addmax(e, vgIgE, y);                       // H
           diag = H[c];
@@ -523,8 +616,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
           for (int c = 0; c + w < (K + 1) / 2; c += 2 * w) m8[c] = T::max2(m8[c], m8[c + w]);
         const V rm = m8[0];
         // Running best of this lane: strict > keeps the first row.
-        const uint32_t keep = keep_mask(T{}, rm, best);
-        best = T::max2(best, rm);
+        const uint32_t keep = update_best(T{}, best, rm);
         if (keep != 0xffffffffu) {
           const uint32_t ipk = (uint32_t)i * 0x00010001u;  // row in both halfwords
           brow = (brow & keep) | (ipk & ~keep);

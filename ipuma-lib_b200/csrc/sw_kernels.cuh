@@ -110,8 +110,8 @@ __device__ __forceinline__ void load_simp(int8_t* s_simp, const int8_t* sim, con
 }
 
 // Forward pass (+ reverse pass unless forwardOnly) for the NP pairs held
-// by one lane group.  For s16x2 lanes a pair whose score exceeds
-// sc.s16Limit (or any pair of a warp that gave up) is flagged in `ovf` and
+// by one lane group.  For 16-bit lanes a pair whose score exceeds the
+// lane's limit (or any pair of a warp that gave up) is flagged in `ovf` and
 // gets no reverse pass (the s32 rerun redoes it).
 // MODE: 0 = by sc.forwardOnly at run time, 1 = forward only, 2 = with the
 // reverse pass (a kernel specialised for one mode holds only its code, so
@@ -136,7 +136,7 @@ __device__ __forceinline__ void align_pairs(const SwConst& sc, uint8_t* s_prof,
     if constexpr (MODE != 2) {
       const bool done = sw_pass<T, K, LANES>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, fw);
 #pragma unroll
-      for (int h = 0; h < NP; ++h) ovf[h] = (NP == 2) && (!done || fw[h].s > sc.s16Limit);
+      for (int h = 0; h < NP; ++h) ovf[h] = (NP == 2) && (!done || fw[h].s > Cell<T>::limit(sc));
     }
     return;
   }
@@ -162,7 +162,7 @@ __device__ __forceinline__ void align_pairs(const SwConst& sc, uint8_t* s_prof,
 #pragma unroll
     for (int h = 0; h < NP; ++h) {
       fw[h] = res[h];
-      ovf[h] = (NP == 2) && (!done || fw[h].s > sc.s16Limit);
+      ovf[h] = (NP == 2) && (!done || fw[h].s > Cell<T>::limit(sc));
       const bool run = !ovf[h] && fw[h].s > 0;
       any |= run;
       ps[h] = run ? PassSeq{codes, a0[h] + fw[h].j, b0[h] + fw[h].i, fw[h].j + 1, fw[h].i + 1, -1, -1}
@@ -185,7 +185,7 @@ __device__ __forceinline__ bool hybrid_pass(const SwConst& sc, uint8_t* s_prof, 
                                             uint16_t* s_bring, const PassSeq (&ps)[2], int2* scr,
                                             long rowsCap, Best (&out)[2]) {
   PassCtl c16;
-  if (!sw_pass<LaneS16x2, K, 32, true>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, out, &c16)) return false;
+  if (!sw_pass<Lane16, K, 32, true>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, out, &c16)) return false;
   if (c16.stoppedAt < 0) return true;
 #pragma unroll 1
   for (int h = 0; h < 2; ++h) {
@@ -430,7 +430,7 @@ __global__ void __launch_bounds__(128) k_plain16(SwConst sc, const int8_t* __res
                                                  long metaOffset, int maxBatches, int totalSlots,
                                                  int2* scratch, long rowsCap, int* results,
                                                  DevStatus* st) {
-  using L = SmemLayout<LaneS16x2, K, 32>;
+  using L = SmemLayout<Lane16, K, 32>;
   extern __shared__ __align__(16) uint8_t smem[];
   const int warps = blockDim.x >> 5;
   const int wib = threadIdx.x >> 5;
@@ -467,7 +467,7 @@ __global__ void __launch_bounds__(128) k_plain16(SwConst sc, const int8_t* __res
     }
     Best fw[2], rv[2];
     bool ovf[2];
-    align_pairs<LaneS16x2, K, 32>(sc, s_prof, s_simp, s_bring, bytes, a0, b0, al, bl, scr, rowsCap, fw, rv, ovf);
+    align_pairs<Lane16, K, 32>(sc, s_prof, s_simp, s_bring, bytes, a0, b0, al, bl, scr, rowsCap, fw, rv, ovf);
 #pragma unroll 1
     for (int h = 0; h < 2; ++h) {
       if (g0 + h >= totalSlots) break;

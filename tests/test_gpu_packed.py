@@ -181,16 +181,27 @@ def test_device_packed_equals_bytes_and_oracle(bits, kind, forward_only):
 
 
 def test_device_packed_high_scores_hybrid_and_s32():
-    # Near-identical long protein pairs: the diagonal bound (read packed)
-    # sends them to the hybrid class, which switches to s32 strips; with
-    # option hybrid 0 they run in the s32 class.
-    wl = workloads.protein_mixed(n=1_200, seed=77, long_identical_frac=0.01)
-    assert (wl.a_len >= 7000).sum() >= 8
-    pairs = ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len)
-    want = _oracle(wl, wl.codes, pairs, True)
-    assert want[0].max() > 32767
+    # Near-identical long protein pairs (scores above int16, held by the
+    # 16-bit lanes), plus W/C-rich pairs scoring above the 16-bit lanes'
+    # range: the diagonal bound (read packed) sends those to the hybrid
+    # class, which switches to s32 strips; with option hybrid 0 they run in
+    # the s32 class.
+    base = workloads.protein_mixed(n=1_200, seed=77, long_identical_frac=0.01)
+    rng = np.random.default_rng(77)
+    wc = np.array([oracle.encode("aa", "W")[0], oracle.encode("aa", "C")[0]], dtype=np.uint8)
+    extra_a = [rng.choice(wc, n).astype(np.uint8) for n in (6800, 7100)]
+    extra_b = [a.copy() for a in extra_a]
+    codes = np.concatenate([base.codes] + extra_a + extra_b).astype(np.uint8)
+    off = base.codes.size
+    a_off = np.concatenate([base.a_off, [off, off + 6800]])
+    b_off = np.concatenate([base.b_off, [off + 6800 + 7100, off + 2 * 6800 + 7100]])
+    a_len = np.concatenate([base.a_len, [6800, 7100]])
+    b_len = np.concatenate([base.b_len, [6800, 7100]])
+    pairs = ib.make_pairs(a_off, a_len, b_off, b_len)
+    want = _oracle(base, codes, pairs, True)
+    assert want[0].max() > 65535 - 1024 - 11 and (want[0] > 32767).sum() >= 8
     for hybrid in (1, 0):
-        got_p, _ = _device_packed(wl, wl.codes, pairs, 5, True, hybrid=hybrid)
+        got_p, _ = _device_packed(base, codes, pairs, 5, True, hybrid=hybrid)
         _same(got_p, want, "5-bit high scores hybrid=%d" % hybrid)
 
 

@@ -149,20 +149,26 @@ def test_protein_workload_sample(forward_only):
 
 def test_protein_mixed_with_s16_overflow():
     """Heavy-tailed protein lengths plus near-identical 7000+ residue pairs
-    whose scores exceed int16: they must come back exact (s32 lanes)."""
+    whose scores exceed int16: they must come back exact (the wavefront
+    classes' biased unsigned 16-bit lanes hold them)."""
     wl = workloads.protein_mixed(n=1_500, seed=13, long_identical_frac=0.004)
     got, want, st = _wl_run(wl, forward_only=False)
     _assert_same(got, want, wl.name)
     assert (want[0] > 32767).sum() >= 3
 
 
+# Largest score the wavefront classes' 16-bit lanes hold (BLOSUM62).
+U16_LIMIT = 65535 - 1024 - 11
+
+
 def test_s16_rerun_of_unpredicted_overflow():
     """A pair whose main diagonal looks unrelated (so it is not routed to
-    s32 lanes up front) but whose gapped score exceeds int16: the s16x2
-    kernel gives up on the device and the pair is rerun in 32-bit."""
+    s32 lanes up front) but whose gapped score exceeds the 16-bit lanes'
+    range: the kernel gives up on the device and the pair is rerun in
+    32-bit."""
     rng = np.random.default_rng(5)
     w, c = oracle.encode("aa", "W")[0], oracle.encode("aa", "C")[0]
-    a = np.where(rng.random(3500) < 0.5, w, c).astype(np.uint8)
+    a = np.where(rng.random(7000) < 0.5, w, c).astype(np.uint8)
     b = np.concatenate([[oracle.encode("aa", "A")[0]], a]).astype(np.uint8)
     short = a[:1000]
     codes = np.concatenate([a, b, short, short])
@@ -178,7 +184,7 @@ def test_s16_rerun_of_unpredicted_overflow():
         want = oracle.sw_batch(codes, pairs["a_off"], pairs["a_len"], pairs["b_off"],
                                pairs["b_len"], sim, -10, -1, forward_only=fwd)
         _assert_same(got, want, "overflow fwd=%s" % fwd)
-        assert want[0][0] > 32767
+        assert want[0][0] > U16_LIMIT
         assert st.overflow_reruns >= 1
 
 
@@ -278,17 +284,21 @@ def _mutated(rng, seq, rate, alphabet):
 
 @pytest.mark.parametrize("forward_only", [True, False])
 def test_hybrid_class_for_scores_above_int16(forward_only):
-    """Near-identical long protein pairs (scores above int16) of different
-    lengths, in warps with short pairs: their strips run in s16x2 while the
-    strip bound holds, then each pair continues in s32.  Same results with
-    the hybrid class on and off, equal to the oracle."""
+    """Near-identical long protein pairs of different lengths, in warps with
+    short pairs.  Pairs rich in W and C score above the 16-bit lanes' range
+    (their main diagonal says so): their strips run in 16-bit lanes while
+    the strip bound holds, then each pair continues in s32.  Ordinary
+    near-identical pairs (scores between the signed and the unsigned 16-bit
+    range) stay in the 16-bit classes.  Same results with the hybrid class
+    on and off, equal to the oracle."""
     rng = np.random.default_rng(71)
     alpha = np.arange(20, dtype=np.uint8)
+    wc = np.array([oracle.encode("aa", "W")[0], oracle.encode("aa", "C")[0]], dtype=np.uint8)
     seqs_a, seqs_b = [], []
-    for la in (7000, 6500, 7300, 5000, 4100, 3600):
-        a = rng.choice(alpha, la).astype(np.uint8)
+    for la, al in ((7000, wc), (6900, wc), (7300, wc), (6500, alpha), (7200, alpha), (3600, alpha)):
+        a = rng.choice(al, la).astype(np.uint8)
         seqs_a.append(a)
-        seqs_b.append(_mutated(rng, a[: la - int(rng.integers(0, 300))], 0.01, alpha))
+        seqs_b.append(_mutated(rng, a[: la - int(rng.integers(0, 300))], 0.01, al))
     for la in (40, 300, 900):
         a = rng.choice(alpha, la).astype(np.uint8)
         seqs_a.append(a)
@@ -300,7 +310,7 @@ def test_hybrid_class_for_scores_above_int16(forward_only):
     sim = oracle.select_matrix("blosum62")
     want = oracle.sw_batch(codes, a_off, a_len, b_off, b_len, sim, -10, -1,
                            forward_only=forward_only)
-    assert (want[0] > 32767).sum() >= 3
+    assert (want[0] > U16_LIMIT).sum() >= 3 and ((want[0] > 32767) & (want[0] <= U16_LIMIT)).sum() >= 2
     for hyb in (1, 0):
         with _engine(case, forward_only, hybrid=hyb, time_launches=1) as e:
             got = e.compare(codes, pairs)
@@ -312,8 +322,8 @@ def test_hybrid_class_for_scores_above_int16(forward_only):
 
 def test_hybrid_class_switches_at_the_first_strip():
     """DNA scored +50/-40: the strip bound fails from the second strip on,
-    so long identical pairs switch to s32 right after strip 0 (and short
-    ones never leave s16x2)."""
+    so long identical pairs (scores above the 16-bit lanes' range) switch
+    to s32 right after strip 0, and short ones never leave 16-bit lanes."""
     rng = np.random.default_rng(72)
     acgt = np.array([1, 2, 3, 4], dtype=np.uint8)
     seqs_a, seqs_b = [], []
@@ -328,7 +338,7 @@ def test_hybrid_class_switches_at_the_first_strip():
     sim = oracle.select_matrix("na", 50, -40, -40)
     for fwd in (True, False):
         want = oracle.sw_batch(codes, a_off, a_len, b_off, b_len, sim, 0, -1, forward_only=fwd)
-        assert (want[0] > 32767).sum() >= 3
+        assert (want[0] > 65535 - 1024 - 50).sum() >= 3
         for hyb in (1, 0):
             with _engine(case, fwd, hybrid=hyb) as e:
                 got = e.compare(codes, pairs)
