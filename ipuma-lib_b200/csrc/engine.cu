@@ -1881,6 +1881,10 @@ int ipuma_gpu_compare_device(ipuma_engine* e, const uint8_t* d_codes, size_t n_c
 int ipuma_gpu_compare_device_packed(ipuma_engine* e, const uint8_t* d_packed, size_t n_codes, int32_t bits,
                                     const ipuma_pair* d_pairs, int32_t n, int32_t max_a_len, int32_t max_b_len,
                                     int32_t* d_score, int32_t* d_arange, int32_t* d_brange, void* stream) {
+  // Only packed widths here: 8 would read one byte per residue from a
+  // buffer the caller sized for packed codes.
+  if (bits != 2 && bits != 4 && bits != 5)
+    return fail(IPUMA_ERR_INVALID_ARG, "bits must be 2, 4 or 5, not %d", bits);
   return compare_dev(e, d_packed, n_codes, bits, d_pairs, n, max_a_len, max_b_len, d_score, d_arange, d_brange,
                      stream);
 }
