@@ -146,8 +146,8 @@ typedef struct ipuma_stats {
 } ipuma_stats;
 
 /* Kernel kinds reported in ipuma_stats.timed_kind.  S16_L<lanes>_K<k>:
- * 16-bit lanes (two pairs per lane group, each score held as score + 1024
- * in an unsigned halfword: scores up to 65535 - 1024 - max(sim)), <lanes>
+ * 16-bit lanes (two pairs per lane group, each score held as the signed
+ * halfword score - 31744: scores up to 65535 - 1024 - max(sim)), <lanes>
  * lanes per group, <k> A columns per lane. */
 #define IPUMA_KERNEL_S32_K16 0     /* s32 lanes, 32 lanes, 16 columns       */
 #define IPUMA_KERNEL_S16_L16_K4 1

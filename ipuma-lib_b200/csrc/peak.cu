@@ -1,8 +1,8 @@
 // peak.cu -- measures the integer/DPX issue peak that bounds the alignment
 // kernels: the instruction mix of one cell update of the wavefront classes
-// (biased unsigned 16-bit halves, two cells per instruction)
-//   1 x prmt (substitution bytes), 5 x viaddmax.u16x2 (F, F term of Y, Y,
-//   E, H), 1 x max.u16x2 (row maximum)
+// (biased 16-bit halves, two cells per instruction)
+//   1 x prmt (substitution bytes), 5 x viaddmax.s16x2 (F, F term of Y, Y,
+//   E, H), 1 x max.s16x2 (row maximum)
 // (7 instructions = 14 lane-ops, two cells), run as independent chains by
 // every thread of a full-occupancy grid.  Reported as lane-ops per second.
 #include <cuda_runtime.h>
@@ -18,7 +18,7 @@ constexpr int kChains = 8;
 constexpr int kIters = 4096;
 
 __global__ void __launch_bounds__(256) k_int_peak(uint32_t seed, uint32_t* sink) {
-  using T = ipuma_dev::LaneU16x2;
+  using T = ipuma_dev::Lane16;
   uint32_t e[kChains], f[kChains], h[kChains], w[kChains];
   const uint32_t g = T::delta(-1), go = T::delta(-2), floor0 = T::splat(0);
 #pragma unroll

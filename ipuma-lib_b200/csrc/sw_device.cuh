@@ -62,7 +62,7 @@ struct SwConst {
   int M;        // alphabet size (rows/cols of the substitution matrix)
   int forwardOnly;
   int s16Limit; // a pair whose score exceeds this is rerun in s32 (signed halves)
-  int u16Limit; // the same for the biased unsigned halves (LaneU16x2)
+  int u16Limit; // the same for the biased halves of the wavefront classes (LaneB16x2)
   int maxSub;   // largest substitution score (strip bound of the hybrid pass)
   int bits;     // bits per residue of the code array (8, or packed 2/4/5: code_at)
 };
@@ -156,37 +156,40 @@ struct LaneS16x2 {
   __device__ __forceinline__ static V shfl_up(V v) { return __shfl_up_sync(FULL, v, 1); }
 };
 
-// Two pairs per warp in biased unsigned 16-bit halves (pair P low, pair Q
-// high): a score v is held as v + BIAS in [0, 65535], so one lane covers
-// scores up to 65535 - BIAS - max(sim) -- twice the signed halfword's range
-// -- with the same instructions per cell.  Every stored value (H, Y, and E,
-// F shifted by -(gI + gE)) is >= 0, so it is >= BIAS when biased; a sum
-// with a profile byte (>= -128), gI + gE or gE (> -1000 on this path)
-// stays >= 0 and no halfword wraps below zero.  The floor 0 of the
-// recurrence is BIAS here: it is folded into the F term of Y (Cell::fterm),
-// so Y needs no relu.  The running best goes through the unsigned DPX max
-// with predicates (update_best).
-struct LaneU16x2 {
+// Two pairs per warp in biased 16-bit halves (pair P low, pair Q high): a
+// score v is held as the signed halfword v + BIAS - 32768, so the signed
+// range [-32768, 32767] covers scores [-BIAS, 65535 - BIAS] -- twice the
+// plain signed halfword's range -- with the same instructions per cell:
+// signed max orders the shifted values like the scores, and the sums are
+// the same modular adds.  Every stored value (H, Y, and E, F shifted by
+// -(gI + gE)) is >= 0, so it sits at least BIAS above the bottom of the
+// range; a sum with a profile byte (>= -128), gI + gE or gE (> -1000 on
+// this path) stays in range and no halfword wraps.  The floor 0 of the
+// recurrence is folded into the F term of Y (Cell::fterm), so Y needs no
+// relu.  The running best compares halves as signed integers
+// (update_best), since two halves may differ by more than 32767.
+struct LaneB16x2 {
   using V = uint32_t;
   static constexpr int NP = 2;
   static constexpr int BIAS = 1024;
+  static constexpr int OFFSET = BIAS - 32768;  // score -> stored halfword
   __device__ __forceinline__ static V splat(int x) {  // a score
-    const uint32_t v = (uint32_t)(x + BIAS) & 0xffffu;
+    const uint32_t v = (uint32_t)(x + OFFSET) & 0xffffu;
     return v | (v << 16);
   }
   __device__ __forceinline__ static V delta(int x) {  // an addend
     const uint32_t v = (uint32_t)x & 0xffffu;
     return v | (v << 16);
   }
-  __device__ __forceinline__ static V add(V a, V b) {  // mod 2^16 per half
+  __device__ __forceinline__ static V add(V a, V b) {
     V d;
     asm("add.s16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
     return d;
   }
-  __device__ __forceinline__ static V addmax(V a, V b, V c) { return __viaddmax_u16x2(a, b, c); }
+  __device__ __forceinline__ static V addmax(V a, V b, V c) { return __viaddmax_s16x2(a, b, c); }
   __device__ __forceinline__ static V max2(V a, V b) {
     V d;
-    asm("max.u16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    asm("max.s16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
     return d;
   }
   template <int C>
@@ -194,13 +197,13 @@ struct LaneU16x2 {
     return prmt(wp, wq, (uint32_t)(C | ((C | 8) << 4) | ((4 + C) << 8) | (((4 + C) | 8) << 12)));
   }
   __device__ __forceinline__ static int half(V v, int h) {
-    return (int)((h == 0) ? (v & 0xffffu) : (v >> 16)) - BIAS;
+    return (h == 0 ? (int)(int16_t)(v & 0xffffu) : (int)(int16_t)(v >> 16)) - OFFSET;
   }
   __device__ __forceinline__ static V shfl_up(V v) { return __shfl_up_sync(FULL, v, 1); }
 };
 
 // The 16-bit lane type of the engine's wavefront classes.
-using Lane16 = LaneU16x2;
+using Lane16 = LaneB16x2;
 
 // The pieces of one cell that differ between lane types.
 //   fterm(F̂, gI+gE)    the F term of Y: F̂ + gI + gE (with the floor 0 of
@@ -221,13 +224,13 @@ struct Cell {
   __device__ __forceinline__ static int limit(const SwConst& sc) { return sc.s16Limit; }
 };
 template <>
-struct Cell<LaneU16x2> {
-  using V = LaneU16x2::V;
+struct Cell<LaneB16x2> {
+  using V = LaneB16x2::V;
   __device__ __forceinline__ static V fterm(V f, V gIgE) {
-    return LaneU16x2::addmax(f, gIgE, LaneU16x2::splat(0));
+    return LaneB16x2::addmax(f, gIgE, LaneB16x2::splat(0));
   }
-  __device__ __forceinline__ static V ymax(V d, V s, V f) { return LaneU16x2::addmax(d, s, f); }
-  __device__ __forceinline__ static V delta(int x) { return LaneU16x2::delta(x); }
+  __device__ __forceinline__ static V ymax(V d, V s, V f) { return LaneB16x2::addmax(d, s, f); }
+  __device__ __forceinline__ static V delta(int x) { return LaneB16x2::delta(x); }
   __device__ __forceinline__ static int limit(const SwConst& sc) { return sc.u16Limit; }
 };
 
@@ -373,13 +376,14 @@ __device__ __forceinline__ uint32_t update_best(T, typename T::V& b, typename T:
   b = T::max2(b, rm);
   return keep;
 }
-// Biased unsigned halves differ by up to 65535, so the signed-difference
-// trick does not apply: the DPX max with predicates (b >= rm per half)
-// gives the new best and the keep mask in one instruction.
-__device__ __forceinline__ uint32_t update_best(LaneU16x2, uint32_t& b, uint32_t rm) {
-  bool hi, lo;
-  b = __vibmax_u16x2(b, rm, &hi, &lo);
-  return (lo ? 0x0000ffffu : 0u) | (hi ? 0xffff0000u : 0u);
+// Biased halves of two scores may differ by more than 32767, so the
+// signed-difference trick does not apply: each half is compared as a
+// signed integer (a half keeps its best and its snapshot while rm <= b).
+__device__ __forceinline__ uint32_t update_best(LaneB16x2, uint32_t& b, uint32_t rm) {
+  const uint32_t keep_lo = ((int16_t)(rm & 0xffffu) <= (int16_t)(b & 0xffffu)) ? 0x0000ffffu : 0u;
+  const uint32_t keep_hi = ((int16_t)(rm >> 16) <= (int16_t)(b >> 16)) ? 0xffff0000u : 0u;
+  b = LaneB16x2::max2(b, rm);
+  return keep_lo | keep_hi;
 }
 
 // -------------------------------------------------------------------------
