@@ -146,9 +146,8 @@ typedef struct ipuma_stats {
 } ipuma_stats;
 
 /* Kernel kinds reported in ipuma_stats.timed_kind.  S16_L<lanes>_K<k>:
- * 16-bit lanes (two pairs per lane group, each score held as the signed
- * halfword score - 31744: scores up to 65535 - 1024 - max(sim)), <lanes>
- * lanes per group, <k> A columns per lane. */
+ * s16x2 lanes (two pairs per lane group), <lanes> lanes per group, <k> A
+ * columns per lane. */
 #define IPUMA_KERNEL_S32_K16 0     /* s32 lanes, 32 lanes, 16 columns       */
 #define IPUMA_KERNEL_S16_L16_K4 1
 #define IPUMA_KERNEL_S16_L16_K8 2
@@ -169,7 +168,8 @@ typedef struct ipuma_stats {
 #define IPUMA_KERNEL_S16_L16_K11 17
 #define IPUMA_KERNEL_S16_L16_K13 18
 #define IPUMA_KERNEL_S16_L16_K15 19
-#define IPUMA_KERNEL_S16_HYBRID 20 /* 16-bit strips while safe, then s32 (scores past the 16-bit range) */
+#define IPUMA_KERNEL_S16_HYBRID 20 /* scores above int16: strips in biased 16-bit halves (score - 31744,
+                                      scores up to 65535 - 1024 - max(sim)) while safe, then s32 */
 #define IPUMA_KERNEL_PLAIN_S16 21  /* one-launch-per-batch wire kernel, 16-bit lanes */
 
 typedef struct ipuma_engine ipuma_engine;
@@ -211,9 +211,8 @@ void ipuma_gpu_destroy(ipuma_engine* e);
  *                 one-launch-per-batch kernel (wire-buffer API only)
  *   "plain_lanes" lanes of the plain kernel: 32 = one comparison slot per
  *                 warp in s32 lanes (default), 16 = two consecutive slots
- *                 per warp in the 16-bit halves of the batched classes, a
- *                 slot that could leave their range redone in s32 by the
- *                 same warp (IPUMA_KERNEL_PLAIN_S16)
+ *                 per warp in s16x2 halves, a slot that could leave int16
+ *                 redone in s32 by the same warp (IPUMA_KERNEL_PLAIN_S16)
  *   "graphs"      1 = capture and replay CUDA graphs for repeated shapes
  *   "tile_k"      0 = kernel class by |A| (default); 1..6 = every pair
  *                 through s16x2 class IPUMA_KERNEL_S16_* (value = kind),
@@ -229,10 +228,10 @@ void ipuma_gpu_destroy(ipuma_engine* e);
  *   "latency_share" share of the batch's modelled time (per mille,
  *                 default 60) one pair's item may take in its class; a
  *                 pair over it takes a class that finishes it sooner
- *   "hybrid"      1 = pairs whose score can pass the 16-bit lanes' range
- *                 run their strips in 16-bit lanes while a strip's values
- *                 provably fit, then in s32 (IPUMA_KERNEL_S16_HYBRID,
- *                 default); 0 = all in s32
+ *   "hybrid"      1 = pairs whose score can pass int16 run their strips
+ *                 in biased 16-bit halves while a strip's values provably
+ *                 fit, then in s32 (IPUMA_KERNEL_S16_HYBRID, default);
+ *                 0 = all in s32
  *   "thread_class" 1 = the per-thread class IPUMA_KERNEL_S16_T_K16 may be
  *                 chosen for pairs that are small relative to the batch,
  *                 0 = never (default) unless tile_k forces it

@@ -357,7 +357,7 @@ int max_batched_groups(ipuma_engine* e) {
   g = std::max(g, batched_grid<Lane16, 12, 32>(e));
   g = std::max(g, batched_grid<Lane16, 16, 32>(e));
   g = std::max(g, batched_grid<LaneS32, 16, 32>(e));
-  g = std::max(g, batched_grid<Lane16, 16, 32, true>(e));
+  g = std::max(g, batched_grid<LaneHi, 16, 32, true>(e));
   return g * kWarpsPerBlock;
 }
 
@@ -459,7 +459,7 @@ void class_grids(ipuma_engine* e, int maxA, int maxB, int* grid, long long* spb)
   const long long rowsCap = std::max(1, maxB);
   for (int c = 0; c < kNumClasses; ++c) {
     switch (c) {
-      case kClsHi: grid[c] = batched_grid<Lane16, 16, 32, true>(e); break;
+      case kClsHi: grid[c] = batched_grid<LaneHi, 16, 32, true>(e); break;
       case 0: grid[c] = batched_grid<Lane16, 4, 16>(e); break;
       case 1: grid[c] = batched_grid<Lane16, 8, 16>(e); break;
       case 2: grid[c] = batched_grid<Lane16, 12, 16>(e); break;
@@ -620,7 +620,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   bp.n_codes = (long long)n_codes;
   bp.bits = bits;
   bp.M = e->M;
-  bp.s16_limit = e->sc.u16Limit;
+  bp.s16_limit = e->sc.s16Limit;
   if ((rc = rb.flag->ensure((size_t)n + 64, s))) return rc;
   const int nkeys = bp.nclass * NBUCKET;
   const int tb = 256;
@@ -677,7 +677,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   }
   if ((enabled >> kClsHi) & 1u) {
     cudaStream_t cs = on(kClsHi);
-    if ((rc = launch_batched<Lane16, 16, 32, true>(e, sc, rb, cs, codes, pairs, list, R + 2 * kClsHi,
+    if ((rc = launch_batched<LaneHi, 16, 32, true>(e, sc, rb, cs, codes, pairs, list, R + 2 * kClsHi,
                                                       heads + kClsHi, rowsCap, score, arange, brange,
                                                       kClasses[kClsHi].kind, kClsHi, kClsHi)))
       return rc;
@@ -1464,15 +1464,16 @@ int ipuma_gpu_create(const ipuma_sw_config* sw, const ipuma_algo_config* algo, i
   e->fast_ok = (gI + gE < 0) && (gE <= 0) && (e->maxSub - (gI + gE) <= 127) &&
                (minSub - (gI + gE) >= -128) && (gI + gE > -1000) && (gE > -1000);
   // 16-bit lanes: H <= limit guarantees no halfword leaves its range (signed
-  // halves of the per-thread class: 32767 - maxSub; the biased unsigned
-  // halves of the wavefront classes: 65535 - bias - maxSub).  Pairs that
-  // may pass the wavefront classes' limit are checked by the binning pass.
+  // halves of the wavefront and per-thread classes: 32767 - maxSub; the
+  // biased halves of the hybrid class: 65535 - bias - maxSub).  The binning
+  // pass sends pairs whose main diagonal may pass the signed limit to the
+  // hybrid class.
   e->sc.s16Limit = 32767 - std::max(0, e->maxSub);
-  e->sc.u16Limit = 65535 - Lane16::BIAS - std::max(0, e->maxSub);
+  e->sc.u16Limit = 65535 - LaneHi::BIAS - std::max(0, e->maxSub);
   e->sc.maxSub = std::max(0, e->maxSub);
   e->sc.bits = 8;
   e->s16_ok = e->fast_ok;
-  e->s16_max_len = e->maxSub > 0 ? (e->sc.u16Limit / e->maxSub) : (1 << 30);
+  e->s16_max_len = e->maxSub > 0 ? (e->sc.s16Limit / e->maxSub) : (1 << 30);
   set_default_rates(e.get());
   max_batched_groups(e.get());  // warm the grid cache
   thread_threads<16>(e.get());

@@ -1,8 +1,8 @@
 // peak.cu -- measures the integer/DPX issue peak that bounds the alignment
 // kernels: the instruction mix of one cell update of the wavefront classes
-// (biased 16-bit halves, two cells per instruction)
-//   1 x prmt (substitution bytes), 5 x viaddmax.s16x2 (F, F term of Y, Y,
-//   E, H), 1 x max.s16x2 (row maximum)
+// (signed 16-bit halves, two cells per instruction)
+//   1 x prmt (substitution bytes), 4 x viaddmax.s16x2 (F, Y with relu, E,
+//   H), 1 x add.s16x2 (F term of Y), 1 x max.s16x2 (row maximum)
 // (7 instructions = 14 lane-ops, two cells), run as independent chains by
 // every thread of a full-occupancy grid.  Reported as lane-ops per second.
 #include <cuda_runtime.h>
@@ -20,7 +20,7 @@ constexpr int kIters = 4096;
 __global__ void __launch_bounds__(256) k_int_peak(uint32_t seed, uint32_t* sink) {
   using T = ipuma_dev::Lane16;
   uint32_t e[kChains], f[kChains], h[kChains], w[kChains];
-  const uint32_t g = T::delta(-1), go = T::delta(-2), floor0 = T::splat(0);
+  const uint32_t g = T::splat(-1), go = T::splat(-2);
 #pragma unroll
   for (int c = 0; c < kChains; ++c) {
     e[c] = seed ^ (threadIdx.x * 2654435761u) ^ c;
@@ -34,8 +34,8 @@ __global__ void __launch_bounds__(256) k_int_peak(uint32_t seed, uint32_t* sink)
     for (int c = 0; c < kChains; ++c) {
       const uint32_t sb = T::sub<1>(w[c], h[c]);          // prmt
       f[c] = T::addmax(f[c], g, h[c]);                    // F
-      const uint32_t ft = T::addmax(f[c], go, floor0);    // F term of Y
-      const uint32_t y = T::addmax(h[c], sb, ft);         // Y
+      const uint32_t ft = T::add(f[c], go);                // F term of Y
+      const uint32_t y = T::addmax_relu(h[c], sb, ft);     // Y
       e[c] = T::addmax(e[c], g, y);                       // E
       h[c] = T::addmax(e[c], go, y);                      // H
       rm = T::max2(rm, h[c]);                             // row maximum

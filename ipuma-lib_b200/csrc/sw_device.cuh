@@ -202,8 +202,13 @@ struct LaneB16x2 {
   __device__ __forceinline__ static V shfl_up(V v) { return __shfl_up_sync(FULL, v, 1); }
 };
 
-// The 16-bit lane type of the engine's wavefront classes.
-using Lane16 = LaneB16x2;
+// The 16-bit lanes of the engine's wavefront classes, and those of the
+// hybrid class, which takes the pairs whose score can pass the signed
+// halfword's range (its strips run in biased halves while their values
+// provably fit, then in s32).  The biased form costs one more add-max per
+// cell (the recurrence's floor), so the ordinary classes keep signed halves.
+using Lane16 = LaneS16x2;
+using LaneHi = LaneB16x2;
 
 // The pieces of one cell that differ between lane types.
 //   fterm(F̂, gI+gE)    the F term of Y: F̂ + gI + gE (with the floor 0 of
@@ -508,7 +513,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
     auto bnd = [&](int r) -> int2 {
       const int2 v = scrIn[r];
       if (HYB && NP == 1 && packedIn) {
-        return make_int2(Lane16::half((uint32_t)v.x, ctl->bndHalf), Lane16::half((uint32_t)v.y, ctl->bndHalf));
+        return make_int2(LaneHi::half((uint32_t)v.x, ctl->bndHalf), LaneHi::half((uint32_t)v.y, ctl->bndHalf));
       }
       return v;
     };

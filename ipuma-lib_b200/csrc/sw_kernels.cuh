@@ -185,7 +185,7 @@ __device__ __forceinline__ bool hybrid_pass(const SwConst& sc, uint8_t* s_prof, 
                                             uint16_t* s_bring, const PassSeq (&ps)[2], int2* scr,
                                             long rowsCap, Best (&out)[2]) {
   PassCtl c16;
-  if (!sw_pass<Lane16, K, 32, true>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, out, &c16)) return false;
+  if (!sw_pass<LaneHi, K, 32, true>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, out, &c16)) return false;
   if (c16.stoppedAt < 0) return true;
 #pragma unroll 1
   for (int h = 0; h < 2; ++h) {

@@ -45,16 +45,16 @@ EXPORTS = [
     "ipuma_gpu_compare_packed", "ipuma_pack_codes", "ipuma_gpu_compare_device_packed",
 ]
 
-KERNEL_NAMES = {0: "k_batched<s32,L32,K16>", 1: "k_batched<b16x2,L16,K4>",
-                2: "k_batched<b16x2,L16,K8>", 3: "k_batched<b16x2,L16,K12>",
-                4: "k_batched<b16x2,L16,K16>", 5: "k_batched<b16x2,L32,K12>",
-                6: "k_batched<b16x2,L32,K16>", 7: "k_batched<s32,L32,K16> rerun",
+KERNEL_NAMES = {0: "k_batched<s32,L32,K16>", 1: "k_batched<s16x2,L16,K4>",
+                2: "k_batched<s16x2,L16,K8>", 3: "k_batched<s16x2,L16,K12>",
+                4: "k_batched<s16x2,L16,K16>", 5: "k_batched<s16x2,L32,K12>",
+                6: "k_batched<s16x2,L32,K16>", 7: "k_batched<s32,L32,K16> rerun",
                 8: "k_plain<K>", 9: "k_exact", 10: "k_thread<s16x2,K16>",
-                11: "k_batched<b16x2,L16,K6>", 12: "k_batched<b16x2,L16,K10>",
-                13: "k_batched<b16x2,L16,K14>", 14: "k_batched<b16x2,L16,K5>",
-                15: "k_batched<b16x2,L16,K7>", 16: "k_batched<b16x2,L16,K9>",
-                17: "k_batched<b16x2,L16,K11>", 18: "k_batched<b16x2,L16,K13>",
-                19: "k_batched<b16x2,L16,K15>", 20: "k_hybrid<b16x2->s32,L32,K16>",
+                11: "k_batched<s16x2,L16,K6>", 12: "k_batched<s16x2,L16,K10>",
+                13: "k_batched<s16x2,L16,K14>", 14: "k_batched<s16x2,L16,K5>",
+                15: "k_batched<s16x2,L16,K7>", 16: "k_batched<s16x2,L16,K9>",
+                17: "k_batched<s16x2,L16,K11>", 18: "k_batched<s16x2,L16,K13>",
+                19: "k_batched<s16x2,L16,K15>", 20: "k_hybrid<b16x2->s32,L32,K16>",
                 21: "k_plain16<K>"}
 MAX_TIMED = 24  # IPUMA_MAX_TIMED
 

@@ -149,23 +149,23 @@ def test_protein_workload_sample(forward_only):
 
 def test_protein_mixed_with_s16_overflow():
     """Heavy-tailed protein lengths plus near-identical 7000+ residue pairs
-    whose scores exceed int16: they must come back exact (the wavefront
-    classes' biased unsigned 16-bit lanes hold them)."""
+    whose scores exceed int16: they must come back exact (the hybrid
+    class's biased 16-bit halves hold them)."""
     wl = workloads.protein_mixed(n=1_500, seed=13, long_identical_frac=0.004)
     got, want, st = _wl_run(wl, forward_only=False)
     _assert_same(got, want, wl.name)
     assert (want[0] > 32767).sum() >= 3
 
 
-# Largest score the wavefront classes' 16-bit lanes hold (BLOSUM62).
+# Largest score the hybrid class's biased 16-bit halves hold (BLOSUM62).
 U16_LIMIT = 65535 - 1024 - 11
 
 
 def test_s16_rerun_of_unpredicted_overflow():
     """A pair whose main diagonal looks unrelated (so it is not routed to
-    s32 lanes up front) but whose gapped score exceeds the 16-bit lanes'
-    range: the kernel gives up on the device and the pair is rerun in
-    32-bit."""
+    the hybrid class up front) but whose gapped score exceeds int16 (and
+    the biased halves' range): the s16x2 kernel gives up on the device and
+    the pair is rerun in 32-bit."""
     rng = np.random.default_rng(5)
     w, c = oracle.encode("aa", "W")[0], oracle.encode("aa", "C")[0]
     a = np.where(rng.random(7000) < 0.5, w, c).astype(np.uint8)
@@ -285,12 +285,12 @@ def _mutated(rng, seq, rate, alphabet):
 @pytest.mark.parametrize("forward_only", [True, False])
 def test_hybrid_class_for_scores_above_int16(forward_only):
     """Near-identical long protein pairs of different lengths, in warps with
-    short pairs.  Pairs rich in W and C score above the 16-bit lanes' range
-    (their main diagonal says so): their strips run in 16-bit lanes while
-    the strip bound holds, then each pair continues in s32.  Ordinary
-    near-identical pairs (scores between the signed and the unsigned 16-bit
-    range) stay in the 16-bit classes.  Same results with the hybrid class
-    on and off, equal to the oracle."""
+    short pairs; their main diagonal sends them to the hybrid class.
+    Ordinary near-identical pairs (scores between int16 and the biased
+    halves' range) run every strip in biased 16-bit halves; pairs rich in W
+    and C score above that range, so their strips run in biased halves
+    while the strip bound holds, then each pair continues in s32.  Same
+    results with the hybrid class on and off, equal to the oracle."""
     rng = np.random.default_rng(71)
     alpha = np.arange(20, dtype=np.uint8)
     wc = np.array([oracle.encode("aa", "W")[0], oracle.encode("aa", "C")[0]], dtype=np.uint8)
@@ -321,9 +321,9 @@ def test_hybrid_class_for_scores_above_int16(forward_only):
 
 
 def test_hybrid_class_switches_at_the_first_strip():
-    """DNA scored +50/-40: the strip bound fails from the second strip on,
-    so long identical pairs (scores above the 16-bit lanes' range) switch
-    to s32 right after strip 0, and short ones never leave 16-bit lanes."""
+    """DNA scored +50/-40: long identical pairs score above the biased
+    halves' range, so once the strip bound fails (after two strips) they
+    switch to s32, and short ones never leave 16-bit lanes."""
     rng = np.random.default_rng(72)
     acgt = np.array([1, 2, 3, 4], dtype=np.uint8)
     seqs_a, seqs_b = [], []
