@@ -503,7 +503,10 @@ size_t scratch_int2(ipuma_engine* e, int maxA, int maxB) {
 
 // Launch order of the classes (longest-tail classes first) and, for two
 // alternating streams, the stream (and scratch region) of each.
-constexpr int kLaunchOrder[kNumClasses] = {17, 16, 5, 4, 6, 3, 15, 9, 14, 2, 13, 8, 12, 1, 11, 7, 10, 0};
+// The hybrid class and the widest class (the long pairs of a heavy-tailed
+// batch) come first and land on different streams, so the widest class's
+// blocks start on the SMs the hybrid class frees during its tail.
+constexpr int kLaunchOrder[kNumClasses] = {17, 5, 16, 4, 6, 3, 15, 9, 14, 2, 13, 8, 12, 1, 11, 7, 10, 0};
 
 int reserve_bufs(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, int n, int maxA, int maxB) {
   int rc;
