@@ -46,10 +46,10 @@ LANE_OPS_PER_CELL = 7  # E: 2, F: 2, H: 2, running max: 1 (int lane-ops)
 METRIC = "bit-exact GCUPS (forward pass, score + end coordinates)"
 
 # DRAM bytes (read + write) per forward-pass cell of the dominant launch,
-# from one ncu capture of that kernel on a smaller case of the same workload
-# (profiles/: the launch reads the codes of its pairs once, so its traffic
-# scales with its cells).
-TRAFFIC_PER_CELL = {"dna_batched": 0.01098}
+# from one ncu capture of that kernel on the same workload
+# (profiles/k_batched_s16x2_L16_K15_dna_1m.md: a launch reads the codes of
+# its own pairs, so its traffic scales with its cells).
+TRAFFIC_PER_CELL = {"dna_batched": 0.00611}
 
 
 def parse(argv=None):
@@ -662,17 +662,19 @@ def main(argv=None):
             for _ in range(args.steps):
                 call()
             wall = max_over_ranks(dist, (time.perf_counter() - t0) / args.steps, dev)
-            return wall, int(db.eng.stats().chunks), bool(np.array_equal(out_np, got))
+            st = db.eng.stats()
+            return wall, int(st.chunks), bool(np.array_equal(out_np, got)), st
 
-        wall_b, chunks_b, same_b = time_call(run_bytes)
+        wall_b, chunks_b, same_b, _ = time_call(run_bytes)
         bytes_path = {"value": total_cells / wall_b / 1e9, "ms_per_step": wall_b * 1e3,
                       "h2d_bytes_per_step": int(wl.codes.nbytes + db.pairs_np.nbytes),
                       "bit_identical_to_device_run": same_b, "chunks": chunks_b,
                       "call": "ipuma_gpu_compare (one byte per residue)"}
-        wall, chunks, same = time_call(run_packed)
+        wall, chunks, same, st = time_call(run_packed)
         e2e = {"value": total_cells / wall / 1e9, "unit": "GCUPS",
                "h2d_bytes_per_step": int(packed_np.nbytes + db.pairs_np.nbytes),
                "d2h_bytes_per_step": int(3 * 4 * wl.n), "ms_per_step": wall * 1e3,
+               "last_call_device_span_ms": st.total_ms,  # first copy to last result, CUDA events
                "bit_identical_to_device_run": same, "chunks": chunks,
                "call": "ipuma_gpu_compare_packed (%d-bit codes, read packed by the kernels)" % bits,
                "bytes_path": bytes_path}

@@ -238,7 +238,7 @@ struct ipuma_engine {
   cudaStream_t stream2 = nullptr, copy_stream = nullptr;
   cudaEvent_t cev[2 * kMaxChunks + 2] = {};
   int chunks = 0;  // option "chunks": 0 automatic, 1 off, n fixed
-  std::map<const void*, std::pair<int, int>> grid_cache;  // kernel -> {smem, grid}
+  std::map<std::pair<const void*, int>, int> grid_cache;  // {kernel, smem} -> grid
   // Captured pipelines of compare_device, by shape and buffers (option "graphs").
   std::map<std::vector<uint64_t>, cudaGraphExec_t> graphs_cache;
   std::map<cudaGraphExec_t, int> graph_launches;
@@ -303,28 +303,35 @@ void raise_smem_limit(int device, K kernel, int smem) {
 // occupancy query or attribute change happens during a graph capture).
 template <class K>
 int occupancy_grid(ipuma_engine* e, K kernel, int smem) {
-  const void* key = reinterpret_cast<const void*>(kernel);
+  const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), smem);
   auto it = e->grid_cache.find(key);
-  if (it != e->grid_cache.end() && it->second.first == smem) return it->second.second;
+  if (it != e->grid_cache.end()) return it->second;
   int nb = 0;
   raise_smem_limit(e->device, kernel, smem);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, kThreads, smem);
   if (nb < 1) nb = 1;
-  e->grid_cache[key] = {smem, nb * e->nsm};
+  e->grid_cache[key] = nb * e->nsm;
   return nb * e->nsm;
 }
 
+// Letters of the query profile for codes of `bits` bits: 2-bit codes are
+// A/C/G/T (codes 1..4), so their profile needs four rows, not one per
+// letter of the alphabet -- less shared memory, more resident blocks.
+int prof_letters(const ipuma_engine* e, int bits) { return (bits == 2 && e->M >= 5) ? 4 : e->M; }
+
+// Shared memory of a wavefront launch whose profile has P letters (P < 0:
+// one per letter of the alphabet).
 template <class T, int K, int LANES>
-int smem_for(const ipuma_engine* e) {
-  return SmemLayout<T, K, LANES>::total(e->M, kWarpsPerBlock);
+int smem_for(const ipuma_engine* e, int P = -1) {
+  return SmemLayout<T, K, LANES>::total(e->M, P < 0 ? e->M : P, kWarpsPerBlock);
 }
 
 // Grid of a k_batched<T, K, LANES, HYB> launch (the instantiation for the
-// engine's forwardOnly, which is fixed at creation).
+// engine's forwardOnly, which is fixed at creation) with a P-letter profile.
 template <class T, int K, int LANES, bool HYB = false>
-int batched_grid(ipuma_engine* e) {
-  return e->sc.forwardOnly ? occupancy_grid(e, k_batched<T, K, LANES, HYB, true>, smem_for<T, K, LANES>(e))
-                           : occupancy_grid(e, k_batched<T, K, LANES, HYB, false>, smem_for<T, K, LANES>(e));
+int batched_grid(ipuma_engine* e, int P) {
+  return e->sc.forwardOnly ? occupancy_grid(e, k_batched<T, K, LANES, HYB, true>, smem_for<T, K, LANES>(e, P))
+                           : occupancy_grid(e, k_batched<T, K, LANES, HYB, false>, smem_for<T, K, LANES>(e, P));
 }
 
 template <int K>
@@ -338,26 +345,29 @@ long thread_threads(ipuma_engine* e) {
   return (long)occupancy_grid(e, k_thread<K>, thread_smem<K>(e)) * kThreads;
 }
 
-// Lane groups (one scratch slice each) of the widest batched launch.
+// Lane groups (one scratch slice each) of the widest batched launch (either
+// profile size).
 int max_batched_groups(ipuma_engine* e) {
   int g = 0;
-  g = std::max(g, batched_grid<Lane16, 4, 16>(e) * 2);
-  g = std::max(g, batched_grid<Lane16, 8, 16>(e) * 2);
-  g = std::max(g, batched_grid<Lane16, 12, 16>(e) * 2);
-  g = std::max(g, batched_grid<Lane16, 16, 16>(e) * 2);
-  g = std::max(g, batched_grid<Lane16, 6, 16>(e) * 2);
-  g = std::max(g, batched_grid<Lane16, 10, 16>(e) * 2);
-  g = std::max(g, batched_grid<Lane16, 14, 16>(e) * 2);
-  g = std::max(g, batched_grid<Lane16, 5, 16>(e) * 2);
-  g = std::max(g, batched_grid<Lane16, 7, 16>(e) * 2);
-  g = std::max(g, batched_grid<Lane16, 9, 16>(e) * 2);
-  g = std::max(g, batched_grid<Lane16, 11, 16>(e) * 2);
-  g = std::max(g, batched_grid<Lane16, 13, 16>(e) * 2);
-  g = std::max(g, batched_grid<Lane16, 15, 16>(e) * 2);
-  g = std::max(g, batched_grid<Lane16, 12, 32>(e));
-  g = std::max(g, batched_grid<Lane16, 16, 32>(e));
-  g = std::max(g, batched_grid<LaneS32, 16, 32>(e));
-  g = std::max(g, batched_grid<LaneHi, 16, 32, true>(e));
+  for (int P : {e->M, prof_letters(e, 2)}) {
+    g = std::max(g, batched_grid<Lane16, 4, 16>(e, P) * 2);
+    g = std::max(g, batched_grid<Lane16, 8, 16>(e, P) * 2);
+    g = std::max(g, batched_grid<Lane16, 12, 16>(e, P) * 2);
+    g = std::max(g, batched_grid<Lane16, 16, 16>(e, P) * 2);
+    g = std::max(g, batched_grid<Lane16, 6, 16>(e, P) * 2);
+    g = std::max(g, batched_grid<Lane16, 10, 16>(e, P) * 2);
+    g = std::max(g, batched_grid<Lane16, 14, 16>(e, P) * 2);
+    g = std::max(g, batched_grid<Lane16, 5, 16>(e, P) * 2);
+    g = std::max(g, batched_grid<Lane16, 7, 16>(e, P) * 2);
+    g = std::max(g, batched_grid<Lane16, 9, 16>(e, P) * 2);
+    g = std::max(g, batched_grid<Lane16, 11, 16>(e, P) * 2);
+    g = std::max(g, batched_grid<Lane16, 13, 16>(e, P) * 2);
+    g = std::max(g, batched_grid<Lane16, 15, 16>(e, P) * 2);
+    g = std::max(g, batched_grid<Lane16, 12, 32>(e, P));
+    g = std::max(g, batched_grid<Lane16, 16, 32>(e, P));
+    g = std::max(g, batched_grid<LaneS32, 16, 32>(e, P));
+    g = std::max(g, batched_grid<LaneHi, 16, 32, true>(e, P));
+  }
   return g * kWarpsPerBlock;
 }
 
@@ -403,8 +413,8 @@ template <class T, int K, int LANES, bool HYB = false>
 int launch_batched(ipuma_engine* e, const SwConst& sc, const RunBufs& rb, cudaStream_t s, const uint8_t* codes,
                    const PairDesc* pairs, const int* list, const int* range, int* head, long rowsCap,
                    int* score, int* arange, int* brange, int kind, int cls, int allot_idx) {
-  const int smem = smem_for<T, K, LANES>(e);
-  const int grid = batched_grid<T, K, LANES, HYB>(e);
+  const int smem = smem_for<T, K, LANES>(e, sc.P);
+  const int grid = batched_grid<T, K, LANES, HYB>(e, sc.P);
   int* ctl = rb.ctl;
   auto* cells = reinterpret_cast<unsigned long long*>(ctl + CTL_CELLS);
   int rc;
@@ -454,29 +464,30 @@ long thread_rows(const ipuma_engine* e, int maxA, int maxB) {
 // Strip-boundary scratch (int2) of one run: the wavefront classes need two
 // columns of rowsCap per lane group, the per-thread class one column of
 // thread_rows per thread.
-// Full-occupancy grid and strip scratch (int2) per block of every class.
-void class_grids(ipuma_engine* e, int maxA, int maxB, int* grid, long long* spb) {
+// Full-occupancy grid and strip scratch (int2) per block of every class,
+// for a P-letter profile.
+void class_grids(ipuma_engine* e, int P, int maxA, int maxB, int* grid, long long* spb) {
   const long long rowsCap = std::max(1, maxB);
   for (int c = 0; c < kNumClasses; ++c) {
     switch (c) {
-      case kClsHi: grid[c] = batched_grid<LaneHi, 16, 32, true>(e); break;
-      case 0: grid[c] = batched_grid<Lane16, 4, 16>(e); break;
-      case 1: grid[c] = batched_grid<Lane16, 8, 16>(e); break;
-      case 2: grid[c] = batched_grid<Lane16, 12, 16>(e); break;
-      case 3: grid[c] = batched_grid<Lane16, 16, 16>(e); break;
-      case 4: grid[c] = batched_grid<Lane16, 12, 32>(e); break;
-      case 5: grid[c] = batched_grid<Lane16, 16, 32>(e); break;
+      case kClsHi: grid[c] = batched_grid<LaneHi, 16, 32, true>(e, P); break;
+      case 0: grid[c] = batched_grid<Lane16, 4, 16>(e, P); break;
+      case 1: grid[c] = batched_grid<Lane16, 8, 16>(e, P); break;
+      case 2: grid[c] = batched_grid<Lane16, 12, 16>(e, P); break;
+      case 3: grid[c] = batched_grid<Lane16, 16, 16>(e, P); break;
+      case 4: grid[c] = batched_grid<Lane16, 12, 32>(e, P); break;
+      case 5: grid[c] = batched_grid<Lane16, 16, 32>(e, P); break;
       case kClsThread: grid[c] = (int)(thread_threads<16>(e) / kThreads); break;
-      case 7: grid[c] = batched_grid<Lane16, 6, 16>(e); break;
-      case 8: grid[c] = batched_grid<Lane16, 10, 16>(e); break;
-      case 9: grid[c] = batched_grid<Lane16, 14, 16>(e); break;
-      case 10: grid[c] = batched_grid<Lane16, 5, 16>(e); break;
-      case 11: grid[c] = batched_grid<Lane16, 7, 16>(e); break;
-      case 12: grid[c] = batched_grid<Lane16, 9, 16>(e); break;
-      case 13: grid[c] = batched_grid<Lane16, 11, 16>(e); break;
-      case 14: grid[c] = batched_grid<Lane16, 13, 16>(e); break;
-      case 15: grid[c] = batched_grid<Lane16, 15, 16>(e); break;
-      default: grid[c] = batched_grid<LaneS32, 16, 32>(e); break;
+      case 7: grid[c] = batched_grid<Lane16, 6, 16>(e, P); break;
+      case 8: grid[c] = batched_grid<Lane16, 10, 16>(e, P); break;
+      case 9: grid[c] = batched_grid<Lane16, 14, 16>(e, P); break;
+      case 10: grid[c] = batched_grid<Lane16, 5, 16>(e, P); break;
+      case 11: grid[c] = batched_grid<Lane16, 7, 16>(e, P); break;
+      case 12: grid[c] = batched_grid<Lane16, 9, 16>(e, P); break;
+      case 13: grid[c] = batched_grid<Lane16, 11, 16>(e, P); break;
+      case 14: grid[c] = batched_grid<Lane16, 13, 16>(e, P); break;
+      case 15: grid[c] = batched_grid<Lane16, 15, 16>(e, P); break;
+      default: grid[c] = batched_grid<LaneS32, 16, 32>(e, P); break;
     }
     if (c == kClsThread)
       spb[c] = (long long)kThreads * thread_rows(e, maxA, maxB);
@@ -492,11 +503,15 @@ void class_grids(ipuma_engine* e, int maxA, int maxB, int* grid, long long* spb)
 size_t scratch_int2(ipuma_engine* e, int maxA, int maxB) {
   int grid[NCLASS_MAX + 1];
   long long spb[NCLASS_MAX + 1];
-  class_grids(e, maxA, maxB, grid, spb);
   long long full = 0, round = 0;
-  for (int c = 0; c < kNumClasses; ++c) {
-    full = std::max(full, (long long)grid[c] * spb[c]);
-    round += spb[c];
+  for (int P : {e->M, prof_letters(e, 2)}) {  // the smaller profile may fit more blocks
+    class_grids(e, P, maxA, maxB, grid, spb);
+    long long r = 0;
+    for (int c = 0; c < kNumClasses; ++c) {
+      full = std::max(full, (long long)grid[c] * spb[c]);
+      r += spb[c];
+    }
+    round = std::max(round, r);
   }
   return (size_t)std::max(full + round, 2 * full);
 }
@@ -537,6 +552,8 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   DevStatus* st = reinterpret_cast<DevStatus*>(ctl + CTL_STATUS);
   SwConst sc = e->sc;
   sc.bits = bits;
+  sc.P = prof_letters(e, bits);
+  sc.pshift = sc.P == e->M ? 0 : 1;
 
   if (!e->fast_ok) {
     // Exact per-thread kernel; C and F rows in global scratch.
@@ -593,7 +610,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   if (e->thread_class && bits == 8) enabled |= 1u << kClsThread;  // k_thread reads bytes only
   if (e->tile_k > 0) enabled |= 1u << (e->tile_k - 1);
   bp.enabled = enabled;
-  class_grids(e, maxA, maxB, bp.grid, bp.scr_per_block);
+  class_grids(e, sc.P, maxA, maxB, bp.grid, bp.scr_per_block);
   bp.scr_cap = (long long)(rb.scratch->cap / sizeof(int2));
   float slot_min = 1e30f;
   for (int c = 0; c < kNumS16; ++c) {
@@ -1030,21 +1047,21 @@ int run_autotune(ipuma_engine* e, const char* cache_path) {
     const int rounds = L > 0 ? 6 : 2;
     int grid = 1;
     switch (c) {
-      case 0: grid = batched_grid<Lane16, 4, 16>(e); break;
-      case 1: grid = batched_grid<Lane16, 8, 16>(e); break;
-      case 2: grid = batched_grid<Lane16, 12, 16>(e); break;
-      case 3: grid = batched_grid<Lane16, 16, 16>(e); break;
-      case 4: grid = batched_grid<Lane16, 12, 32>(e); break;
-      case 5: grid = batched_grid<Lane16, 16, 32>(e); break;
-      case 7: grid = batched_grid<Lane16, 6, 16>(e); break;
-      case 8: grid = batched_grid<Lane16, 10, 16>(e); break;
-      case 9: grid = batched_grid<Lane16, 14, 16>(e); break;
-      case 10: grid = batched_grid<Lane16, 5, 16>(e); break;
-      case 11: grid = batched_grid<Lane16, 7, 16>(e); break;
-      case 12: grid = batched_grid<Lane16, 9, 16>(e); break;
-      case 13: grid = batched_grid<Lane16, 11, 16>(e); break;
-      case 14: grid = batched_grid<Lane16, 13, 16>(e); break;
-      case 15: grid = batched_grid<Lane16, 15, 16>(e); break;
+      case 0: grid = batched_grid<Lane16, 4, 16>(e, e->M); break;
+      case 1: grid = batched_grid<Lane16, 8, 16>(e, e->M); break;
+      case 2: grid = batched_grid<Lane16, 12, 16>(e, e->M); break;
+      case 3: grid = batched_grid<Lane16, 16, 16>(e, e->M); break;
+      case 4: grid = batched_grid<Lane16, 12, 32>(e, e->M); break;
+      case 5: grid = batched_grid<Lane16, 16, 32>(e, e->M); break;
+      case 7: grid = batched_grid<Lane16, 6, 16>(e, e->M); break;
+      case 8: grid = batched_grid<Lane16, 10, 16>(e, e->M); break;
+      case 9: grid = batched_grid<Lane16, 14, 16>(e, e->M); break;
+      case 10: grid = batched_grid<Lane16, 5, 16>(e, e->M); break;
+      case 11: grid = batched_grid<Lane16, 7, 16>(e, e->M); break;
+      case 12: grid = batched_grid<Lane16, 9, 16>(e, e->M); break;
+      case 13: grid = batched_grid<Lane16, 11, 16>(e, e->M); break;
+      case 14: grid = batched_grid<Lane16, 13, 16>(e, e->M); break;
+      case 15: grid = batched_grid<Lane16, 15, 16>(e, e->M); break;
       default: grid = (int)(thread_threads<16>(e) / kThreads); break;
     }
     const int minPairs = grid * kWarpsPerBlock * perItem * rounds;
@@ -1475,6 +1492,8 @@ int ipuma_gpu_create(const ipuma_sw_config* sw, const ipuma_algo_config* algo, i
   e->sc.u16Limit = 65535 - LaneHi::BIAS - std::max(0, e->maxSub);
   e->sc.maxSub = std::max(0, e->maxSub);
   e->sc.bits = 8;
+  e->sc.P = m;
+  e->sc.pshift = 0;
   e->s16_ok = e->fast_ok;
   e->s16_max_len = e->maxSub > 0 ? (e->sc.s16Limit / e->maxSub) : (1 << 30);
   set_default_rates(e.get());

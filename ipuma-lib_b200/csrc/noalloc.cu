@@ -68,9 +68,9 @@ __global__ void __launch_bounds__(64) k_noalloc(SwConst sc, SimParam sim, const 
   const int wib = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   int8_t* s_simp = reinterpret_cast<int8_t*>(smem);
-  uint8_t* wbase = smem + L::simp_bytes(sc.M) + wib * L::warp_bytes(sc.M);
+  uint8_t* wbase = smem + L::simp_bytes(sc.M) + wib * L::warp_bytes(sc.P);
   uint8_t* s_prof = wbase;
-  uint16_t* s_bring = reinterpret_cast<uint16_t*>(wbase + L::prof_bytes(sc.M));
+  uint16_t* s_bring = reinterpret_cast<uint16_t*>(wbase + L::prof_bytes(sc.P));
   const int M = sc.M;
   for (int k = threadIdx.x; k < M * (M + 1); k += blockDim.x) {
     const int a = k / (M + 1), x = k % (M + 1);
@@ -168,6 +168,8 @@ extern "C" int ipuma_gpu_compare_noalloc(const ipuma_sw_config* sw, int32_t forw
   sc.s16Limit = 32767;  // (16-bit lanes are not used here)
   sc.u16Limit = 32767;
   sc.bits = 8;  // one byte per residue
+  sc.P = m;     // a profile row per letter
+  sc.pshift = 0;
   // Warps that fit the static scratch at this row count (2 rows per B row).
   const long rowsCap = max_b_len;
   const long warpsFit = kScratchInt2 / (2 * rowsCap);
@@ -175,7 +177,7 @@ extern "C" int ipuma_gpu_compare_noalloc(const ipuma_sw_config* sw, int32_t forw
   // blocks of kWarps warps never index past the array.
   const long warps = std::max<long>(kWarps, std::min<long>({warpsFit, (long)ds->nsm * 16, (long)n}));
   const int blocks = (int)(warps / kWarps);
-  const int smem = SmemLayout<LaneS32, 16, 32>::total(m, kWarps);
+  const int smem = SmemLayout<LaneS32, 16, 32>::total(m, m, kWarps);
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (cudaMemsetAsync(ds->status, 0, sizeof(DevStatus), s) != cudaSuccess)
     return fail(IPUMA_ERR_CUDA, "clearing the status word failed");

@@ -65,6 +65,8 @@ struct SwConst {
   int u16Limit; // the same for the biased halves of the wavefront classes (LaneB16x2)
   int maxSub;   // largest substitution score (strip bound of the hybrid pass)
   int bits;     // bits per residue of the code array (8, or packed 2/4/5: code_at)
+  int P;        // letters of the query profile (M, or 4 for 2-bit A/C/G/T codes)
+  int pshift;   // profile row of a code: code - pshift (1 for 2-bit codes, else 0)
 };
 
 // Control of a hybrid pass (sw_pass with HYB): an s16x2 pass that stops
@@ -122,6 +124,7 @@ struct LaneS32 {
     return (int)prmt(wp, 0u, (uint32_t)(C | ((C | 8) << 4) | ((C | 8) << 8) | ((C | 8) << 12)));
   }
   __device__ __forceinline__ static int half(V v, int /*h*/) { return v; }
+  __device__ __forceinline__ static V pack2(int lo, int /*hi*/) { return lo; }
   __device__ __forceinline__ static V shfl_up(V v) { return __shfl_up_sync(FULL, v, 1); }
 };
 
@@ -152,6 +155,9 @@ struct LaneS16x2 {
   }
   __device__ __forceinline__ static int half(V v, int h) {
     return h == 0 ? (int)(int16_t)(v & 0xffff) : (int)(int16_t)(v >> 16);
+  }
+  __device__ __forceinline__ static V pack2(int lo, int hi) {
+    return (uint32_t)(lo & 0xffff) | ((uint32_t)(hi & 0xffff) << 16);
   }
   __device__ __forceinline__ static V shfl_up(V v) { return __shfl_up_sync(FULL, v, 1); }
 };
@@ -198,6 +204,9 @@ struct LaneB16x2 {
   }
   __device__ __forceinline__ static int half(V v, int h) {
     return (h == 0 ? (int)(int16_t)(v & 0xffffu) : (int)(int16_t)(v >> 16)) - OFFSET;
+  }
+  __device__ __forceinline__ static V pack2(int lo, int hi) {  // two scores
+    return ((uint32_t)(lo + OFFSET) & 0xffffu) | (((uint32_t)(hi + OFFSET) & 0xffffu) << 16);
   }
   __device__ __forceinline__ static V shfl_up(V v) { return __shfl_up_sync(FULL, v, 1); }
 };
@@ -258,6 +267,33 @@ __device__ __forceinline__ int code_at(const uint8_t* base, long long idx, int b
   return bits == 2 ? x + 1 : x;
 }
 
+// Sequential reader of residues idx, idx + 1, ... of a packed code array
+// (bits = 2, 4 or 5, layout as in code_at): one 32-bit load per word of the
+// stream, each word loaded only once the next residue reaches into it.
+struct PackedStream {
+  const uint32_t* w;  // next word to load
+  uint64_t buf;       // bits not yet consumed, lowest first
+  int nbuf;           // valid bits in buf
+  int bits;
+  __device__ __forceinline__ PackedStream(const uint8_t* base, long long idx, int bits_) : bits(bits_) {
+    const long long bit = idx * bits;
+    w = reinterpret_cast<const uint32_t*>(base) + (bit >> 5);
+    const int skip = (int)(bit & 31);
+    buf = (uint64_t)__ldg(w++) >> skip;
+    nbuf = 32 - skip;
+  }
+  __device__ __forceinline__ int next() {
+    if (nbuf < bits) {
+      buf |= (uint64_t)__ldg(w++) << nbuf;
+      nbuf += 32;
+    }
+    const int x = (int)(buf & ((1u << bits) - 1u));
+    buf >>= bits;
+    nbuf -= bits;
+    return bits == 2 ? x + 1 : x;
+  }
+};
+
 // One sequence pair as seen by a pass: A[j] = residue a + j * da and
 // B[i] = residue b + i * db of the code array at `base` (bits per residue
 // in SwConst).  The reverse pass reads A[Aend..0] and B[Bend..0] with
@@ -285,8 +321,10 @@ __device__ __forceinline__ bool better(int s1, int i1, int j1, int s2, int i2, i
 // -------------------------------------------------------------------------
 // Query profile of one group's strip: lane l's K columns of letter x at
 // prof[x * LANES * KP + l * KP + c] = sim[A[col0 + l * K + c]][x] as int8,
-// KP = K rounded up to whole 32-bit words (bytes c >= K are unused).  Row M
-// (the padding letter) and columns past |A| hold SUB_PAD.
+// KP = K rounded up to whole 32-bit words (bytes c >= K are unused).  The
+// profile has P + 1 rows: row x < P is letter x + pshift (2-bit A/C/G/T
+// codes need only the rows of codes 1..4), row P (the padding letter) and
+// columns past |A| hold SUB_PAD.
 // -------------------------------------------------------------------------
 template <int K>
 struct ProfileWords {
@@ -295,9 +333,10 @@ struct ProfileWords {
 };
 
 template <int K, int LANES>
-__device__ __forceinline__ void build_profile(uint8_t* prof, const int8_t* s_simp, int M, int bits,
+__device__ __forceinline__ void build_profile(uint8_t* prof, const int8_t* s_simp, const SwConst& sc,
                                               const PassSeq& ps, int col0, int lane) {
   // s_simp[a * (M + 1) + x] = sim[a][x] and SUB_PAD for x == M.
+  const int M = sc.M, P = sc.P, bits = sc.bits;
   constexpr int KP = ProfileWords<K>::KP;
   constexpr int SWP = LANES * KP;
   int acode[KP];
@@ -306,14 +345,15 @@ __device__ __forceinline__ void build_profile(uint8_t* prof, const int8_t* s_sim
     const int col = col0 + lane * K + c;
     acode[c] = (c < K && col < ps.alen) ? code_at(ps.base, ps.a + (long long)col * ps.da, bits) : -1;
   }
-  for (int x = 0; x <= M; ++x) {
+  for (int x = 0; x <= P; ++x) {
+    const int xs = x < P ? x + sc.pshift : M;  // column of s_simp
 #pragma unroll
     for (int w = 0; w < KP / 4; ++w) {
       uint32_t word = 0;
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const int a = acode[4 * w + q];
-        const int v = (a >= 0) ? (int)s_simp[a * (M + 1) + x] : SUB_PAD;
+        const int v = (a >= 0) ? (int)s_simp[a * (M + 1) + xs] : SUB_PAD;
         word |= ((uint32_t)(uint8_t)(int8_t)v) << (8 * q);
       }
       *reinterpret_cast<uint32_t*>(prof + x * SWP + lane * KP + 4 * w) = word;
@@ -391,6 +431,22 @@ __device__ __forceinline__ uint32_t update_best(LaneB16x2, uint32_t& b, uint32_t
   return keep_lo | keep_hi;
 }
 
+// Raises each lane's running best to the best of its group (per pair)
+// minus one.  A row maximum strictly below a score that some cell of the
+// pair already holds can never be the pair's answer, so after the raise
+// only rows that can still win (ties included: the row order decides
+// those) pass update_best and take the snapshot blend.  A lane left at the
+// raised value holds no cell of that score, and its best stays below the
+// group's, so it never wins the group reduction at the end of the strip.
+template <class T, int LANES>
+__device__ __forceinline__ typename T::V raise_to_group(typename T::V best) {
+  typename T::V g = best;
+#pragma unroll
+  for (int off = LANES / 2; off > 0; off >>= 1)
+    g = T::max2(g, (typename T::V)__shfl_xor_sync(FULL, g, off, LANES));
+  return T::max2(best, T::add(g, Cell<T>::delta(-1)));
+}
+
 // -------------------------------------------------------------------------
 // One full pass (forward or reverse) of one warp.
 //
@@ -405,7 +461,7 @@ __device__ __forceinline__ uint32_t update_best(LaneB16x2, uint32_t& b, uint32_t
 // the lane's limit (Cell::limit, checked every 32 steps, warp-uniformly); the caller reruns
 // the warp's pairs in s32 lanes.
 //
-//   s_prof   : this group's profile area, NP * (M + 1) * LANES * K bytes
+//   s_prof   : this group's profile area, NP * (P + 1) * LANES * KP bytes
 //   s_simp   : substitution table with the padding column (build_profile)
 //   s_bring  : this group's 64-entry ring of B letters (P low byte, Q high)
 //   scr      : this group's scratch, 2 * rowsCap int2 (only used when the
@@ -428,8 +484,8 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
   constexpr int SWP = LANES * KP;        // profile bytes per letter
   constexpr int NP = T::NP;
   const int lane = threadIdx.x & (LANES - 1);
-  const int M = sc.M;
-  const int profStride = (M + 1) * SWP;
+  const int P = sc.P;
+  const int profStride = (P + 1) * SWP;
 
   const int strip0 = HYB ? ctl->strip0 : 0;
   int rowsG = 0, amax = 0;
@@ -521,7 +577,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
     __syncwarp();
 #pragma unroll
     for (int h = 0; h < NP; ++h)
-      build_profile<K, LANES>(s_prof + h * profStride, s_simp, M, sc.bits, ps[h], col0, lane);
+      build_profile<K, LANES>(s_prof + h * profStride, s_simp, sc, ps[h], col0, lane);
     __threadfence_block();
     __syncwarp();
 
@@ -533,7 +589,9 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
       snap[c] = vZero;
     }
     V outY = vZero, outE = vE0, diagIn = vZero;
-    V best = vZero;
+    // Running best of the lane, started one below the pair's best of the
+    // strips before (a cell that ties it can still win on its row).
+    V best = T::pack2(max(out[0].s - 1, 0), max(out[NP - 1].s - 1, 0));
     // Row of each lane's best, one halfword per pair (rows < 65536).
     uint32_t brow = 0;
 
@@ -552,7 +610,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
       uint32_t v = 0;
 #pragma unroll
       for (int h = 0; h < NP; ++h) {
-        const int x = (r < ps[h].blen) ? code_at(ps[h].base, ps[h].b + (long long)r * ps[h].db, sc.bits) : M;
+        const int x = (r < ps[h].blen) ? code_at(ps[h].base, ps[h].b + (long long)r * ps[h].db, sc.bits) - sc.pshift : P;
         v |= (uint32_t)x << (8 * h);
       }
       return v;
@@ -666,6 +724,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
           }
         }
       }
+      if (t0 > 0) best = raise_to_group<T, LANES>(best);
       s_bring[(t0 + lane) & 63] = (uint16_t)bnext;
       bnext = fetch_letters(t0 + LANES + lane);
       __syncwarp();

@@ -91,12 +91,13 @@ template <class T, int K, int LANES>
 struct SmemLayout {
   static constexpr int SW = LANES * K;
   static constexpr int GROUPS = 32 / LANES;
+  // M = alphabet size (substitution table), P = letters of the profile.
   __host__ __device__ static int simp_bytes(int M) { return ((M * (M + 1)) + 15) & ~15; }
-  __host__ __device__ static int prof_bytes(int M) { return T::NP * (M + 1) * LANES * ProfileWords<K>::KP; }
+  __host__ __device__ static int prof_bytes(int P) { return T::NP * (P + 1) * LANES * ProfileWords<K>::KP; }
   __host__ __device__ static int ring_bytes() { return 64 * 2; }
-  __host__ __device__ static int group_bytes(int M) { return (prof_bytes(M) + ring_bytes() + 15) & ~15; }
-  __host__ __device__ static int warp_bytes(int M) { return GROUPS * group_bytes(M); }
-  __host__ __device__ static int total(int M, int warps) { return simp_bytes(M) + warps * warp_bytes(M); }
+  __host__ __device__ static int group_bytes(int P) { return (prof_bytes(P) + ring_bytes() + 15) & ~15; }
+  __host__ __device__ static int warp_bytes(int P) { return GROUPS * group_bytes(P); }
+  __host__ __device__ static int total(int M, int P, int warps) { return simp_bytes(M) + warps * warp_bytes(P); }
 };
 
 // Loads the substitution table with its padding column: simp[a][x] =
@@ -296,9 +297,9 @@ __global__ void __launch_bounds__(128, (FWD && !HYB) ? 4 : 3) k_batched(SwConst 
   const int group = lane32 / LANES;
   const int glane = lane32 & (LANES - 1);
   int8_t* s_simp = reinterpret_cast<int8_t*>(smem);
-  uint8_t* gbase = smem + L::simp_bytes(sc.M) + wib * L::warp_bytes(sc.M) + group * L::group_bytes(sc.M);
+  uint8_t* gbase = smem + L::simp_bytes(sc.M) + wib * L::warp_bytes(sc.P) + group * L::group_bytes(sc.P);
   uint8_t* s_prof = gbase;
-  uint16_t* s_bring = reinterpret_cast<uint16_t*>(gbase + L::prof_bytes(sc.M));
+  uint16_t* s_bring = reinterpret_cast<uint16_t*>(gbase + L::prof_bytes(sc.P));
   load_simp(s_simp, sim, sc);
   __syncthreads();
 
@@ -387,9 +388,9 @@ __global__ void __launch_bounds__(128) k_plain(SwConst sc, const int8_t* __restr
   const int wib = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   int8_t* s_simp = reinterpret_cast<int8_t*>(smem);
-  uint8_t* wbase = smem + L::simp_bytes(sc.M) + wib * L::warp_bytes(sc.M);
+  uint8_t* wbase = smem + L::simp_bytes(sc.M) + wib * L::warp_bytes(sc.P);
   uint8_t* s_prof = wbase;
-  uint16_t* s_bring = reinterpret_cast<uint16_t*>(wbase + L::prof_bytes(sc.M));
+  uint16_t* s_bring = reinterpret_cast<uint16_t*>(wbase + L::prof_bytes(sc.P));
   load_simp(s_simp, sim, sc);
   __syncthreads();
   const long gw = (long)blockIdx.x * warps + wib;
@@ -436,9 +437,9 @@ __global__ void __launch_bounds__(128) k_plain16(SwConst sc, const int8_t* __res
   const int wib = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   int8_t* s_simp = reinterpret_cast<int8_t*>(smem);
-  uint8_t* wbase = smem + L::simp_bytes(sc.M) + wib * L::warp_bytes(sc.M);
+  uint8_t* wbase = smem + L::simp_bytes(sc.M) + wib * L::warp_bytes(sc.P);
   uint8_t* s_prof = wbase;  // the s32 redo uses the first half of it
-  uint16_t* s_bring = reinterpret_cast<uint16_t*>(wbase + L::prof_bytes(sc.M));
+  uint16_t* s_bring = reinterpret_cast<uint16_t*>(wbase + L::prof_bytes(sc.P));
   load_simp(s_simp, sim, sc);
   __syncthreads();
   const long gw = (long)blockIdx.x * warps + wib;
@@ -638,11 +639,22 @@ static_assert(THR_NSB * THR_NRB <= NBUCKET, "per-thread buckets");
 // Best ungapped score along the main diagonal (a lower bound of the local
 // alignment score): pairs that surely pass the s16 limit go straight to
 // s32 lanes instead of giving up half way in s16x2.
+// Packed codes are read as two sequential streams; the loop ends as soon
+// as the bound passes `limit` (all the caller asks).
 static __device__ int diagonal_bound(const uint8_t* codes, int bits, long long a, long long b, int n,
-                                     const int8_t* sim, int M) {
+                                     const int8_t* sim, int M, int limit) {
   int run = 0, best = 0;
-  for (int k = 0; k < n; ++k) {
-    run = max(run + (int)sim[code_at(codes, a + k, bits) * M + code_at(codes, b + k, bits)], 0);
+  if (bits == 8) {
+    for (int k = 0; k < n && best <= limit; ++k) {
+      run = max(run + (int)sim[codes[a + k] * M + codes[b + k]], 0);
+      best = max(best, run);
+    }
+    return best;
+  }
+  PackedStream sa(codes, a, bits), sb(codes, b, bits);
+  for (int k = 0; k < n && best <= limit; ++k) {
+    const int x = sa.next(), y = sb.next();
+    run = max(run + (int)sim[x * M + y], 0);
     best = max(best, run);
   }
   return best;
@@ -729,6 +741,22 @@ static __global__ void k_bin_count(BinParams bp, const uint8_t* __restrict__ cod
                             const PairDesc* __restrict__ pairs, int n, int* hist, uint8_t* s32_flag,
                             unsigned long long* class_cells, unsigned long long* class_cost, DevStatus* st,
                             int* score, int* arange, int* brange) {
+  // The substitution matrix in shared memory for the diagonal bounds.
+  __shared__ int8_t s_sim[32 * 32];
+  const bool smemSim = bp.M <= 32;
+  if (smemSim)
+    for (int k = threadIdx.x; k < bp.M * bp.M; k += blockDim.x) s_sim[k] = sim[k];
+  __syncthreads();
+  const int8_t* simT = smemSim ? s_sim : sim;
+  // Per-class sums of the block, added to the global ones once at the end
+  // (a batch has a handful of classes: one global address per class would
+  // take every pair's atomic).
+  __shared__ unsigned long long s_cells[NCLASS_MAX + 1], s_cost[NCLASS_MAX + 1];
+  for (int k = threadIdx.x; k <= NCLASS_MAX; k += blockDim.x) {
+    s_cells[k] = 0;
+    s_cost[k] = 0;
+  }
+  __syncthreads();
   for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
     const PairDesc d = pairs[p];
     const int state = pair_state(d, bp.n_codes, bp.max_a, bp.max_b);
@@ -742,13 +770,21 @@ static __global__ void k_bin_count(BinParams bp, const uint8_t* __restrict__ cod
     }
     bool s32 = false;
     if (!bp.force_s32 && min(d.a_len, d.b_len) > bp.s16_max_len)
-      s32 = diagonal_bound(codes, bp.bits, d.a_off, d.b_off, min(d.a_len, d.b_len), sim, bp.M) > bp.s16_limit;
+      s32 = diagonal_bound(codes, bp.bits, d.a_off, d.b_off, min(d.a_len, d.b_len), simT, bp.M, bp.s16_limit) >
+            bp.s16_limit;
     s32_flag[p] = s32 ? 1 : 0;
     float cost = 0.f;
     const int key = pair_key(bp, d.a_len, d.b_len, s32, thread_cap(bp), &cost);
-    atomicAdd(&hist[key], 1);
-    atomicAdd(&class_cells[key / NBUCKET], (unsigned long long)d.a_len * (unsigned long long)d.b_len);
-    atomicAdd(&class_cost[key / NBUCKET], (unsigned long long)fmaxf(cost, 1.f));
+    // One histogram update per distinct key among the warp's lanes.
+    const unsigned same = __match_any_sync(__activemask(), key);
+    if ((int)(threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&hist[key], __popc(same));
+    atomicAdd(&s_cells[key / NBUCKET], (unsigned long long)d.a_len * (unsigned long long)d.b_len);
+    atomicAdd(&s_cost[key / NBUCKET], (unsigned long long)fmaxf(cost, 1.f));
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < bp.nclass; k += blockDim.x) {
+    if (s_cells[k]) atomicAdd(&class_cells[k], s_cells[k]);
+    if (s_cost[k]) atomicAdd(&class_cost[k], s_cost[k]);
   }
 }
 
@@ -756,29 +792,50 @@ __device__ __forceinline__ int run_total(const int* hist, const int* offs, int n
   return offs[nkeys - 1] + hist[nkeys - 1];
 }
 
-// Single block: exclusive scan of the histogram into `offs`, and per class
-// the {start, count} range consumed by k_batched.
+// Single block (blockDim.x a multiple of 32): exclusive scan of the
+// histogram into `offs`, and per class the {start, count} range consumed by
+// k_batched.  The keys go tile by tile (blockDim.x keys, coalesced, kTiles
+// tiles of loads in flight), each tile scanned across the block and offset
+// by the running total of the tiles before.
 static __global__ void k_bin_scan(BinParams bp, int nkeys, const int* hist, int* offs, int* class_range,
                                   const unsigned long long* class_cost, ClassAllot* allot, DevStatus* st) {
-  __shared__ int s_sum[1024];
-  const int tid = threadIdx.x;
-  const int per = (nkeys + blockDim.x - 1) / blockDim.x;
-  int local = 0;
-  for (int k = tid * per; k < min(nkeys, (tid + 1) * per); ++k) local += hist[k];
-  s_sum[tid] = local;
-  __syncthreads();
-  for (int off = 1; off < blockDim.x; off <<= 1) {
-    int v = (tid >= off) ? s_sum[tid - off] : 0;
-    __syncthreads();
-    s_sum[tid] += v;
-    __syncthreads();
+  constexpr int kTiles = 8;
+  __shared__ int s_warp[32];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  int carry = 0;
+  for (int base = 0; base < nkeys; base += kTiles * blockDim.x) {
+    int v[kTiles];
+#pragma unroll
+    for (int j = 0; j < kTiles; ++j) {
+      const int k = base + j * blockDim.x + tid;
+      v[j] = k < nkeys ? hist[k] : 0;
+    }
+#pragma unroll
+    for (int j = 0; j < kTiles; ++j) {
+      int x = v[j];  // inclusive prefix within the warp
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(FULL, x, off);
+        if (lane >= off) x += y;
+      }
+      if (lane == 31) s_warp[wid] = x;
+      __syncthreads();
+      if (wid == 0) {
+        int w = lane < nw ? s_warp[lane] : 0;  // inclusive prefix of the warp totals
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+          const int y = __shfl_up_sync(FULL, w, off);
+          if (lane >= off) w += y;
+        }
+        if (lane < nw) s_warp[lane] = w;
+      }
+      __syncthreads();
+      const int k = base + j * blockDim.x + tid;
+      if (k < nkeys) offs[k] = carry + (wid > 0 ? s_warp[wid - 1] : 0) + x - v[j];
+      carry += s_warp[nw - 1];
+      __syncthreads();  // s_warp is rewritten by the next tile
+    }
   }
-  int run = s_sum[tid] - local;
-  for (int k = tid * per; k < min(nkeys, (tid + 1) * per); ++k) {
-    offs[k] = run;
-    run += hist[k];
-  }
-  __syncthreads();
   if (tid < nkeys / NBUCKET) {
     const int c = tid;
     class_range[2 * c] = offs[c * NBUCKET];
@@ -823,8 +880,16 @@ static __global__ void k_bin_scatter(BinParams bp, const PairDesc* __restrict__ 
   for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
     const PairDesc d = pairs[p];
     if (pair_state(d, bp.n_codes, bp.max_a, bp.max_b) != PAIR_OK) continue;
-    const int pos = atomicAdd(&offs[pair_key(bp, d.a_len, d.b_len, s32_flag[p] != 0, thread_cap(bp))], 1);
-    list[pos] = (int)p;
+    const int key = pair_key(bp, d.a_len, d.b_len, s32_flag[p] != 0, thread_cap(bp));
+    // One atomic per distinct key among the warp's lanes; each lane takes
+    // the slot of its rank in the group.
+    const unsigned act = __activemask();
+    const unsigned same = __match_any_sync(act, key);
+    const int lane = (int)(threadIdx.x & 31), leader = __ffs(same) - 1;
+    int pos0 = 0;
+    if (lane == leader) pos0 = atomicAdd(&offs[key], __popc(same));
+    pos0 = __shfl_sync(act, pos0, leader);
+    list[pos0 + __popc(same & ((1u << lane) - 1u))] = (int)p;
   }
 }
 
