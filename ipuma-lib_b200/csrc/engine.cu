@@ -647,6 +647,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   const int gb = std::min<int>((n + tb - 1) / tb, e->nsm * 8);
   k_bin_total<<<gb, tb, 0, s>>>(bp, pairs, n,
                                 reinterpret_cast<unsigned long long*>(ctl + CTL_CELLS) + CELLS_TOTAL);
+  k_bin_bound<<<gb, tb, 0, s>>>(bp, codes, e->d_sim.as<int8_t>(), pairs, n, rb.flag->as<uint8_t>());
   k_bin_count<<<gb, tb, 0, s>>>(bp, codes, e->d_sim.as<int8_t>(), pairs, n, ctl + CTL_HIST,
                                 rb.flag->as<uint8_t>(),
                                 reinterpret_cast<unsigned long long*>(ctl + CTL_CELLS),
@@ -658,7 +659,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   k_bin_scatter<<<gb, tb, 0, s>>>(bp, pairs, n, rb.flag->as<uint8_t>(), ctl + CTL_OFFS,
                                   rb.list->as<int>());
   CUDA_TRY(cudaGetLastError());
-  *launches += 4;
+  *launches += 5;
 
   int* list = rb.list->as<int>();
   int* heads = ctl + CTL_HEADS;

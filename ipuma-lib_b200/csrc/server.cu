@@ -16,7 +16,9 @@
 // Resident sequence sets: a caller that aligns against the same sequences
 // again and again uploads them once (ipuma_server_add_sequences); requests
 // then carry only pair descriptors into that set and batches stage nothing
-// but pairs.  A batch holds requests of one scoring and one set.
+// but pairs.  A batch holds requests of one scoring and one set.  A set of
+// A/C/G/T codes only also gets a 2-bit copy, which the nucleic-acid batches
+// on it read.
 //
 // Engines for every slot and scoring are created, autotuned (one scoring
 // after the other) and given device buffers for reserve_b_len rows when
@@ -135,6 +137,10 @@ size_t batch_bytes(size_t codes, size_t pairs) {
 struct ResidentSet {
   uint8_t* d_codes = nullptr;
   size_t n_codes = 0;
+  // 2-bit copy (ipuma_pack_codes) when every code is A, C, G or T (1..4):
+  // nucleic-acid batches on the set read it through
+  // ipuma_gpu_compare_device_packed, whose profiles hold four letters.
+  uint8_t* d_packed2 = nullptr;
 };
 
 constexpr int kShards = 64;
@@ -332,8 +338,12 @@ void worker_loop(ipuma_server* s, int slot_index) {
       }
     }
     if (rc == IPUMA_OK && npairs > 0) {
-      rc = ipuma_gpu_compare_device(st.engines[kind], d_codes, n_codes_batch, d_pairs, (int32_t)npairs, maxA, maxB,
-                                    d_out, d_out + npairs, d_out + 2 * npairs, st.stream);
+      if (set >= 0 && rs.d_packed2 && s->scorings[kind].datatype == IPUMA_DT_NUCLEIC_ACID)
+        rc = ipuma_gpu_compare_device_packed(st.engines[kind], rs.d_packed2, rs.n_codes, 2, d_pairs, (int32_t)npairs,
+                                             maxA, maxB, d_out, d_out + npairs, d_out + 2 * npairs, st.stream);
+      else
+        rc = ipuma_gpu_compare_device(st.engines[kind], d_codes, n_codes_batch, d_pairs, (int32_t)npairs, maxA, maxB,
+                                      d_out, d_out + npairs, d_out + 2 * npairs, st.stream);
       if (rc) msg = ipuma_last_error();
     }
     if (rc == IPUMA_OK && npairs > 0) {
@@ -493,9 +503,22 @@ int ipuma_server_add_sequences(ipuma_server* s, const uint8_t* codes, size_t n_c
     cudaFree(rs.d_codes);
     return fail(IPUMA_ERR_CUDA, "copying the sequence set failed");
   }
+  if (n_codes && std::all_of(codes, codes + n_codes, [](uint8_t c) { return c >= 1 && c <= 4; })) {
+    // Packed arrays are read a word at a time: whole words plus one.
+    const size_t bytes = ((n_codes * 2 + 7) / 8 + 3) / 4 * 4 + 8;
+    std::vector<uint8_t> packed(bytes, 0);
+    if (ipuma_pack_codes(codes, n_codes, 2, packed.data()) == IPUMA_OK &&
+        cudaMalloc(&rs.d_packed2, bytes) == cudaSuccess &&
+        cudaMemcpy(rs.d_packed2, packed.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaFree(rs.d_packed2);
+      rs.d_packed2 = nullptr;
+    }
+    cudaGetLastError();  // a failed copy only leaves the set without its 2-bit form
+  }
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->closing) {
     cudaFree(rs.d_codes);
+    cudaFree(rs.d_packed2);
     return fail(IPUMA_ERR_CLOSED, "server is closed");
   }
   *set_id = (int32_t)s->sets.size();
@@ -642,7 +665,10 @@ void ipuma_server_destroy(ipuma_server* s) {
   for (auto& row : s->engines)
     for (auto* e : row)
       if (e) ipuma_gpu_destroy(e);
-  for (auto& rs : s->sets) cudaFree(rs.d_codes);
+  for (auto& rs : s->sets) {
+    cudaFree(rs.d_codes);
+    cudaFree(rs.d_packed2);
+  }
   if (s->d_pool) cudaFree(s->d_pool);
   delete s;
 }

@@ -637,27 +637,59 @@ constexpr int THR_NRB = 144;
 static_assert(THR_NSB * THR_NRB <= NBUCKET, "per-thread buckets");
 
 // Best ungapped score along the main diagonal (a lower bound of the local
-// alignment score): pairs that surely pass the s16 limit go straight to
-// s32 lanes instead of giving up half way in s16x2.
-// Packed codes are read as two sequential streams; the loop ends as soon
-// as the bound passes `limit` (all the caller asks).
-static __device__ int diagonal_bound(const uint8_t* codes, int bits, long long a, long long b, int n,
-                                     const int8_t* sim, int M, int limit) {
-  int run = 0, best = 0;
-  if (bits == 8) {
-    for (int k = 0; k < n && best <= limit; ++k) {
-      run = max(run + (int)sim[codes[a + k] * M + codes[b + k]], 0);
-      best = max(best, run);
+// alignment score): pairs that surely pass the s16 limit go to the hybrid
+// (or s32) class instead of giving up half way in s16x2.  One warp per
+// pair: lane l takes the l-th of 32 consecutive segments of the diagonal
+// and summarises it as {sum, best prefix, best suffix, best run} (all >= 0
+// but the sum); an ordered tree of shuffles joins the summaries, the best
+// run of the whole diagonal ending in lane 0 (the maximum-subarray score
+// that max(run + s, 0) computes sequentially).
+struct DiagRun {
+  int sum, pre, suf, best;
+};
+
+__device__ __forceinline__ DiagRun join_runs(const DiagRun& l, const DiagRun& r) {
+  return DiagRun{l.sum + r.sum, max(l.pre, l.sum + r.pre), max(r.suf, r.sum + l.suf),
+                 max(max(l.best, r.best), l.suf + r.pre)};
+}
+
+static __device__ int warp_diagonal_bound(const uint8_t* codes, int bits, long long a, long long b, int n,
+                                          const int8_t* sim, int M) {
+  const int lane = threadIdx.x & 31;
+  const int seg = (n + 31) / 32;
+  const int k0 = min(n, lane * seg), k1 = min(n, k0 + seg);
+  DiagRun r{0, 0, 0, 0};
+  int run = 0;
+  auto take = [&](int s) {
+    r.sum += s;
+    r.pre = max(r.pre, r.sum);
+    run = max(run + s, 0);
+    r.best = max(r.best, run);
+  };
+  // A code outside the alphabet (no row of the matrix) counts 0 here.
+  auto score = [&](int x, int y) { return (x < M && y < M) ? (int)sim[x * M + y] : 0; };
+  if (k0 < k1) {
+    if (bits == 8) {
+      for (int k = k0; k < k1; ++k) take(score(codes[a + k], codes[b + k]));
+    } else {
+      PackedStream sa(codes, a + k0, bits), sb(codes, b + k0, bits);
+      for (int k = k0; k < k1; ++k) {
+        const int x = sa.next(), y = sb.next();
+        take(score(x, y));
+      }
     }
-    return best;
   }
-  PackedStream sa(codes, a, bits), sb(codes, b, bits);
-  for (int k = 0; k < n && best <= limit; ++k) {
-    const int x = sa.next(), y = sb.next();
-    run = max(run + (int)sim[x * M + y], 0);
-    best = max(best, run);
+  r.suf = run;  // best sum of a suffix (empty allowed)
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    DiagRun o;
+    o.sum = __shfl_down_sync(FULL, r.sum, off);
+    o.pre = __shfl_down_sync(FULL, r.pre, off);
+    o.suf = __shfl_down_sync(FULL, r.suf, off);
+    o.best = __shfl_down_sync(FULL, r.best, off);
+    if ((lane & (2 * off - 1)) == 0 && lane + off < 32) r = join_runs(r, o);
   }
-  return best;
+  return __shfl_sync(FULL, r.best, 0);
 }
 
 // Class of a pair: the kernel with the lowest modelled time
@@ -737,17 +769,46 @@ static __global__ void k_bin_total(BinParams bp, const PairDesc* __restrict__ pa
   if ((threadIdx.x & 31) == 0 && local) atomicAdd(total, local);
 }
 
-static __global__ void k_bin_count(BinParams bp, const uint8_t* __restrict__ codes, const int8_t* __restrict__ sim,
-                            const PairDesc* __restrict__ pairs, int n, int* hist, uint8_t* s32_flag,
-                            unsigned long long* class_cells, unsigned long long* class_cost, DevStatus* st,
-                            int* score, int* arange, int* brange) {
-  // The substitution matrix in shared memory for the diagonal bounds.
+// A pair whose diagonal bound decides its class: both sequences longer than
+// the longest pair that cannot pass the s16 limit.
+__device__ __forceinline__ bool bound_candidate(const BinParams& bp, const PairDesc& d) {
+  return !bp.force_s32 && min(d.a_len, d.b_len) > bp.s16_max_len &&
+         pair_state(d, bp.n_codes, bp.max_a, bp.max_b) == PAIR_OK;
+}
+
+// s32_flag of every candidate pair (k_bin_count reads it): warps take 32
+// pairs at a time and compute the diagonal bound of each candidate among
+// them together (warp_diagonal_bound).  blockDim.x is a multiple of 32.
+static __global__ void k_bin_bound(BinParams bp, const uint8_t* __restrict__ codes,
+                                   const int8_t* __restrict__ sim, const PairDesc* __restrict__ pairs, int n,
+                                   uint8_t* s32_flag) {
   __shared__ int8_t s_sim[32 * 32];
   const bool smemSim = bp.M <= 32;
   if (smemSim)
     for (int k = threadIdx.x; k < bp.M * bp.M; k += blockDim.x) s_sim[k] = sim[k];
   __syncthreads();
   const int8_t* simT = smemSim ? s_sim : sim;
+  const int lane = threadIdx.x & 31;
+  const long warps = (long)gridDim.x * (blockDim.x / 32);
+  for (long base = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32 * 32; base < n; base += warps * 32) {
+    const long p = base + lane;
+    const bool cand = p < n && bound_candidate(bp, pairs[p]);
+    unsigned m = __ballot_sync(FULL, cand);
+    while (m) {
+      const long q = base + __ffs(m) - 1;
+      m &= m - 1;
+      const PairDesc d = pairs[q];
+      const int bound =
+          warp_diagonal_bound(codes, bp.bits, d.a_off, d.b_off, min(d.a_len, d.b_len), simT, bp.M);
+      if (lane == 0) s32_flag[q] = bound > bp.s16_limit ? 1 : 0;
+    }
+  }
+}
+
+static __global__ void k_bin_count(BinParams bp, const uint8_t* __restrict__ codes, const int8_t* __restrict__ sim,
+                            const PairDesc* __restrict__ pairs, int n, int* hist, uint8_t* s32_flag,
+                            unsigned long long* class_cells, unsigned long long* class_cost, DevStatus* st,
+                            int* score, int* arange, int* brange) {
   // Per-class sums of the block, added to the global ones once at the end
   // (a batch has a handful of classes: one global address per class would
   // take every pair's atomic).
@@ -768,10 +829,10 @@ static __global__ void k_bin_count(BinParams bp, const uint8_t* __restrict__ cod
       brange[p] = 0;
       continue;
     }
+    // Candidates (both sequences longer than s16_max_len) got their flag
+    // from k_bin_bound.
     bool s32 = false;
-    if (!bp.force_s32 && min(d.a_len, d.b_len) > bp.s16_max_len)
-      s32 = diagonal_bound(codes, bp.bits, d.a_off, d.b_off, min(d.a_len, d.b_len), simT, bp.M, bp.s16_limit) >
-            bp.s16_limit;
+    if (bound_candidate(bp, d)) s32 = s32_flag[p] != 0;
     s32_flag[p] = s32 ? 1 : 0;
     float cost = 0.f;
     const int key = pair_key(bp, d.a_len, d.b_len, s32, thread_cap(bp), &cost);

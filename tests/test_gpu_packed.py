@@ -139,9 +139,10 @@ def test_protein_5bit_host_call_equals_bytes_and_oracle(forward_only):
         _same(got, want, "5-bit chunks=%d" % chunks)
 
 
-def _device_packed(wl, codes, pairs, bits, forward_only, graphs=0, **opts):
+def _device_packed(wl, codes, pairs, bits, forward_only, graphs=0, reruns=None, **opts):
     """compare_device_packed on a device copy of the packed codes (padded as
-    the call requires) and compare_device on the byte codes."""
+    the call requires) and compare_device on the byte codes; `reruns`, when
+    given, collects each call's count of s16x2 pairs rerun in s32."""
     torch = pytest.importorskip("torch")
     packed = ib.pack_codes(codes, bits)
     buf = np.zeros(ib.device_packed_bytes(codes.size, bits), np.uint8)
@@ -162,6 +163,8 @@ def _device_packed(wl, codes, pairs, bits, forward_only, graphs=0, **opts):
                 e.compare_device(d_bytes.data_ptr(), codes.size, d_pairs.data_ptr(), *args)
             torch.cuda.synchronize()
             outs.append(tuple(out.cpu().numpy()))
+            if reruns is not None:
+                reruns.append(int(e.stats().overflow_reruns))
     return outs
 
 
@@ -201,8 +204,14 @@ def test_device_packed_high_scores_hybrid_and_s32():
     want = _oracle(base, codes, pairs, True)
     assert want[0].max() > 65535 - 1024 - 11 and (want[0] > 32767).sum() >= 8
     for hybrid in (1, 0):
-        got_p, _ = _device_packed(base, codes, pairs, 5, True, hybrid=hybrid)
+        reruns = []
+        got_p, got_b = _device_packed(base, codes, pairs, 5, True, hybrid=hybrid, reruns=reruns)
         _same(got_p, want, "5-bit high scores hybrid=%d" % hybrid)
+        _same(got_b, want, "byte high scores hybrid=%d" % hybrid)
+        # Every pair above the s16 limit has a diagonal bound above it (checked
+        # on the CPU for this batch), so none starts in s16x2 lanes and has to
+        # be rerun: the warp-parallel bound routed them all.
+        assert reruns == [0, 0], reruns
 
 
 def test_device_packed_exact_kernel_for_unusual_gaps():
