@@ -378,11 +378,11 @@ typedef struct ipuma_server_config {
   int32_t forward_only;            /* 1: no reverse pass (start coordinates 0) */
   int32_t slots;                   /* concurrent device batches; 0 = 4 */
   int64_t pool_bytes;              /* device pool; 0 = a quarter of the free memory */
-  int32_t max_batch_pairs;         /* pairs per device batch; 0 = 65536 */
+  int32_t max_batch_pairs;         /* pairs per device batch; 0 = 262144 */
   int32_t device;
   int32_t one_request_per_batch;   /* 1: no coalescing (each batch = one request or
                                       part of one), the per-request baseline */
-  int64_t max_batch_cells;         /* cells per device batch (latency bound); 0 = 4e9 */
+  int64_t max_batch_cells;         /* cells per device batch (latency bound); 0 = 2e10 */
   int32_t reserve_b_len;           /* |B| the engines' buffers are sized for at start;
                                       0 = 2048 (longer pairs grow them on demand) */
 } ipuma_server_config;

@@ -915,8 +915,10 @@ std::string tune_key(const ipuma_engine* e) {
   cudaDeviceProp prop;
   cudaGetDeviceProperties(&prop, e->device);
   char buf[512];
-  snprintf(buf, sizeof(buf), "%s|sm%d%d|M=%d|sim=%d|gI=%d|gE=%d|v5", prop.name, prop.major, prop.minor, e->M,
-           e->sw.similarity, e->sw.gap_init, e->sw.gap_extend);
+  // The rates are those of the engine's kernels, which differ by mode: a
+  // full alignment (forward + reverse pass) takes longer per cell.
+  snprintf(buf, sizeof(buf), "%s|sm%d%d|M=%d|sim=%d|gI=%d|gE=%d|fwd=%d|v6", prop.name, prop.major, prop.minor, e->M,
+           e->sw.similarity, e->sw.gap_init, e->sw.gap_extend, e->sc.forwardOnly);
   for (char* c = buf; *c; ++c)
     if (*c == '\t' || *c == '\n') *c = ' ';
   return buf;

@@ -448,11 +448,11 @@ int ipuma_server_create(const ipuma_server_config* cfg, ipuma_server** out) {
   s->scorings.assign(cfg->scorings, cfg->scorings + cfg->n_scorings);
   s->cfg.scorings = nullptr;
   if (s->cfg.slots <= 0) s->cfg.slots = 4;
-  if (s->cfg.max_batch_pairs <= 0) s->cfg.max_batch_pairs = 65536;
+  if (s->cfg.max_batch_pairs <= 0) s->cfg.max_batch_pairs = 262144;
   // 4e9 cells: ~2 ms of device time; measured on B200 with 64-pair
   // requests, 2e9 saturated at 80 % of the device rate, 4e9 sustains 90 %
   // with p99 15 ms, 8e9 adds little.
-  if (s->cfg.max_batch_cells <= 0) s->cfg.max_batch_cells = 4000000000LL;
+  if (s->cfg.max_batch_cells <= 0) s->cfg.max_batch_cells = 20000000000LL;
   if (s->cfg.reserve_b_len <= 0) s->cfg.reserve_b_len = 2048;
   s->cfg.reserve_b_len = std::min(s->cfg.reserve_b_len, 65535);
   s->device = cfg->device;
