@@ -683,14 +683,19 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
           for (int c = 0; c + w < (K + 1) / 2; c += 2 * w) m8[c] = T::max2(m8[c], m8[c + w]);
         const V rm = m8[0];
         // Running best of this lane: strict > keeps the first row.
-        // The blend runs on every step, improved or not: some lane of the
-        // warp improves on most steps, and a branch around it cost more
-        // than it saved (measured on B200: +1 % DNA, +3 % protein batches).
+        // With two pairs per lane (16-bit halves) the blend runs on every
+        // step, improved or not: some lane of the warp improves on most
+        // steps, and a branch around it cost more than it saved (measured
+        // on B200: +1 % DNA, +3 % protein batches).  With one pair per
+        // warp (s32 lanes) improvements are rarer and the branch pays
+        // (the plain s32 kernel ran 16-20 % slower without it).
         const uint32_t keep = update_best(T{}, best, rm);
-        const uint32_t ipk = (uint32_t)i * 0x00010001u;  // row in both halfwords
-        brow = (brow & keep) | (ipk & ~keep);
+        if (NP == 2 || keep != 0xffffffffu) {
+          const uint32_t ipk = (uint32_t)i * 0x00010001u;  // row in both halfwords
+          brow = (brow & keep) | (ipk & ~keep);
 #pragma unroll
-        for (int c = 0; c < K; ++c) snap[c] = (V)(((uint32_t)snap[c] & keep) | ((uint32_t)H[c] & ~keep));
+          for (int c = 0; c < K; ++c) snap[c] = (V)(((uint32_t)snap[c] & keep) | ((uint32_t)H[c] & ~keep));
+        }
         if (hasOut && lane == LANES - 1) scrOut[i] = make_int2((int)outY, (int)outE);
         if constexpr (HYB && NP == 2) bmax = T::max2(bmax, T::addmax(outE, vgIgE, outY));
       }
