@@ -452,7 +452,10 @@ def protein_target(ib, torch, wl, dev, local, stream, reps):
         "plain_bit_identical": plain["s32"]["bit_identical_to_batched"] and
                                plain["s16x2"]["bit_identical_to_batched"],
         "oracle_sample": {"pairs": checked, "mismatching_fields": mism},
-        "trace": trace,
+        # Device trace of one step, summarised: the span of its class launches
+        # and its longest launch.
+        "trace_span_ms": max((t["end_ms"] for t in trace), default=None),
+        "trace_longest": max(trace, key=lambda t: t["end_ms"] - t["start_ms"], default=None),
     }
 
 
