@@ -677,7 +677,8 @@ def main(argv=None):
         e2e = {"value": total_cells / wall / 1e9, "unit": "GCUPS",
                "h2d_bytes_per_step": int(packed_np.nbytes + db.pairs_np.nbytes),
                "d2h_bytes_per_step": int(3 * 4 * wl.n), "ms_per_step": wall * 1e3,
-               "last_call_device_span_ms": st.total_ms,  # first copy to last result, CUDA events
+               "last_call_ms": {"device_span": st.total_ms,  # first copy to last result, CUDA events
+                                "host_check": st.host_check_ms, "host_wall": st.host_wall_ms},
                "bit_identical_to_device_run": same, "chunks": chunks,
                "call": "ipuma_gpu_compare_packed (%d-bit codes, read packed by the kernels)" % bits,
                "bytes_path": bytes_path}

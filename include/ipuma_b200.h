@@ -143,6 +143,11 @@ typedef struct ipuma_stats {
   double trace_start_ms[IPUMA_MAX_TIMED];
   double trace_end_ms[IPUMA_MAX_TIMED];
   int64_t trace_cells[IPUMA_MAX_TIMED];
+  /* Host-buffer calls (ipuma_gpu_compare, ipuma_gpu_compare_packed): host
+   * wall time of the descriptor check (bounds, maxima, code ranges per
+   * chunk) and of the whole call. */
+  double host_check_ms;
+  double host_wall_ms;
 } ipuma_stats;
 
 /* Kernel kinds reported in ipuma_stats.timed_kind.  S16_L<lanes>_K<k>:

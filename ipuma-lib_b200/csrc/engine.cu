@@ -1740,6 +1740,7 @@ static int compare_host(ipuma_engine* e, const uint8_t* codes, size_t n_codes, i
   if (n == 0) return IPUMA_OK;
   if (!codes || !pairs || !score || !arange || !brange) return fail(IPUMA_ERR_INVALID_ARG, "null buffer");
   std::lock_guard<std::mutex> lk(e->mu);
+  const auto h0 = std::chrono::steady_clock::now();
   const int nch = e->time_launches ? 1 : chunk_count(e, n, n_codes);
   // Host-side bounds check of every pair (the kernels trust the
   // descriptors), with the code ranges each chunk of pairs reads; large
@@ -1773,6 +1774,7 @@ static int compare_host(ipuma_engine* e, const uint8_t* codes, size_t n_codes, i
   }
   if (maxA > 65535 || maxB > 65535)
     return fail(IPUMA_ERR_TOO_LONG, "sequence longer than 65535 (ranges are uint16)");
+  const auto h1 = std::chrono::steady_clock::now();
   CUDA_TRY(cudaSetDevice(e->device));
   cudaStream_t s = e->stream;
   int rc;
@@ -1881,6 +1883,9 @@ static int compare_host(ipuma_engine* e, const uint8_t* codes, size_t n_codes, i
   e->stats.pairs = n;
   e->stats.launches = launches;
   e->stats.chunks = nch;
+  e->stats.host_check_ms = std::chrono::duration<double, std::milli>(h1 - h0).count();
+  e->stats.host_wall_ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count();
   return IPUMA_OK;
 }
 

@@ -94,7 +94,8 @@ class Stats(ctypes.Structure):
                 ("trace_kind", ctypes.c_int32 * MAX_TIMED),
                 ("trace_start_ms", ctypes.c_double * MAX_TIMED),
                 ("trace_end_ms", ctypes.c_double * MAX_TIMED),
-                ("trace_cells", ctypes.c_int64 * MAX_TIMED)]
+                ("trace_cells", ctypes.c_int64 * MAX_TIMED),
+                ("host_check_ms", ctypes.c_double), ("host_wall_ms", ctypes.c_double)]
 
 
 class ServerConfig(ctypes.Structure):
