@@ -176,10 +176,6 @@ typedef struct ipuma_stats {
 #define IPUMA_KERNEL_S16_HYBRID 20 /* scores above int16: strips in biased 16-bit halves (score - 31744,
                                       scores up to 65535 - 1024 - max(sim)) while safe, then s32 */
 #define IPUMA_KERNEL_PLAIN_S16 21  /* one-launch-per-batch wire kernel, 16-bit lanes */
-#define IPUMA_KERNEL_S16_L32_K10 22
-#define IPUMA_KERNEL_S16_L32_K13 23
-#define IPUMA_KERNEL_S16_L32_K14 24
-#define IPUMA_KERNEL_S16_L32_K15 25
 
 typedef struct ipuma_engine ipuma_engine;
 
@@ -227,8 +223,7 @@ void ipuma_gpu_destroy(ipuma_engine* e);
  *                 through s16x2 class IPUMA_KERNEL_S16_* (value = kind),
  *                 7 = every pair through IPUMA_KERNEL_S16_T_K16, 8, 9, 10 =
  *                 IPUMA_KERNEL_S16_L16_K6, _K10, _K14, 11 .. 16 =
- *                 IPUMA_KERNEL_S16_L16_K5, _K7, _K9, _K11, _K13, _K15,
- *                 17 .. 20 = IPUMA_KERNEL_S16_L32_K10, _K13, _K14, _K15
+ *                 IPUMA_KERNEL_S16_L16_K5, _K7, _K9, _K11, _K13, _K15
  *   "concurrent"  3 = by batch size (default): mode 1 below 48,000 pairs,
  *                 mode 2 above; 2 = class launches alternate between two
  *                 streams, so each starts on the SMs the previous one

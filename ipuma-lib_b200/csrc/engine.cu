@@ -96,7 +96,7 @@ struct DevBuf {
 struct ClassDef {
   int lanes, k, kind, width;
 };
-constexpr int kNumS16 = 20;     // s16x2 classes chosen by cost
+constexpr int kNumS16 = 16;     // s16x2 classes chosen by cost
 constexpr int kNumClasses = kNumS16 + 2;  // + the s32 class + the hybrid class
 constexpr ClassDef kClasses[kNumClasses] = {
     {16, 4, IPUMA_KERNEL_S16_L16_K4, 64},    {16, 8, IPUMA_KERNEL_S16_L16_K8, 128},
@@ -107,8 +107,6 @@ constexpr ClassDef kClasses[kNumClasses] = {
     {16, 5, IPUMA_KERNEL_S16_L16_K5, 80},    {16, 7, IPUMA_KERNEL_S16_L16_K7, 112},
     {16, 9, IPUMA_KERNEL_S16_L16_K9, 144},   {16, 11, IPUMA_KERNEL_S16_L16_K11, 176},
     {16, 13, IPUMA_KERNEL_S16_L16_K13, 208}, {16, 15, IPUMA_KERNEL_S16_L16_K15, 240},
-    {32, 10, IPUMA_KERNEL_S16_L32_K10, 320}, {32, 13, IPUMA_KERNEL_S16_L32_K13, 416},
-    {32, 14, IPUMA_KERNEL_S16_L32_K14, 448}, {32, 15, IPUMA_KERNEL_S16_L32_K15, 480},
     {32, 16, IPUMA_KERNEL_S32_K16, 512},     {32, 16, IPUMA_KERNEL_S16_HYBRID, 512},
 };
 constexpr int kClsWidest = 5;  // widest wavefront class (very long |A|)
@@ -135,17 +133,14 @@ constexpr float kLatencyMinBatchPs = 0.f;
 // warps, so the classes share the SMs (mode 1); larger ones alternate two
 // streams (mode 2), which keeps one class per SM.
 constexpr int kShareModeMaxPairs = 48000;
-// The 16-lane classes at 16-column steps (every K from 4 to 16) and the
-// 32-lane classes of 320 to 480 columns cut column padding on large
-// batches; a smaller batch uses the 64-column steps only (K = 4, 8, 12, 16;
-// 384 and 512 columns with 32 lanes), since every class launch costs a few
-// microseconds even when empty.  (The 32-lane ones take the long pairs
-// that the latency bound keeps out of the 16-lane classes.)
+// The 16-lane classes at 16-column steps (every K from 4 to 16) cut column
+// padding on large batches; a smaller batch uses the 64-column steps only
+// (K = 4, 8, 12, 16), since every class launch costs a few microseconds
+// even when empty.
 constexpr int kFineClassMinPairs = 150000;
 constexpr unsigned kCoarseClasses = (1u << 0) | (1u << 1) | (1u << 2) | (1u << 3) | (1u << 4) | (1u << 5);
 constexpr unsigned kFineClasses = (1u << 7) | (1u << 8) | (1u << 9) | (1u << 10) | (1u << 11) | (1u << 12) |
-                                  (1u << 13) | (1u << 14) | (1u << 15) | (1u << 16) | (1u << 17) |
-                                  (1u << 18) | (1u << 19);
+                                  (1u << 13) | (1u << 14) | (1u << 15);
 constexpr int kWarpsPerBlock = 4;
 // Chunked upload/compute overlap of ipuma_gpu_compare.
 constexpr int kMaxChunks = 8;
@@ -370,10 +365,6 @@ int max_batched_groups(ipuma_engine* e) {
     g = std::max(g, batched_grid<Lane16, 15, 16>(e, P) * 2);
     g = std::max(g, batched_grid<Lane16, 12, 32>(e, P));
     g = std::max(g, batched_grid<Lane16, 16, 32>(e, P));
-    g = std::max(g, batched_grid<Lane16, 10, 32>(e, P));
-    g = std::max(g, batched_grid<Lane16, 13, 32>(e, P));
-    g = std::max(g, batched_grid<Lane16, 14, 32>(e, P));
-    g = std::max(g, batched_grid<Lane16, 15, 32>(e, P));
     g = std::max(g, batched_grid<LaneS32, 16, 32>(e, P));
     g = std::max(g, batched_grid<LaneHi, 16, 32, true>(e, P));
   }
@@ -496,10 +487,6 @@ void class_grids(ipuma_engine* e, int P, int maxA, int maxB, int* grid, long lon
       case 13: grid[c] = batched_grid<Lane16, 11, 16>(e, P); break;
       case 14: grid[c] = batched_grid<Lane16, 13, 16>(e, P); break;
       case 15: grid[c] = batched_grid<Lane16, 15, 16>(e, P); break;
-      case 16: grid[c] = batched_grid<Lane16, 10, 32>(e, P); break;
-      case 17: grid[c] = batched_grid<Lane16, 13, 32>(e, P); break;
-      case 18: grid[c] = batched_grid<Lane16, 14, 32>(e, P); break;
-      case 19: grid[c] = batched_grid<Lane16, 15, 32>(e, P); break;
       default: grid[c] = batched_grid<LaneS32, 16, 32>(e, P); break;
     }
     if (c == kClsThread)
@@ -534,7 +521,7 @@ size_t scratch_int2(ipuma_engine* e, int maxA, int maxB) {
 // The hybrid class and the widest class (the long pairs of a heavy-tailed
 // batch) come first and land on different streams, so the widest class's
 // blocks start on the SMs the hybrid class frees during its tail.
-constexpr int kLaunchOrder[kNumClasses] = {21, 5, 20, 19, 18, 17, 4, 16, 6, 3, 15, 9, 14, 2, 13, 8, 12, 1, 11, 7, 10, 0};
+constexpr int kLaunchOrder[kNumClasses] = {17, 5, 16, 4, 6, 3, 15, 9, 14, 2, 13, 8, 12, 1, 11, 7, 10, 0};
 
 int reserve_bufs(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, int n, int maxA, int maxB) {
   int rc;
@@ -718,13 +705,9 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
     if ((rc = done(kClsHi))) return rc;
     ++*launches;
   }
-  IPUMA_LAUNCH(LaneS32, 16, 32, kClsS32)
+  IPUMA_LAUNCH(LaneS32, 16, 32, 16)
   IPUMA_LAUNCH(Lane16, 16, 32, 5)
-  IPUMA_LAUNCH(Lane16, 15, 32, 19)
-  IPUMA_LAUNCH(Lane16, 14, 32, 18)
-  IPUMA_LAUNCH(Lane16, 13, 32, 17)
   IPUMA_LAUNCH(Lane16, 12, 32, 4)
-  IPUMA_LAUNCH(Lane16, 10, 32, 16)
   if ((enabled >> kClsThread) & 1u) {
     cudaStream_t cs = on(kClsThread);
     if ((rc = launch_thread<16>(e, rb, cs, codes, pairs, list, R + 2 * kClsThread, heads + kClsThread,
@@ -914,8 +897,8 @@ void set_s32_rates(ipuma_engine* e) {
 
 void set_default_rates(ipuma_engine* e) {
   // Measured on B200 with the nucleic-acid alphabet (uniform related pairs).
-  const float slot[kNumS16] = {0.385f, 0.286f, 0.263f, 0.25f,  0.3125f, 0.3125f, 0.3f,    0.33f,   0.27f,   0.25f,
-                               0.36f,  0.31f,  0.28f,  0.26f, 0.25f,   0.25f,   0.3125f, 0.3125f, 0.3125f, 0.3125f};
+  const float slot[kNumS16] = {0.385f, 0.286f, 0.263f, 0.25f, 0.3125f, 0.3125f, 0.3f, 0.33f,
+                               0.27f,  0.25f,  0.36f,  0.31f, 0.28f,   0.26f,   0.25f, 0.25f};
   for (int c = 0; c < kNumS16; ++c) {
     e->slot_ps[c] = slot[c];
     e->strip_ps[c] = 0.f;
@@ -934,7 +917,7 @@ std::string tune_key(const ipuma_engine* e) {
   char buf[512];
   // The rates are those of the engine's kernels, which differ by mode: a
   // full alignment (forward + reverse pass) takes longer per cell.
-  snprintf(buf, sizeof(buf), "%s|sm%d%d|M=%d|sim=%d|gI=%d|gE=%d|fwd=%d|v7", prop.name, prop.major, prop.minor, e->M,
+  snprintf(buf, sizeof(buf), "%s|sm%d%d|M=%d|sim=%d|gI=%d|gE=%d|fwd=%d|v6", prop.name, prop.major, prop.minor, e->M,
            e->sw.similarity, e->sw.gap_init, e->sw.gap_extend, e->sc.forwardOnly);
   for (char* c = buf; *c; ++c)
     if (*c == '\t' || *c == '\n') *c = ' ';
@@ -1082,10 +1065,6 @@ int run_autotune(ipuma_engine* e, const char* cache_path) {
       case 13: grid = batched_grid<Lane16, 11, 16>(e, e->M); break;
       case 14: grid = batched_grid<Lane16, 13, 16>(e, e->M); break;
       case 15: grid = batched_grid<Lane16, 15, 16>(e, e->M); break;
-      case 16: grid = batched_grid<Lane16, 10, 32>(e, e->M); break;
-      case 17: grid = batched_grid<Lane16, 13, 32>(e, e->M); break;
-      case 18: grid = batched_grid<Lane16, 14, 32>(e, e->M); break;
-      case 19: grid = batched_grid<Lane16, 15, 32>(e, e->M); break;
       default: grid = (int)(thread_threads<16>(e) / kThreads); break;
     }
     const int minPairs = grid * kWarpsPerBlock * perItem * rounds;
