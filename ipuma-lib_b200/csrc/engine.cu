@@ -137,7 +137,7 @@ constexpr int kShareModeMaxPairs = 48000;
 // padding on large batches; a smaller batch uses the 64-column steps only
 // (K = 4, 8, 12, 16), since every class launch costs a few microseconds
 // even when empty.
-constexpr int kFineClassMinPairs = 150000;
+constexpr int kFineClassMinPairs = 50000;
 constexpr unsigned kCoarseClasses = (1u << 0) | (1u << 1) | (1u << 2) | (1u << 3) | (1u << 4) | (1u << 5);
 constexpr unsigned kFineClasses = (1u << 7) | (1u << 8) | (1u << 9) | (1u << 10) | (1u << 11) | (1u << 12) |
                                   (1u << 13) | (1u << 14) | (1u << 15);
@@ -380,6 +380,11 @@ struct RunBufs {
   DevBuf* list;
   DevBuf* ovf;
   DevBuf* flag;
+  // First of the two class streams of alternating launches (0 or 2): a
+  // second buffer set runs its classes on streams of its own, so its
+  // launches fill the tails of a run on the first set instead of queueing
+  // behind them.
+  int cls_base = 0;
 };
 
 // The engine's default set (control block at the start of d_ctl).
@@ -670,7 +675,7 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
   if (conc) CUDA_TRY(cudaEventRecord(e->fork_ev, s));
   // Stream of a class: its own (shares) or one of two by launch position.
   auto stream_of = [&](int cls) -> int {
-    if (mode == 2) return bp.slot_of[cls];
+    if (mode == 2) return rb.cls_base + bp.slot_of[cls];
     return cls;
   };
   auto on = [&](int cls) -> cudaStream_t {
@@ -1278,7 +1283,7 @@ WireSet wire_set(ipuma_engine* e, int k) {
   if (k == 0) return WireSet{&e->d_inputs, &e->d_wres, &e->d_pairs, &e->d_ctl, main_bufs(e), e->stream};
   WireBufs& w = e->w1;
   return WireSet{&w.inputs, &w.results, &w.pairs, &w.ctl,
-                 RunBufs{w.ctl.as<int>(), &w.scratch, &w.list, &w.ovf, &w.flag}, e->wstream1};
+                 RunBufs{w.ctl.as<int>(), &w.scratch, &w.list, &w.ovf, &w.flag, 2}, e->wstream1};
 }
 
 int take_event(ipuma_engine* e, cudaEvent_t* ev) {
@@ -1860,7 +1865,7 @@ static int compare_host(ipuma_engine* e, const uint8_t* codes, size_t n_codes, i
       if (!ev) CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     int nmax = 0;
     for (int k = 0; k < nch; ++k) nmax = std::max(nmax, cbeg[k + 1] - cbeg[k]);
-    const RunBufs rb1{nullptr, &e->x_scratch, &e->x_list, &e->x_ovf, &e->x_flag};
+    const RunBufs rb1{nullptr, &e->x_scratch, &e->x_list, &e->x_ovf, &e->x_flag, 2};
     if ((rc = e->d_ctl.ensure(sizeof(int) * CTL_INTS * (size_t)nch, s))) return rc;
     if ((rc = reserve_bufs(e, main_bufs(e), s, nmax, maxA, maxB))) return rc;
     if ((rc = reserve_bufs(e, rb1, s, nmax, maxA, maxB))) return rc;
