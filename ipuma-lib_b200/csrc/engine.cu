@@ -137,7 +137,7 @@ constexpr int kShareModeMaxPairs = 48000;
 // padding on large batches; a smaller batch uses the 64-column steps only
 // (K = 4, 8, 12, 16), since every class launch costs a few microseconds
 // even when empty.
-constexpr int kFineClassMinPairs = 50000;
+constexpr int kFineClassMinPairs = 150000;
 constexpr unsigned kCoarseClasses = (1u << 0) | (1u << 1) | (1u << 2) | (1u << 3) | (1u << 4) | (1u << 5);
 constexpr unsigned kFineClasses = (1u << 7) | (1u << 8) | (1u << 9) | (1u << 10) | (1u << 11) | (1u << 12) |
                                   (1u << 13) | (1u << 14) | (1u << 15);
