@@ -1519,7 +1519,7 @@ int ipuma_gpu_create(const ipuma_sw_config* sw, const ipuma_algo_config* algo, i
   // pass sends pairs whose main diagonal may pass the signed limit to the
   // hybrid class.
   e->sc.s16Limit = 32767 - std::max(0, e->maxSub);
-  e->sc.u16Limit = 65535 - LaneHi::BIAS - std::max(0, e->maxSub);
+  e->sc.u16Limit = 65535 - LaneB16x2::BIAS - std::max(0, e->maxSub);
   e->sc.maxSub = std::max(0, e->maxSub);
   e->sc.bits = 8;
   e->sc.P = m;
