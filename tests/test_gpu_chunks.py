@@ -144,3 +144,21 @@ def test_bad_pair_deep_in_a_large_batch_is_reported():
         small = pairs[:1000].copy()
         got = e.compare(wl.codes, small)
         _same(got, _oracle(wl, wl.codes, small, True), "after a rejected call")
+
+
+def test_bad_pair_in_a_later_chunk_is_reported():
+    """A pair outside the code array in a later chunk of a chunked call is
+    reported by index, and the engine stays usable for the corrected batch."""
+    wl = workloads.dna_batched(n=520_000, seed=47)
+    pairs = ib.make_pairs(wl.a_off, wl.a_len, wl.b_off, wl.b_len)
+    pairs["a_off"][400_123] = wl.codes.size + 5
+    with _engine(wl, True) as e:
+        with pytest.raises(ib.IpumaError) as ei:
+            e.compare(wl.codes, pairs)
+        assert ei.value.code == ib.ERR_INVALID_ARG
+        assert "400123" in str(ei.value)
+        pairs["a_off"][400_123] = wl.a_off[400_123]
+        got = e.compare(wl.codes, pairs)
+        assert e.stats().chunks == 2
+        idx = np.random.default_rng(1).choice(wl.n, 2_000, replace=False)
+        _same(tuple(a[idx] for a in got), _oracle(wl, wl.codes, pairs, True, idx), "after a rejected call")
