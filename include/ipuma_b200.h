@@ -121,7 +121,8 @@ typedef struct ipuma_stats {
   double total_ms;      /* device time including copies                      */
   int64_t cells;        /* sum of |A|*|B| (forward pass, ipuma's definition) */
   int64_t pairs;
-  int64_t s32_pairs;    /* pairs aligned in exact 32-bit lanes               */
+  int64_t s32_pairs;    /* pairs the binning sent to the s32 or hybrid class
+                           (main-diagonal score above the 16-bit limit)      */
   int64_t overflow_reruns; /* s16x2 pairs that were rerun in 32-bit          */
   int32_t launches;     /* kernels launched by the call                      */
   int32_t used_graph;   /* 1 when the call replayed a captured CUDA graph     */

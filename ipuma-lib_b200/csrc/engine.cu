@@ -771,11 +771,13 @@ int check_status(ipuma_engine* e, cudaStream_t s, int nblk = 1) {
   DevStatus stk[kMaxChunks];
   unsigned long long cellsk[kMaxChunks][NCELLS];
   unsigned long long tracek[kMaxChunks][2 * (NCLASS_MAX + 1)];
+  int rangesk[kMaxChunks][2 * NCLASS_MAX];
   nblk = std::max(1, std::min(nblk, kMaxChunks));
   for (int k = 0; k < nblk; ++k) {
     const int* ctl = e->d_ctl.as<int>() + (size_t)k * CTL_INTS;
     CUDA_TRY(cudaMemcpyAsync(&stk[k], ctl + CTL_STATUS, sizeof(DevStatus), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaMemcpyAsync(cellsk[k], ctl + CTL_CELLS, sizeof(cellsk[k]), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(rangesk[k], ctl + CTL_RANGES, sizeof(rangesk[k]), cudaMemcpyDeviceToHost, s));
     if (e->trace)
       CUDA_TRY(cudaMemcpyAsync(tracek[k], ctl + CTL_TRACE, sizeof(tracek[k]), cudaMemcpyDeviceToHost, s));
   }
@@ -811,6 +813,11 @@ int check_status(ipuma_engine* e, cudaStream_t s, int nblk = 1) {
     for (int c = 0; c < NCELLS; ++c) cells[c] += cellsk[k][c];
   }
   e->stats.overflow_reruns = st.overflow_count;
+  // Pairs the binning sent to the s32 and hybrid classes ({start, count}
+  // list ranges per class).
+  e->stats.s32_pairs = 0;
+  for (int k = 0; k < nblk; ++k)
+    e->stats.s32_pairs += (int64_t)rangesk[k][2 * kClsS32 + 1] + (int64_t)rangesk[k][2 * kClsHi + 1];
   e->stats.n_timed = e->n_timed;
   for (int k = 0; k < e->n_timed; ++k) {
     float ms = 0;

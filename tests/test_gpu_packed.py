@@ -139,10 +139,11 @@ def test_protein_5bit_host_call_equals_bytes_and_oracle(forward_only):
         _same(got, want, "5-bit chunks=%d" % chunks)
 
 
-def _device_packed(wl, codes, pairs, bits, forward_only, graphs=0, reruns=None, **opts):
+def _device_packed(wl, codes, pairs, bits, forward_only, graphs=0, reruns=None, routed=None, **opts):
     """compare_device_packed on a device copy of the packed codes (padded as
-    the call requires) and compare_device on the byte codes; `reruns`, when
-    given, collects each call's count of s16x2 pairs rerun in s32."""
+    the call requires) and compare_device on the byte codes; `reruns` and
+    `routed`, when given, collect each call's count of s16x2 pairs rerun in
+    s32 and of pairs the binning sent to the s32 / hybrid classes."""
     torch = pytest.importorskip("torch")
     packed = ib.pack_codes(codes, bits)
     buf = np.zeros(ib.device_packed_bytes(codes.size, bits), np.uint8)
@@ -165,6 +166,8 @@ def _device_packed(wl, codes, pairs, bits, forward_only, graphs=0, reruns=None, 
             outs.append(tuple(out.cpu().numpy()))
             if reruns is not None:
                 reruns.append(int(e.stats().overflow_reruns))
+            if routed is not None:
+                routed.append(int(e.stats().s32_pairs))
     return outs
 
 
@@ -204,14 +207,19 @@ def test_device_packed_high_scores_hybrid_and_s32():
     want = _oracle(base, codes, pairs, True)
     assert want[0].max() > 65535 - 1024 - 11 and (want[0] > 32767).sum() >= 8
     for hybrid in (1, 0):
-        reruns = []
-        got_p, got_b = _device_packed(base, codes, pairs, 5, True, hybrid=hybrid, reruns=reruns)
+        reruns, routed = [], []
+        got_p, got_b = _device_packed(base, codes, pairs, 5, True, hybrid=hybrid, reruns=reruns,
+                                      routed=routed)
         _same(got_p, want, "5-bit high scores hybrid=%d" % hybrid)
         _same(got_b, want, "byte high scores hybrid=%d" % hybrid)
         # Every pair above the s16 limit has a diagonal bound above it (checked
         # on the CPU for this batch), so none starts in s16x2 lanes and has to
         # be rerun: the warp-parallel bound routed them all.
         assert reruns == [0, 0], reruns
+        # A diagonal bound never exceeds the score, so the routed pairs are
+        # exactly those above the limit here (all of them caught).
+        above = int((want[0] > 32767 - 11).sum())
+        assert routed == [above, above], (routed, above)
 
 
 def test_device_packed_exact_kernel_for_unusual_gaps():
