@@ -507,7 +507,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
   int capRows[NP];
 #pragma unroll
   for (int h = 0; h < NP; ++h) capRows[h] = ps[h].blen;
-  const unsigned gmask = (LANES == 32) ? FULL : (0xFFFFu << (threadIdx.x & 16));
+  const unsigned gmask = (LANES == 32) ? FULL : (((1u << LANES) - 1u) << (threadIdx.x & (32 - LANES)));
   using C = Cell<T>;
   const V vgE = C::delta(sc.gE);
   const V vgEp = C::delta(max(sc.gE, sc.gIgE));
