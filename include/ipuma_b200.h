@@ -177,6 +177,13 @@ typedef struct ipuma_stats {
 #define IPUMA_KERNEL_S16_HYBRID 20 /* scores above int16: strips in biased 16-bit halves (score - 31744,
                                       scores up to 65535 - 1024 - max(sim)) while safe, then s32 */
 #define IPUMA_KERNEL_PLAIN_S16 21  /* one-launch-per-batch wire kernel, 16-bit lanes */
+/* 8-lane groups (four per warp), used instead of S16_L16_K4 .. _K8 of the
+ * same strip widths when the codes are 2-bit (four-row profiles) */
+#define IPUMA_KERNEL_S16_L8_K8 22
+#define IPUMA_KERNEL_S16_L8_K10 23
+#define IPUMA_KERNEL_S16_L8_K12 24
+#define IPUMA_KERNEL_S16_L8_K14 25
+#define IPUMA_KERNEL_S16_L8_K16 26
 
 typedef struct ipuma_engine ipuma_engine;
 
@@ -224,7 +231,8 @@ void ipuma_gpu_destroy(ipuma_engine* e);
  *                 through s16x2 class IPUMA_KERNEL_S16_* (value = kind),
  *                 7 = every pair through IPUMA_KERNEL_S16_T_K16, 8, 9, 10 =
  *                 IPUMA_KERNEL_S16_L16_K6, _K10, _K14, 11 .. 16 =
- *                 IPUMA_KERNEL_S16_L16_K5, _K7, _K9, _K11, _K13, _K15
+ *                 IPUMA_KERNEL_S16_L16_K5, _K7, _K9, _K11, _K13, _K15,
+ *                 17 .. 21 = IPUMA_KERNEL_S16_L8_K8, _K10, _K12, _K14, _K16
  *   "concurrent"  3 = by batch size (default): mode 1 below 48,000 pairs,
  *                 mode 2 above; 2 = class launches alternate between two
  *                 streams, so each starts on the SMs the previous one

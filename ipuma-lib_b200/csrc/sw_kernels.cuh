@@ -565,7 +565,7 @@ static __global__ void k_exact(SwConst sc, const int8_t* __restrict__ sim, const
 constexpr int NROWB = 256;    // row buckets (16 per power of two)
 constexpr int NSTRIPB = 16;   // strip-count buckets
 constexpr int NBUCKET = NROWB * NSTRIPB;
-constexpr int NCLASS_MAX = 18;
+constexpr int NCLASS_MAX = 23;
 
 // Log-linear bucket of |B| (16 sub-buckets per power of two): pairs that
 // share a bucket differ by at most 1/16 in rows, so the groups of a warp

@@ -110,7 +110,7 @@ def test_reference_codelet_answers(fixture, forward_only):
         _assert_same(_gpu(case, forward_only), want, case["name"])
 
 
-@pytest.mark.parametrize("tile_k", list(range(1, 17)))
+@pytest.mark.parametrize("tile_k", list(range(1, 22)))
 def test_random_answers_each_tile_width(tile_k):
     """Forces every pair through one s16x2 kernel class (16 or 32 lanes per
     group, 4..16 columns per lane -- widths that are not whole words use
