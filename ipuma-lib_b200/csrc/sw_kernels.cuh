@@ -1,10 +1,11 @@
 // sw_kernels.cuh -- the __global__ kernels of the engine.
 //
-//   k_batched<T, K>   persistent kernel over a cost-ordered work list; each
-//                     warp pulls work items (one pair for s32 lanes, two for
-//                     s16x2) from an atomic queue head.  s16x2 items whose
-//                     score could have left int16 are appended to an overflow
-//                     list that a second k_batched<LaneS32, K> launch reruns.
+//   k_batched<T, K, LANES>  persistent kernel over a cost-ordered work list;
+//                     each warp pulls work items (per group of LANES lanes one
+//                     pair for s32 lanes, two for 16-bit halves) from an
+//                     atomic queue head.  s16x2 items whose score could have
+//                     left int16 are appended to an overflow list that a
+//                     second k_batched<LaneS32, K> launch reruns.
 //   k_plain<K>        the one-launch-per-batch kernel over the reference's
 //                     wire buffer (Seqs || Meta, ipu_batch_affine.cpp:287) with
 //                     results in its Scores || ARanges || BRanges layout; one
@@ -13,7 +14,14 @@
 //                     cell by cell in int32; used for scoring configurations
 //                     that the wavefront kernels do not cover (gI + gE >= 0 or
 //                     gE > 0).
-//   k_bin_*           the cost-binning pre-pass that orders the work list.
+//   k_plain16<K>      the same wire-buffer kernel with two slots per warp in
+//                     s16x2 halves (a slot that could leave int16 is redone
+//                     in s32 by the same warp).
+//   k_bin_*           the cost-binning pre-pass that orders the work list:
+//                     k_bin_total (batch cells), k_bin_bound (main-diagonal
+//                     bounds of the long pairs, a warp per pair), k_bin_count
+//                     (class and bucket of every pair), k_bin_scan (list
+//                     offsets and class shares), k_bin_scatter (the list).
 #pragma once
 #include "sw_device.cuh"
 
