@@ -463,7 +463,9 @@ __device__ __forceinline__ typename T::V raise_to_group(typename T::V best) {
 //
 //   s_prof   : this group's profile area, NP * (P + 1) * LANES * KP bytes
 //   s_simp   : substitution table with the padding column (build_profile)
-//   s_bring  : this group's 64-entry ring of B letters (P low byte, Q high)
+//   s_bring  : this group's rings of B letters, 64 entries per pair (pair h
+//              at s_bring + 64 h), each the byte offset of the letter's
+//              profile row (letter * LANES * KP)
 //   scr      : this group's scratch, 2 * rowsCap int2 (only used when the
 //              pass needs more than one strip)
 //   out      : best cell per pair, in pass coordinates
@@ -486,6 +488,8 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
   const int lane = threadIdx.x & (LANES - 1);
   const int P = sc.P;
   const int profStride = (P + 1) * SWP;
+  const uint8_t* profP = s_prof + lane * KP;  // this lane's columns of pair P's profile
+  const uint8_t* profQ = profP + profStride;  // ... and of pair Q's
 
   const int strip0 = HYB ? ctl->strip0 : 0;
   int rowsG = 0, amax = 0;
@@ -603,15 +607,15 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
       if (LANES + lane < rowsG) chunkNext = bnd(LANES + lane);
     }
 
-    // B letters, LANES rows at a time: lane k of `bnext` holds the letters
-    // of row (t0 + LANES + k) and is parked in the group's ring every LANES
-    // steps.
+    // B letters, LANES rows at a time: lane k of `bnext` holds the profile
+    // row offsets of row (t0 + LANES + k) (pair h in halfword h) and is
+    // parked in the group's rings every LANES steps.
     auto fetch_letters = [&](int r) -> uint32_t {
       uint32_t v = 0;
 #pragma unroll
       for (int h = 0; h < NP; ++h) {
         const int x = (r < ps[h].blen) ? code_at(ps[h].base, ps[h].b + (long long)r * ps[h].db, sc.bits) - sc.pshift : P;
-        v |= (uint32_t)x << (8 * h);
+        v |= (uint32_t)(x * SWP) << (16 * h);
       }
       return v;
     };
@@ -639,10 +643,10 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
       const int i = t - lane;
       if (!decltype(check)::value || (i >= 0 && i < rowsG)) {
         uint32_t wp[KP / 4], wq[KP / 4];
-        const uint32_t letters = s_bring[i & 63];
-        load_profile_row<KP>(wp, s_prof + (letters & 0xff) * SWP + lane * KP);
+        const int slot = i & 63;
+        load_profile_row<KP>(wp, profP + s_bring[slot]);
         if constexpr (NP == 2) {
-          load_profile_row<KP>(wq, s_prof + profStride + (letters >> 8) * SWP + lane * KP);
+          load_profile_row<KP>(wq, profQ + s_bring[64 + slot]);
         } else {
 #pragma unroll
           for (int q = 0; q < KP / 4; ++q) wq[q] = 0;
@@ -732,6 +736,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
       }
       if (t0 > 0) best = raise_to_group<T, LANES>(best);
       s_bring[(t0 + lane) & 63] = (uint16_t)bnext;
+      if constexpr (NP == 2) s_bring[64 + ((t0 + lane) & 63)] = (uint16_t)(bnext >> 16);
       bnext = fetch_letters(t0 + LANES + lane);
       __syncwarp();
       if (hasIn && t0 > 0) {
