@@ -463,9 +463,10 @@ __device__ __forceinline__ typename T::V raise_to_group(typename T::V best) {
 //
 //   s_prof   : this group's profile area, NP * (P + 1) * LANES * KP bytes
 //   s_simp   : substitution table with the padding column (build_profile)
-//   s_bring  : this group's rings of B letters, 64 entries per pair (pair h
-//              at s_bring + 64 h), each the byte offset of the letter's
-//              profile row (letter * LANES * KP)
+//   s_bring  : this group's rings of B letters, 64 entries per pair stored
+//              twice (pair h at s_bring + 128 h, entry e also at e + 64, so
+//              a block of steps reads base + k without wrapping), each the
+//              byte offset of the letter's profile row (letter * LANES * KP)
 //   scr      : this group's scratch, 2 * rowsCap int2 (only used when the
 //              pass needs more than one strip)
 //   out      : best cell per pair, in pass coordinates
@@ -621,14 +622,18 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
     };
     uint32_t bnext = fetch_letters(lane);
 
-    // One wavefront step: lane works on row t - lane (when CHECK, only if
-    // that row exists for its group).
-    auto step = [&](int t, auto check) {
+    // Ring slot of this lane's row at the first step of the current block.
+    int ringBase = 0;
+
+    // One wavefront step, step k of the block starting at t0 = t - k: lane
+    // works on row t - lane (when CHECK, only if that row exists for its
+    // group).
+    auto step = [&](int t, int k, auto check) {
       V recvY = __shfl_up_sync(FULL, outY, 1, LANES);
       V recvE = __shfl_up_sync(FULL, outE, 1, LANES);
       if (hasIn) {
-        const int bx = __shfl_sync(FULL, chunk.x, t & (LANES - 1), LANES);
-        const int by = __shfl_sync(FULL, chunk.y, t & (LANES - 1), LANES);
+        const int bx = __shfl_sync(FULL, chunk.x, k, LANES);
+        const int by = __shfl_sync(FULL, chunk.y, k, LANES);
         if (lane == 0) {
           recvY = (V)bx;
           recvE = (V)by;
@@ -643,10 +648,10 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
       const int i = t - lane;
       if (!decltype(check)::value || (i >= 0 && i < rowsG)) {
         uint32_t wp[KP / 4], wq[KP / 4];
-        const int slot = i & 63;
+        const int slot = ringBase + k;  // (i mod 64), < 64 + LANES
         load_profile_row<KP>(wp, profP + s_bring[slot]);
         if constexpr (NP == 2) {
-          load_profile_row<KP>(wq, profQ + s_bring[64 + slot]);
+          load_profile_row<KP>(wq, profQ + s_bring[128 + slot]);
         } else {
 #pragma unroll
           for (int q = 0; q < KP / 4; ++q) wq[q] = 0;
@@ -735,8 +740,12 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
         }
       }
       if (t0 > 0) best = raise_to_group<T, LANES>(best);
-      s_bring[(t0 + lane) & 63] = (uint16_t)bnext;
-      if constexpr (NP == 2) s_bring[64 + ((t0 + lane) & 63)] = (uint16_t)(bnext >> 16);
+      {
+        const int w = (t0 + lane) & 63;
+        s_bring[w] = s_bring[w + 64] = (uint16_t)bnext;
+        if constexpr (NP == 2) s_bring[128 + w] = s_bring[192 + w] = (uint16_t)(bnext >> 16);
+      }
+      ringBase = (t0 - lane) & 63;
       bnext = fetch_letters(t0 + LANES + lane);
       __syncwarp();
       if (hasIn && t0 > 0) {
@@ -746,10 +755,10 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
       }
       if (t0 >= LANES - 1 && t0 + LANES - 1 < rowsMin) {
 #pragma unroll kStepUnroll
-        for (int k = 0; k < LANES; ++k) step(t0 + k, std::false_type{});
+        for (int k = 0; k < LANES; ++k) step(t0 + k, k, std::false_type{});
       } else {
 #pragma unroll 1
-        for (int k = 0; k < LANES; ++k) step(t0 + k, std::true_type{});
+        for (int k = 0; k < LANES; ++k) step(t0 + k, k, std::true_type{});
       }
     }
 

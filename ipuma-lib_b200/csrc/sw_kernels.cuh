@@ -102,7 +102,7 @@ struct SmemLayout {
   // M = alphabet size (substitution table), P = letters of the profile.
   __host__ __device__ static int simp_bytes(int M) { return ((M * (M + 1)) + 15) & ~15; }
   __host__ __device__ static int prof_bytes(int P) { return T::NP * (P + 1) * LANES * ProfileWords<K>::KP; }
-  __host__ __device__ static int ring_bytes() { return 64 * 2 * T::NP; }  // a uint16 ring per pair
+  __host__ __device__ static int ring_bytes() { return 128 * 2 * T::NP; }  // a doubled uint16 ring per pair
   __host__ __device__ static int group_bytes(int P) { return (prof_bytes(P) + ring_bytes() + 15) & ~15; }
   __host__ __device__ static int warp_bytes(int P) { return GROUPS * group_bytes(P); }
   __host__ __device__ static int total(int M, int P, int warps) { return simp_bytes(M) + warps * warp_bytes(P); }
