@@ -49,7 +49,7 @@ METRIC = "bit-exact GCUPS (forward pass, score + end coordinates)"
 # from one ncu capture of that kernel on the same workload
 # (profiles/k_batched_s16x2_L16_K15_dna_1m.md: a launch reads the codes of
 # its own pairs, so its traffic scales with its cells).
-TRAFFIC_PER_CELL = {"dna_batched": 0.00602}
+TRAFFIC_PER_CELL = {"dna_batched": 0.00622}
 
 
 def parse(argv=None):
