@@ -1818,12 +1818,13 @@ static int compare_host(ipuma_engine* e, const uint8_t* codes, size_t n_codes, i
   // batches are checked on several threads.
   int32_t cbeg[kMaxChunks + 1];
   // Chunk k+1's upload overlaps chunk k's kernels, so chunks grow (weights
-  // 1, 3, 6, 9, ...: 10 %, 30 %, 60 % for three chunks) and the first one,
+  // 1, 5.67, 11.3, ...: 6 %, 31 %, 63 % for three chunks) and the first one,
   // whose upload no kernel hides, is the smallest.  (1M DNA pairs, 2-bit
-  // codes, B200: 17.9-18.4 ms per call against 19.1-19.5 with equal chunks.)
+  // codes, B200: 16.9-17.5 ms per call against 17.7-18.0 with 10/30/60 %
+  // chunks and 19.1-19.5 with equal ones.)
   {
     double w[kMaxChunks], tot = 0, acc = 0;
-    for (int k = 0; k < nch; ++k) tot += (w[k] = k == 0 ? 1.0 : 3.0 * k);
+    for (int k = 0; k < nch; ++k) tot += (w[k] = k == 0 ? 1.0 : 5.67 * k);
     cbeg[0] = 0;
     for (int k = 1; k <= nch; ++k) {
       acc += w[k - 1];
