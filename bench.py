@@ -14,7 +14,8 @@ pinned inputs and outputs, copies included.  `targets` holds the single-GPU targ
 engine: the batched engine against the plain one-launch-per-batch kernel (in
 s32 and in s16x2 lanes, on the same pairs in the reference wire format) on
 the 200,000-pair protein batch and the 500,000-pair heavy-tailed protein
-batch, and the serving loop at 64-pair requests.
+batch, the serving loop at 64-pair requests, and strip teams (the warps of a
+block sharing one long pair couple's strips) on a small batch of long pairs.
 
 `--gpus N` runs N ranks, one per GPU (it re-launches itself through
 torch.distributed.run when WORLD_SIZE is unset): every rank aligns its own
@@ -459,6 +460,43 @@ def protein_target(ib, torch, wl, dev, local, stream, reps):
     }
 
 
+def long_pair_target(ib, reps=3):
+    """A small batch of long pairs through the host-buffer call: 296 unrelated
+    6000 x 6000 protein pairs (148 two-pair items, one per SM), with strip
+    teams (the default of a forward-only engine) and with one warp per item
+    (team_warps 0).  The results of both must be identical and match the
+    oracle on a sample."""
+    import oracle
+    n, length = 296, 6000
+    rng = np.random.default_rng(20)
+    codes = rng.integers(0, 20, 2 * n * length).astype(np.uint8)
+    off = np.arange(2 * n, dtype=np.int64) * length
+    lens = np.full(n, length, dtype=np.int32)
+    pairs = ib.make_pairs(off[0::2], lens, off[1::2], lens)
+    sw = ib.sw_config(-11, -1, 1, -1, -1, "blosum62", "aa")
+    ms, res = {}, {}
+    for warps in (8, 0):
+        with ib.Engine(sw, ib.algo_config(forward_only=True)) as e:
+            e.set_option("team_warps", warps)
+            e.compare(codes, pairs)  # warm-up: autotuning and buffers
+            best = float("inf")
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                res[warps] = e.compare(codes, pairs)
+                best = min(best, time.perf_counter() - t0)
+            ms[warps] = best * 1e3
+    chk = np.array([0, n // 2, n - 1])
+    want = oracle.sw_batch(codes, pairs["a_off"][chk], pairs["a_len"][chk], pairs["b_off"][chk],
+                           pairs["b_len"][chk], oracle.select_matrix("blosum62"), -11, -1,
+                           forward_only=True)
+    mism = int(sum((res[8][k][chk] != want[k]).sum() for k in range(3)))
+    return {"pairs": n, "lengths": "%d x %d" % (length, length), "call": "ipuma_gpu_compare, host buffers",
+            "teams_of_8_ms": ms[8], "one_warp_per_item_ms": ms[0], "speedup": ms[0] / ms[8],
+            "teams_gcups": n * length * length / (ms[8] * 1e-3) / 1e9,
+            "bit_identical": all(np.array_equal(a, b) for a, b in zip(res[8], res[0])),
+            "oracle_sample": {"pairs": int(chk.size), "mismatching_fields": mism}}
+
+
 def serving_section(args, ib, dev, local, wls, peak):
     """Open-loop Poisson sweep of the serving loop on resident sequence sets:
     50% DNA / 50% protein requests (subsets of the DNA and protein
@@ -715,11 +753,13 @@ def main(argv=None):
         tg = {"what": "1 GPU: the batched engine against the plain one-launch-per-batch kernel "
                       "(s32 and s16x2 lanes, same pairs in the wire format) on the mixed-length "
                       "protein batches, target >= 3x; the serving loop at 64-pair requests, "
-                      "target >= 80% of the device rate with p99 < 50 ms"}
+                      "target >= 80% of the device rate with p99 < 50 ms; strip teams on a small "
+                      "batch of long pairs against one warp per item"}
         tg["protein_mixed_500k"] = protein_target(ib, torch, wls["protein_mixed"], dev, local,
                                                   stream, args.target_reps)
         tg["protein_200k"] = protein_target(ib, torch, wls["protein"], dev, local, stream,
                                             args.target_reps)
+        tg["long_pairs_small_batch"] = long_pair_target(ib)
         if plain:
             tg["dna_batched_1m"] = {"batched_gcups": value,
                                     "plain_s32_gcups": plain["s32"]["gcups"],

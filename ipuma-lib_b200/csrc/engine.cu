@@ -97,7 +97,7 @@ struct ClassDef {
   int lanes, k, kind, width;
 };
 constexpr int kNumS16 = 21;     // s16x2 classes chosen by cost
-constexpr int kNumClasses = kNumS16 + 2;  // + the s32 class + the hybrid class
+constexpr int kNumClasses = kNumS16 + 3;  // + the s32 class, the hybrid class, the strip-team class
 constexpr ClassDef kClasses[kNumClasses] = {
     {16, 4, IPUMA_KERNEL_S16_L16_K4, 64},    {16, 8, IPUMA_KERNEL_S16_L16_K8, 128},
     {16, 12, IPUMA_KERNEL_S16_L16_K12, 192}, {16, 16, IPUMA_KERNEL_S16_L16_K16, 256},
@@ -111,6 +111,7 @@ constexpr ClassDef kClasses[kNumClasses] = {
     {8, 12, IPUMA_KERNEL_S16_L8_K12, 96},    {8, 14, IPUMA_KERNEL_S16_L8_K14, 112},
     {8, 16, IPUMA_KERNEL_S16_L8_K16, 128},
     {32, 16, IPUMA_KERNEL_S32_K16, 512},     {32, 16, IPUMA_KERNEL_S16_HYBRID, 512},
+    {32, 16, IPUMA_KERNEL_S16_TEAM, 512},
 };
 constexpr int kClsWidest = 5;  // widest wavefront class (very long |A|)
 constexpr int kMaxTimed = IPUMA_MAX_TIMED;  // launches timed per call (time_launches)
@@ -119,6 +120,14 @@ constexpr int kClsS32 = kNumS16;
 // Hybrid class: pairs whose score can pass int16 (main-diagonal bound) run
 // their safe strips in s16x2 and the rest in s32 (option "hybrid").
 constexpr int kClsHi = kNumS16 + 1;
+// Strip-team class (k_strips<16>, forward-only engines): the warps of a
+// block share one item's 512-column strips, so a long pair finishes up to
+// `warps` times sooner.  Chosen for pairs of at least two strips whose
+// one-warp latency the batch cannot hide (pair_key), and for |A| above
+// long_a.  Warps per team: option "team_warps" (0 = off), capped by the
+// batch's strip count.
+constexpr int kClsTeam = kNumS16 + 2;
+constexpr int kTeamWarpsDefault = 8;
 // Per-thread class: rows it accepts (its boundary scratch is rows x threads)
 // and the share of the batch's time one of its pairs may take.
 constexpr int kThrMaxRows = 2048;
@@ -213,6 +222,8 @@ struct ipuma_engine {
   int trace = 0;      // option "trace": first start / last end of every class launch
   int graphs = 0;
   int tile_k = 0;
+  int team_warps = kTeamWarpsDefault;  // option "team_warps": warps of a strip team (0 = no team class)
+  int smem_optin = 0;                  // shared memory a block may opt in to
   int time_launches = 0;
   // option "thread_class": the per-thread class may be chosen.  Off by
   // default: on the benchmark batches its divergence between pairs of
@@ -314,13 +325,15 @@ void raise_smem_limit(int device, K kernel, int smem) {
 // once per kernel and engine (engine creation warms the cache, so no
 // occupancy query or attribute change happens during a graph capture).
 template <class K>
-int occupancy_grid(ipuma_engine* e, K kernel, int smem) {
-  const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), smem);
+int occupancy_grid(ipuma_engine* e, K kernel, int smem, int threads = kThreads) {
+  // Key: the kernel and its shared memory (and block size, when not kThreads).
+  const auto key =
+      std::make_pair(reinterpret_cast<const void*>(kernel), smem + (threads == kThreads ? 0 : threads << 20));
   auto it = e->grid_cache.find(key);
   if (it != e->grid_cache.end()) return it->second;
   int nb = 0;
   raise_smem_limit(e->device, kernel, smem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, kThreads, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem);
   if (nb < 1) nb = 1;
   e->grid_cache[key] = nb * e->nsm;
   return nb * e->nsm;
@@ -344,6 +357,29 @@ template <class T, int K, int LANES, bool HYB = false>
 int batched_grid(ipuma_engine* e, int P) {
   return e->sc.forwardOnly ? occupancy_grid(e, k_batched<T, K, LANES, HYB, true>, smem_for<T, K, LANES>(e, P))
                            : occupancy_grid(e, k_batched<T, K, LANES, HYB, false>, smem_for<T, K, LANES>(e, P));
+}
+
+int team_smem(const ipuma_engine* e, int P, int warps) {
+  return SmemLayout<Lane16, 16, 32>::total(e->M, P, warps);
+}
+
+// Static shared memory of k_strips (progress words, merge slots) plus slack.
+constexpr int kTeamStaticSmem = 1024;
+
+// Warps of a strip team for a batch whose longest A is maxA, with a
+// P-letter profile: the engine's team_warps, but no more than the strips
+// of that A (a warp without a strip would idle for the whole item) and no
+// more than the shared memory holds.  0: no team (fewer than 2 warps).
+int team_warps_for(const ipuma_engine* e, int P, int maxA) {
+  const int strips = (std::max(maxA, 1) + kClasses[kClsTeam].width - 1) / kClasses[kClsTeam].width;
+  int w = std::min({e->team_warps, strips, kTeamMaxWarps});
+  while (w >= 2 && team_smem(e, P, w) + kTeamStaticSmem > e->smem_optin) --w;
+  return w >= 2 ? w : 0;
+}
+
+// Grid of a k_strips<16> launch with `warps` warps per block.
+int team_grid(ipuma_engine* e, int P, int warps) {
+  return occupancy_grid(e, k_strips<16>, team_smem(e, P, warps), 32 * warps);
 }
 
 template <int K>
@@ -384,6 +420,9 @@ int max_batched_groups(ipuma_engine* e) {
     g = std::max(g, batched_grid<Lane16, 16, 32>(e, P));
     g = std::max(g, batched_grid<LaneS32, 16, 32>(e, P));
     g = std::max(g, batched_grid<LaneHi, 16, 32, true>(e, P));
+    // Warm the cache of the team grids (no occupancy query during a capture).
+    for (int w = 2; w <= std::min(e->team_warps, kTeamMaxWarps); ++w)
+      if (team_smem(e, P, w) + kTeamStaticSmem <= e->smem_optin) team_grid(e, P, w);
   }
   return g * kWarpsPerBlock;
 }
@@ -452,6 +491,25 @@ int launch_batched(ipuma_engine* e, const SwConst& sc, const RunBufs& rb, cudaSt
   return timed_end(e, s);
 }
 
+// Launches the strip-team class (`warps` warps per block) over its list range.
+int launch_team(ipuma_engine* e, const SwConst& sc, const RunBufs& rb, cudaStream_t s, const uint8_t* codes,
+                const PairDesc* pairs, const int* list, const int* range, int* head, long rowsCap, int* score,
+                int* arange, int* brange, int warps) {
+  const int smem = team_smem(e, sc.P, warps);
+  const int grid = team_grid(e, sc.P, warps);
+  int* ctl = rb.ctl;
+  auto* cells = reinterpret_cast<unsigned long long*>(ctl + CTL_CELLS);
+  int rc;
+  if ((rc = timed_begin(e, s, kClasses[kClsTeam].kind, kClsTeam))) return rc;
+  k_strips<16><<<grid, 32 * warps, smem, s>>>(
+      sc, e->d_sim.as<int8_t>(), codes, pairs, list, range, head, rb.scratch->as<int2>(), rowsCap, score, arange,
+      brange, rb.ovf->as<int>(), cells + CELLS_RERUN, reinterpret_cast<DevStatus*>(ctl + CTL_STATUS),
+      reinterpret_cast<const ClassAllot*>(ctl + CTL_ALLOT) + kClsTeam,
+      e->trace ? reinterpret_cast<unsigned long long*>(ctl + CTL_TRACE) + 2 * kClsTeam : nullptr);
+  CUDA_TRY(cudaGetLastError());
+  return timed_end(e, s);
+}
+
 // Launches the per-thread class over its list range; rowsCap = rows of
 // the boundary scratch per thread.
 template <int K>
@@ -514,6 +572,12 @@ void class_grids(ipuma_engine* e, int P, int maxA, int maxB, int* grid, long lon
       case 18: grid[c] = batched_grid<Lane16, 12, 8>(e, P); break;
       case 19: grid[c] = batched_grid<Lane16, 14, 8>(e, P); break;
       case 20: grid[c] = batched_grid<Lane16, 16, 8>(e, P); break;
+      case kClsTeam: {
+        const int w = team_warps_for(e, P, maxA);
+        grid[c] = w ? team_grid(e, P, w) : 0;
+        spb[c] = (long long)w * rowsCap;  // one boundary column per warp of a team
+        continue;
+      }
       default: grid[c] = batched_grid<LaneS32, 16, 32>(e, P); break;
     }
     if (c == kClsThread)
@@ -548,7 +612,7 @@ size_t scratch_int2(ipuma_engine* e, int maxA, int maxB) {
 // The hybrid class and the widest class (the long pairs of a heavy-tailed
 // batch) come first and land on different streams, so the widest class's
 // blocks start on the SMs the hybrid class frees during its tail.
-constexpr int kLaunchOrder[kNumClasses] = {22, 5, 21, 4, 6, 3, 15, 9, 14, 2, 13, 8, 12, 1, 20, 11, 19, 7, 18, 10, 17, 0, 16};
+constexpr int kLaunchOrder[kNumClasses] = {23, 22, 5, 21, 4, 6, 3, 15, 9, 14, 2, 13, 8, 12, 1, 20, 11, 19, 7, 18, 10, 17, 0, 16};
 
 int reserve_bufs(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, int n, int maxA, int maxB) {
   int rc;
@@ -640,8 +704,13 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
     for (const auto& w : kNarrowPairs)
       if ((enabled >> w[0]) & 1u) enabled = (enabled & ~(1u << w[0])) | (1u << w[1]);
   }
+  // Strip teams: forward-only engines, batches with pairs of two strips or more.
+  const int teamW = (e->sc.forwardOnly && e->team_warps >= 2) ? team_warps_for(e, sc.P, maxA) : 0;
+  if (teamW >= 2 && maxA > kClasses[kClsTeam].width) enabled |= 1u << kClsTeam;
   if (e->tile_k > 0) enabled |= 1u << (e->tile_k - 1);
   bp.enabled = enabled;
+  bp.team_cls = ((enabled >> kClsTeam) & 1u) ? kClsTeam : -1;
+  bp.team_warps = std::max(teamW, 1);
   class_grids(e, sc.P, maxA, maxB, bp.grid, bp.scr_per_block);
   bp.scr_cap = (long long)(rb.scratch->cap / sizeof(int2));
   float slot_min = 1e30f;
@@ -651,6 +720,9 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
     bp.step_ps[c] = e->slot_ps[c] * 64.f * (float)kClasses[c].k * (float)(bp.grid[c] * kWarpsPerBlock);
     if (c != kClsThread) slot_min = std::min(slot_min, e->slot_ps[c]);
   }
+  // A warp of a team steps like one of the widest class's warps.
+  bp.step_ps[kClsTeam] =
+      e->slot_ps[kClsTeam] * 64.f * (float)kClasses[kClsTeam].k * (float)(bp.grid[kClsTeam] * bp.team_warps);
   bp.batch_ps_per_cell = slot_min / kPackingEfficiency;
   bp.lat_share = e->latency_share;
   bp.lat_min_ps = kLatencyMinBatchPs;
@@ -727,6 +799,14 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
       return rc;                                                                                       \
     if ((rc = done(cls))) return rc;                                                                   \
     ++*launches;                                                                                       \
+  }
+  if ((enabled >> kClsTeam) & 1u) {
+    cudaStream_t cs = on(kClsTeam);
+    if ((rc = launch_team(e, sc, rb, cs, codes, pairs, list, R + 2 * kClsTeam, heads + kClsTeam, rowsCap, score,
+                          arange, brange, teamW)))
+      return rc;
+    if ((rc = done(kClsTeam))) return rc;
+    ++*launches;
   }
   if ((enabled >> kClsHi) & 1u) {
     cudaStream_t cs = on(kClsHi);
@@ -937,6 +1017,10 @@ void set_s32_rates(ipuma_engine* e) {
   // strips run there).
   e->slot_ps[kClsHi] = e->slot_ps[kClsS32];
   e->strip_ps[kClsHi] = e->strip_ps[kClsS32];
+  // Strip teams run the widest class's strips (plus the waits of a
+  // pipeline that fills and drains once per item: modelled in pair_key).
+  e->slot_ps[kClsTeam] = e->slot_ps[kClsWidest];
+  e->strip_ps[kClsTeam] = e->strip_ps[kClsWidest];
 }
 
 void set_default_rates(ipuma_engine* e) {
@@ -1520,6 +1604,7 @@ int ipuma_gpu_create(const ipuma_sw_config* sw, const ipuma_algo_config* algo, i
     return fail(IPUMA_ERR_NO_DEVICE, "device %d is sm_%d%d; this library is built for sm_100a",
                 device, prop.major, prop.minor);
   e->nsm = prop.multiProcessorCount;
+  e->smem_optin = (int)prop.sharedMemPerBlockOptin;
   CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
   for (auto& ev : e->ev) CUDA_TRY(cudaEventCreate(&ev));
   // Class streams and their fork/join events (created here: no stream or
@@ -1649,9 +1734,16 @@ int ipuma_gpu_set_option(ipuma_engine* e, const char* name, int64_t value) {
       return fail(IPUMA_ERR_INVALID_ARG, "chunks must be 0 (automatic) .. %d", kMaxChunks);
     e->chunks = (int)value;
   } else if (k == "tile_k") {
-    if (value < 0 || value > kNumS16)
-      return fail(IPUMA_ERR_INVALID_ARG, "tile_k must be 0 (automatic) or a kernel class 1..%d", kNumS16);
+    if (value < 0 || (value > kNumS16 && value != kClsTeam + 1))
+      return fail(IPUMA_ERR_INVALID_ARG, "tile_k must be 0 (automatic), a kernel class 1..%d or %d (strip teams)",
+                  kNumS16, kClsTeam + 1);
+    if (value == kClsTeam + 1 && !e->sc.forwardOnly)
+      return fail(IPUMA_ERR_INVALID_ARG, "tile_k %d (strip teams) needs a forward-only engine", kClsTeam + 1);
     e->tile_k = (int)value;
+  } else if (k == "team_warps") {
+    if (value != 0 && (value < 2 || value > kTeamMaxWarps))
+      return fail(IPUMA_ERR_INVALID_ARG, "team_warps must be 0 (no strip teams) or 2..%d", kTeamMaxWarps);
+    e->team_warps = (int)value;
   } else {
     return fail(IPUMA_ERR_INVALID_ARG, "unknown option '%s'", name);
   }

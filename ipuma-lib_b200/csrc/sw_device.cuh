@@ -94,6 +94,35 @@ struct PassStop {
   int target[2] = {0, 0};  // per pair; 0 for a pair without a reverse pass
 };
 
+// Strip team: the `warps` warps of a block run one pass together, warp w
+// taking strips w, w + warps, w + 2 * warps, ...  Strip s writes its
+// boundary column to scratch buffer s % warps and, after every block of
+// steps, publishes (s << 16) | rows-written in prog[warp]; strip s + 1
+// waits for the rows it is about to read.  The values only grow within a
+// pass (a warp moves to higher strips), so a consumer never mistakes the
+// producer's next strip for the one it reads.  Strip s + warps overwrites
+// buffer s % warps only after strip s + 1 has read those rows: it depends,
+// through strips s + warps - 1, ..., s + 2, on rows that strip s + 1
+// produced after reading them.  Every wait is bounded: past kTeamWaitNs
+// the warp sets `*err` (if 0) to errCode and `*abort`, and every warp of
+// the team leaves the pass at its next wait or block.
+constexpr unsigned long long kTeamWaitNs = 2000000000ull;
+struct StripTeam {
+  int* prog = nullptr;   // shared memory, one word per warp
+  int* abort = nullptr;  // shared memory: nonzero once any warp gave up
+  int* err = nullptr;    // status word of the launch
+  int errCode = 0;
+  int warp = 0;
+  int warps = 1;
+};
+
+// Device clock in nanoseconds (bounded waits; the trace of class launches).
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // -------------------------------------------------------------------------
 // Lane types
 // -------------------------------------------------------------------------
@@ -476,11 +505,12 @@ __device__ __forceinline__ typename T::V raise_to_group(typename T::V best) {
 // it; an s32 pass with ctl->strip0 > 0 starts there from the packed
 // boundary half ctl->bndHalf in buffer ctl->scrBase, keeping `out` (the
 // best of the strips before) and using the two other buffers.
-template <class T, int K, int LANES, bool HYB = false, bool EARLY = false>
+template <class T, int K, int LANES, bool HYB = false, bool EARLY = false, bool TEAM = false>
 __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, const int8_t* s_simp,
                                         uint16_t* s_bring, const PassSeq (&ps)[T::NP], int2* scr,
                                         long rowsCap, Best (&out)[T::NP], PassCtl* ctl = nullptr,
-                                        PassStop stop = PassStop{}) {
+                                        PassStop stop = PassStop{}, StripTeam team = StripTeam{}) {
+  static_assert(!TEAM || (LANES == 32 && !HYB && !EARLY), "strip teams run whole-warp forward passes");
   using V = typename T::V;
   constexpr int SW = LANES * K;          // columns per strip
   constexpr int KP = ProfileWords<K>::KP;
@@ -533,6 +563,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
   // Scratch buffer written by strip s: 0/1 alternating, or for an s32
   // continuation the two buffers other than the one holding its input.
   auto wbuf = [&](int sidx) -> int {
+    if constexpr (TEAM) return sidx % team.warps;
     if (!HYB || strip0 == 0) return sidx & 1;
     return (ctl->scrBase + 1 + ((sidx - strip0) & 1)) % 3;
   };
@@ -540,7 +571,48 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
   // the bound of the next strip.
   V bmax = vZero;
 
-  for (int strip = strip0; strip < nstrips; ++strip) {
+  // TEAM: marks the team as given up (overflow, or a wait that ran out).
+  auto team_fail = [&]() {
+    if constexpr (TEAM) {
+      if (lane == 0) *(volatile int*)team.abort = 1;
+    }
+  };
+  // TEAM: waits until the previous warp published `need` rows of strip
+  // s's boundary.  Warp-uniform result; false once the team gave up.
+  auto team_wait = [&](int s, int need) -> bool {
+    bool ok = true;
+    if constexpr (TEAM) {
+      const int target = (s << 16) | need;
+      const volatile int* pr = team.prog + (team.warp + team.warps - 1) % team.warps;
+      const volatile int* ab = team.abort;
+      unsigned long long t_start = 0;
+      for (int it = 0; *pr < target; ++it) {
+        if (*ab != 0) {
+          ok = false;
+          break;
+        }
+        if ((it & 255) == 0) {
+          const unsigned long long now = global_ns();
+          if (it == 0) t_start = now;
+          if (now - t_start > kTeamWaitNs || it >= (1 << 26)) {
+            atomicCAS(team.err, 0, team.errCode);
+            *(volatile int*)team.abort = 1;
+            ok = false;
+            break;
+          }
+        }
+        __nanosleep(64);
+      }
+      __threadfence_block();  // the boundary rows are read after the flag
+      ok = __all_sync(FULL, ok);
+    }
+    return ok;
+  };
+  bool teamGaveUp = false;
+
+  const int stripFirst = strip0 + (TEAM ? team.warp : 0);
+  const int stripStep = TEAM ? team.warps : 1;
+  for (int strip = stripFirst; strip < nstrips; strip += stripStep) {
     if constexpr (EARLY) {
       if (stop.on && strip > strip0) {
         rowsG = 0;
@@ -603,6 +675,12 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
     // Boundary (Y, Ê) of the previous strip's last column: lane k of the
     // group's chunk registers holds row (chunkBase + k).
     int2 chunk = make_int2(0, 0), chunkNext = make_int2(0, 0);
+    if constexpr (TEAM) {
+      if (hasIn && !team_wait(strip - 1, min(2 * LANES, rowsG))) {
+        teamGaveUp = true;
+        break;
+      }
+    }
     if (hasIn) {
       if (lane < rowsG) chunk = bnd(lane);
       if (LANES + lane < rowsG) chunkNext = bnd(LANES + lane);
@@ -739,6 +817,13 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
           }
         }
       }
+      if constexpr (TEAM) {
+        // Another warp gave up: this pass's results are not used.
+        if (__any_sync(FULL, *(volatile int*)team.abort != 0)) {
+          teamGaveUp = true;
+          break;
+        }
+      }
       if (t0 > 0) best = raise_to_group<T, LANES>(best);
       {
         const int w = (t0 + lane) & 63;
@@ -749,6 +834,12 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
       bnext = fetch_letters(t0 + LANES + lane);
       __syncwarp();
       if (hasIn && t0 > 0) {
+        if constexpr (TEAM) {
+          if (!team_wait(strip - 1, min(t0 + 2 * LANES, rowsG))) {
+            teamGaveUp = true;
+            break;
+          }
+        }
         chunk = chunkNext;
         const int r = t0 + LANES + lane;
         chunkNext = (r < rowsG) ? bnd(r) : make_int2(0, 0);
@@ -760,11 +851,25 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
 #pragma unroll 1
         for (int k = 0; k < LANES; ++k) step(t0 + k, k, std::true_type{});
       }
+      if constexpr (TEAM) {
+        // Lane LANES - 1 wrote the boundary rows up to t0 (those below
+        // rowsG): release them to the next strip's warp.
+        if (hasOut && lane == LANES - 1) {
+          __threadfence_block();
+          *(volatile int*)(team.prog + team.warp) = (strip << 16) | min(t0 + 1, rowsG);
+        }
+      }
+    }
+    if constexpr (TEAM) {
+      if (teamGaveUp) break;
     }
 
     if constexpr (NP == 2) {
       if (!gaveUp) gaveUp = __any_sync(FULL, T::half(best, 0) > lim || T::half(best, 1) > lim);
-      if (gaveUp) return false;
+      if (gaveUp) {
+        team_fail();
+        return false;
+      }
     }
     // Strip result: first column of the lane's snapshot that holds its best.
 #pragma unroll
@@ -796,6 +901,9 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
       __threadfence_block();
       __syncwarp();
     }
+  }
+  if constexpr (TEAM) {
+    if (teamGaveUp) return false;
   }
   return true;
 }

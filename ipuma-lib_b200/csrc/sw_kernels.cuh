@@ -17,6 +17,11 @@
 //   k_plain16<K>      the same wire-buffer kernel with two slots per warp in
 //                     s16x2 halves (a slot that could leave int16 is redone
 //                     in s32 by the same warp).
+//   k_strips<K>       the strip-team kernel: the warps of a block share the
+//                     strips of one item (two pairs in s16x2 halves), each
+//                     strip waiting on the boundary rows of the one before
+//                     (forward pass; long pairs whose latency would end
+//                     the launch).
 //   k_bin_*           the cost-binning pre-pass that orders the work list:
 //                     k_bin_total (batch cells), k_bin_bound (main-diagonal
 //                     bounds of the long pairs, a warp per pair), k_bin_count
@@ -59,16 +64,10 @@ struct ClassAllot {
   int pad;
 };
 
-// Device clock in nanoseconds (the trace of class launches).
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
 constexpr int ERR_SCRATCH = 1;  // a pass needed more scratch rows than provided
 constexpr int ERR_LENGTH = 2;   // a pair exceeded the stated maximum lengths
 constexpr int ERR_RANGE = 3;    // a pair's offsets or lengths lie outside the code array
+constexpr int ERR_WAIT = 4;     // a strip team's wait for a boundary ran out (kTeamWaitNs)
 
 // What a kernel does with one pair descriptor of a device-resident batch,
 // checked before any code is read (the same rules as the host-side check of
@@ -377,6 +376,110 @@ __global__ void __launch_bounds__(128, (FWD && !HYB) ? 4 : 3) k_batched(SwConst 
   if (trace && lane32 == 0) atomicMax(&trace[1], global_ns());
 }
 
+// Strip-team kernel (forward pass only): the blockDim.x / 32 warps of a
+// block align one item -- the two pairs of a 32-lane s16x2 group -- taking
+// its 32 * K wide strips round robin (sw_pass with TEAM), so a long pair
+// finishes up to `warps` times sooner than on one warp.  Each warp keeps
+// the best cell of its own strips; the block merges them with the
+// first-strict-maximum order (better), which is the order-independent
+// total order the one-warp pass applies strip by strip.  A team that gave
+// up (a 16-bit overflow, or a wait past kTeamWaitNs, which also sets
+// ERR_WAIT) sends both pairs to the s32 rerun.  Block scratch: `warps`
+// boundary columns of rowsCap rows.
+constexpr int kTeamMaxWarps = 8;
+template <int K>
+__global__ void __launch_bounds__(256, 2) k_strips(SwConst sc, const int8_t* __restrict__ sim,
+                                                   const uint8_t* __restrict__ codes,
+                                                   const PairDesc* __restrict__ pairs,
+                                                   const int* __restrict__ list, const int* __restrict__ range,
+                                                   int* queue_head, int2* scratch, long rowsCap, int* score,
+                                                   int* arange, int* brange, int* overflow_list,
+                                                   unsigned long long* rerun_cells, DevStatus* st,
+                                                   const ClassAllot* __restrict__ allot,
+                                                   unsigned long long* trace) {
+  if ((int)blockIdx.x >= allot->blocks) return;
+  scratch += allot->base;
+  if (trace && threadIdx.x == 0) atomicMax(&trace[0], ~global_ns());
+  using T = LaneS16x2;
+  using L = SmemLayout<T, K, 32>;
+  constexpr int NP = 2;
+  extern __shared__ __align__(16) uint8_t smem[];
+  __shared__ int s_prog[kTeamMaxWarps];
+  __shared__ int s_abort, s_item;
+  __shared__ Best s_res[kTeamMaxWarps][NP];
+  const int warps = blockDim.x >> 5;
+  const int wib = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  int8_t* s_simp = reinterpret_cast<int8_t*>(smem);
+  uint8_t* s_prof = smem + L::simp_bytes(sc.M) + wib * L::warp_bytes(sc.P);
+  uint16_t* s_bring = reinterpret_cast<uint16_t*>(s_prof + L::prof_bytes(sc.P));
+  load_simp(s_simp, sim, sc);
+
+  const int n = range[1];
+  list += range[0];
+  const int items = (n + NP - 1) / NP;
+  int2* scr = scratch + (long)blockIdx.x * warps * rowsCap;
+  const StripTeam team{s_prog, &s_abort, &st->error, ERR_WAIT, wib, warps};
+  while (true) {
+    __syncthreads();  // the previous item's merge is done; s_simp is loaded
+    if (threadIdx.x == 0) {
+      s_item = atomicAdd(queue_head, 1);
+      s_abort = 0;
+    }
+    if (threadIdx.x < warps) s_prog[threadIdx.x] = -1;
+    __syncthreads();
+    const int item = s_item;
+    if (item >= items) break;
+    int pid[NP];
+    PairDesc d[NP];
+    bool tooLong = false;
+#pragma unroll
+    for (int h = 0; h < NP; ++h) {
+      const int k = item * NP + h;
+      pid[h] = (k < n) ? list[k] : -1;
+      d[h] = (pid[h] >= 0) ? pairs[pid[h]] : PairDesc{0, 0, 0, 0};
+      tooLong |= d[h].b_len > rowsCap;
+    }
+    if (tooLong) {
+      // The host sizes the scratch for the longest B; report, never trap.
+      if (threadIdx.x == 0) atomicCAS(&st->error, 0, ERR_SCRATCH);
+      continue;
+    }
+    PassSeq ps[NP];
+#pragma unroll
+    for (int h = 0; h < NP; ++h) {
+      const bool empty = d[h].a_len <= 0 || d[h].b_len <= 0;
+      ps[h] = PassSeq{codes, d[h].a_off, d[h].b_off, empty ? 0 : d[h].a_len, empty ? 0 : d[h].b_len, 1, 1};
+    }
+    Best out[NP];
+    sw_pass<T, K, 32, false, false, true>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, out, nullptr,
+                                          PassStop{}, team);
+    if (lane == 0) {
+#pragma unroll
+      for (int h = 0; h < NP; ++h) s_res[wib][h] = out[h];
+    }
+    __syncthreads();
+    if (threadIdx.x < NP) {
+      const int h = threadIdx.x;
+      if (pid[h] >= 0) {
+        Best b = s_res[0][h];
+        for (int w = 1; w < warps; ++w) {
+          const Best c = s_res[w][h];
+          if (better(c.s, c.i, c.j, b.s, b.i, b.j)) b = c;
+        }
+        if (s_abort != 0 || b.s > Cell<T>::limit(sc)) {
+          const int slot = atomicAdd(&st->overflow_count, 1);
+          overflow_list[slot] = pid[h];
+          if (rerun_cells) atomicAdd(rerun_cells, (unsigned long long)d[h].a_len * (unsigned long long)d[h].b_len);
+        } else {
+          write_result(sc, b, Best{0, 0, 0}, score, arange, brange, pid[h]);
+        }
+      }
+    }
+  }
+  if (trace && lane == 0) atomicMax(&trace[1], global_ns());
+}
+
 // One-launch-per-batch kernel over the reference wire buffer.
 // Comparison slot g = tile * maxBatches + slot reads Meta[4g..4g+3] =
 // {a_len, a_off, b_len, b_off}, byte offsets into the tile's Seqs region
@@ -573,7 +676,7 @@ static __global__ void k_exact(SwConst sc, const int8_t* __restrict__ sim, const
 constexpr int NROWB = 256;    // row buckets (16 per power of two)
 constexpr int NSTRIPB = 16;   // strip-count buckets
 constexpr int NBUCKET = NROWB * NSTRIPB;
-constexpr int NCLASS_MAX = 23;
+constexpr int NCLASS_MAX = 24;
 
 // Log-linear bucket of |B| (16 sub-buckets per power of two): pairs that
 // share a bucket differ by at most 1/16 in rows, so the groups of a warp
@@ -608,6 +711,8 @@ struct BinParams {
   int long_a;                  // |A| above which the widest class is used
   int widest;                  // that class
   int forced_class;        // >= 0: every s16x2 pair goes to this class
+  int team_cls;            // strip-team class (-1: none in this batch)
+  int team_warps;          // warps per team
   int n_s16_classes;
   int max_a, max_b;        // stated maxima (violations set ERR_LENGTH)
   long long n_codes;       // residues in the code array (pairs past it set ERR_RANGE)
@@ -700,6 +805,16 @@ static __device__ int warp_diagonal_bound(const uint8_t* codes, int bits, long l
   return __shfl_sync(FULL, r.best, 0);
 }
 
+// Steps a team warp starts behind the warp before it: it reads boundary
+// rows two blocks of 32 ahead, which that warp publishes a block later.
+constexpr float kTeamLagSteps = 96.f;
+// Share of the batch's modelled time above which a pair's one-warp latency
+// sends it to a strip team (measured on B200: a 500,000-pair heavy-tailed
+// protein batch, whose 8,000-residue pairs take about a third of its time
+// on one warp, ran 10 % slower with them in teams; batches of a few hundred
+// long pairs ran 3.7-5.6 times faster).
+constexpr float kTeamLatencyShare = 0.5f;
+
 // Class of a pair: the kernel with the lowest modelled time
 //   strips * ((|B| + lanes) * width * slot_ps + strip_ps)
 // where strips * width covers |A|, |B| + lanes counts the fill and drain of
@@ -715,36 +830,62 @@ __device__ __forceinline__ int pair_key(const BinParams& bp, int alen, int blen,
     cls = bp.cls_hi;
   } else if (bp.forced_class >= 0) {
     cls = bp.forced_class;
-  } else if (alen > bp.long_a) {
-    // Very long pairs are few and each keeps one warp busy for long: their
-    // latency, not throughput, sets the end of the launch, and the widest
-    // strips finish a pair in the fewest steps.
-    cls = bp.widest;
   } else {
-    cls = 0;
-    float bestCost = -1.f, bestLat = -1.f;
-    int latCls = 0;
-    const bool thr_ok = bp.thr_on && blen <= bp.thr_max_rows && (float)alen * (float)blen <= thr_cap;
     const float batch_ps = bp.total_cells ? (float)(*bp.total_cells) * bp.batch_ps_per_cell : 0.f;
-    const float lat_cap = batch_ps >= bp.lat_min_ps ? bp.lat_share * batch_ps : 3.0e38f;
-    for (int c = 0; c < bp.n_s16_classes; ++c) {
-      if (!((bp.enabled >> c) & 1u)) continue;
-      if (c == bp.thr_cls && !thr_ok) continue;
-      const int strips = (alen + bp.width[c] - 1) / bp.width[c];
-      const float lat = (float)strips * (float)(blen + bp.lanes[c]) * bp.step_ps[c];
-      if (bestLat < 0.f || lat < bestLat) {
-        bestLat = lat;
-        latCls = c;
+    float bestLat = -1.f;  // one-warp latency of the class picked below
+    if (alen > bp.long_a) {
+      // Very long pairs are few and each keeps one warp busy for long: their
+      // latency, not throughput, sets the end of the launch, and the widest
+      // strips finish a pair in the fewest steps.
+      cls = bp.widest;
+      bestLat = (float)((alen + bp.width[cls] - 1) / bp.width[cls]) * (float)(blen + bp.lanes[cls]) *
+                bp.step_ps[cls];
+    } else {
+      cls = 0;
+      float bestCost = -1.f;
+      int latCls = 0;
+      const bool thr_ok = bp.thr_on && blen <= bp.thr_max_rows && (float)alen * (float)blen <= thr_cap;
+      const float lat_cap = batch_ps >= bp.lat_min_ps ? bp.lat_share * batch_ps : 3.0e38f;
+      for (int c = 0; c < bp.n_s16_classes; ++c) {
+        if (!((bp.enabled >> c) & 1u)) continue;
+        if (c == bp.thr_cls && !thr_ok) continue;
+        const int strips = (alen + bp.width[c] - 1) / bp.width[c];
+        const float lat = (float)strips * (float)(blen + bp.lanes[c]) * bp.step_ps[c];
+        if (bestLat < 0.f || lat < bestLat) {
+          bestLat = lat;
+          latCls = c;
+        }
+        if (lat > lat_cap) continue;
+        const float cost =
+            (float)strips * ((float)(blen + bp.lanes[c]) * (float)bp.width[c] * bp.slot_ps[c] + bp.strip_ps[c]);
+        if (bestCost < 0.f || cost < bestCost) {
+          bestCost = cost;
+          cls = c;
+        }
       }
-      if (lat > lat_cap) continue;
-      const float cost =
-          (float)strips * ((float)(blen + bp.lanes[c]) * (float)bp.width[c] * bp.slot_ps[c] + bp.strip_ps[c]);
-      if (bestCost < 0.f || cost < bestCost) {
-        bestCost = cost;
-        cls = c;
+      if (bestCost < 0.f) {
+        cls = latCls;  // every class is too slow: the fastest
+      } else {
+        bestLat = 0.f;  // a class keeps the pair under the latency cap
       }
     }
-    if (bestCost < 0.f) cls = latCls;  // every class is too slow: the fastest
+    // A strip team, when even the fastest warp would take a large share of
+    // the whole batch's modelled time (kTeamLatencyShare: below it the
+    // other pairs' work hides the pair, and a team's fill and idle warps
+    // only cost throughput) and the team finishes the pair sooner.  Its
+    // warps take the strips round robin, each starting about kTeamLagSteps
+    // behind the warp before it.
+    const int tc = bp.team_cls;
+    if (tc >= 0 && bestLat > kTeamLatencyShare * batch_ps) {
+      const int strips = (alen + bp.width[tc] - 1) / bp.width[tc];
+      if (strips >= 2) {
+        const int rounds = (strips + bp.team_warps - 1) / bp.team_warps;
+        const float lat = ((float)rounds * (float)(blen + bp.lanes[tc]) +
+                           kTeamLagSteps * (float)(min(strips, bp.team_warps) - 1)) *
+                          bp.step_ps[tc];
+        if (lat < bestLat) cls = tc;
+      }
+    }
   }
   const int strips = (alen + bp.width[cls] - 1) / bp.width[cls];
   if (cost_out)

@@ -57,7 +57,8 @@ KERNEL_NAMES = {0: "k_batched<s32,L32,K16>", 1: "k_batched<s16x2,L16,K4>",
                 19: "k_batched<s16x2,L16,K15>", 20: "k_hybrid<b16x2->s32,L32,K16>",
                 21: "k_plain16<K>", 22: "k_batched<s16x2,L8,K8>",
                 23: "k_batched<s16x2,L8,K10>", 24: "k_batched<s16x2,L8,K12>",
-                25: "k_batched<s16x2,L8,K14>", 26: "k_batched<s16x2,L8,K16>"}
+                25: "k_batched<s16x2,L8,K14>", 26: "k_batched<s16x2,L8,K16>",
+                27: "k_strips<s16x2,L32,K16> team"}
 MAX_TIMED = 24  # IPUMA_MAX_TIMED
 
 
