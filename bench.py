@@ -74,6 +74,9 @@ def parse(argv=None):
                     help="arrival window of each offered-load point")
     ap.add_argument("--target-reps", type=int, default=3,
                     help="timed replays per arm of each protein target")
+    ap.add_argument("--long-pairs-only", action="store_true",
+                    help="print only the strip-team comparison on the small batch of long "
+                         "pairs (one JSON object; the case of its ncu summary)")
     ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
                     help="engine option (ipuma_gpu_set_option) for the batched engines")
     return ap.parse_args(argv)
@@ -597,6 +600,10 @@ def main(argv=None):
         return launch_ranks(args, argv)
     if args.impl == "reference":
         return run_reference(args)
+    if args.long_pairs_only:
+        import ipuma_b200 as ib
+        print(json.dumps(long_pair_target(ib)), flush=True)
+        return 0
 
     ws, rank, local = dist_env()
     for kv in args.option:

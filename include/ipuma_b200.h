@@ -185,7 +185,7 @@ typedef struct ipuma_stats {
 #define IPUMA_KERNEL_S16_L8_K14 25
 #define IPUMA_KERNEL_S16_L8_K16 26
 #define IPUMA_KERNEL_S16_TEAM 27   /* s16x2, 512-column strips shared by a team of warps (one block per
-                                      two pairs; forward-only engines, long pairs) */
+                                      two pairs; long pairs of small batches) */
 
 typedef struct ipuma_engine ipuma_engine;
 
@@ -235,8 +235,7 @@ void ipuma_gpu_destroy(ipuma_engine* e);
  *                 IPUMA_KERNEL_S16_L16_K6, _K10, _K14, 11 .. 16 =
  *                 IPUMA_KERNEL_S16_L16_K5, _K7, _K9, _K11, _K13, _K15,
  *                 17 .. 21 = IPUMA_KERNEL_S16_L8_K8, _K10, _K12, _K14, _K16,
- *                 24 = every pair through strip teams (IPUMA_KERNEL_S16_TEAM;
- *                 forward-only engines)
+ *                 24 = every pair through strip teams (IPUMA_KERNEL_S16_TEAM)
  *   "concurrent"  3 = by batch size (default): mode 1 below 48,000 pairs,
  *                 mode 2 above; 2 = class launches alternate between two
  *                 streams, so each starts on the SMs the previous one
@@ -259,17 +258,17 @@ void ipuma_gpu_destroy(ipuma_engine* e);
  *                 as usual (ipuma_stats trace_*)
  *   "autotune"    1 = measure the kernel-class rates before the first batch
  *                 (default), 0 = built-in rates unless ipuma_gpu_autotune
- *   "long_a"      |A| above which a pair takes the widest s16x2 class, or a
- *                 strip team (default 3072): long pairs are latency-bound
+ *   "long_a"      |A| above which a pair takes the widest s16x2 class
+ *                 (default 3072): long pairs are latency-bound
  *   "team_warps"  warps of a strip team (IPUMA_KERNEL_S16_TEAM): 2..8
  *                 (default 8; fewer when the batch's longest A has fewer
  *                 512-column strips or the shared memory holds fewer),
- *                 0 = no teams.  Forward-only engines: a team's warps take
- *                 the strips of one pair couple round robin, so a long pair
- *                 finishes up to that many times sooner; the cost model
- *                 sends a pair there when |A| > long_a, or when no one-warp
- *                 class keeps it under latency_share and a team finishes it
- *                 sooner
+ *                 0 = no teams.  A team's warps take the strips of one pair
+ *                 couple round robin (forward pass, then the reverse pass
+ *                 for start coordinates), so a long pair finishes up to that
+ *                 many times sooner; the cost model sends a pair there when
+ *                 its one-warp latency exceeds half of the batch's modelled
+ *                 time and a team finishes it sooner
  *   "chunks"      ipuma_gpu_compare(_packed) only: 0 = split large batches into up
  *                 to 8 chunks whose uploads overlap the alignment of the
  *                 previous chunks (default), 1 = upload everything first,

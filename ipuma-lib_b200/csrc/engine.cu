@@ -120,11 +120,10 @@ constexpr int kClsS32 = kNumS16;
 // Hybrid class: pairs whose score can pass int16 (main-diagonal bound) run
 // their safe strips in s16x2 and the rest in s32 (option "hybrid").
 constexpr int kClsHi = kNumS16 + 1;
-// Strip-team class (k_strips<16>, forward-only engines): the warps of a
-// block share one item's 512-column strips, so a long pair finishes up to
-// `warps` times sooner.  Chosen for pairs of at least two strips whose
-// one-warp latency the batch cannot hide (pair_key), and for |A| above
-// long_a.  Warps per team: option "team_warps" (0 = off), capped by the
+// Strip-team class (k_strips<16>): the warps of a block share one item's
+// 512-column strips, so a long pair finishes up to `warps` times sooner.
+// Chosen for pairs of at least two strips whose one-warp latency the batch
+// cannot hide (pair_key).  Warps per team: option "team_warps" (0 = off), capped by the
 // batch's strip count.
 constexpr int kClsTeam = kNumS16 + 2;
 constexpr int kTeamWarpsDefault = 8;
@@ -368,11 +367,12 @@ constexpr int kTeamStaticSmem = 1024;
 
 // Warps of a strip team for a batch whose longest A is maxA, with a
 // P-letter profile: the engine's team_warps, but no more than the strips
-// of that A (a warp without a strip would idle for the whole item) and no
-// more than the shared memory holds.  0: no team (fewer than 2 warps).
+// of that A (a warp without a strip would idle for the whole item; two at
+// least) and no more than the shared memory holds.  0: no team (the option
+// is 0, or two warps do not fit).
 int team_warps_for(const ipuma_engine* e, int P, int maxA) {
   const int strips = (std::max(maxA, 1) + kClasses[kClsTeam].width - 1) / kClasses[kClsTeam].width;
-  int w = std::min({e->team_warps, strips, kTeamMaxWarps});
+  int w = std::min({e->team_warps, std::max(strips, 2), kTeamMaxWarps});
   while (w >= 2 && team_smem(e, P, w) + kTeamStaticSmem > e->smem_optin) --w;
   return w >= 2 ? w : 0;
 }
@@ -704,9 +704,14 @@ int run_batched(ipuma_engine* e, const RunBufs& rb, cudaStream_t s, const uint8_
     for (const auto& w : kNarrowPairs)
       if ((enabled >> w[0]) & 1u) enabled = (enabled & ~(1u << w[0])) | (1u << w[1]);
   }
-  // Strip teams: forward-only engines, batches with pairs of two strips or more.
-  const int teamW = (e->sc.forwardOnly && e->team_warps >= 2) ? team_warps_for(e, sc.P, maxA) : 0;
-  if (teamW >= 2 && maxA > kClasses[kClsTeam].width) enabled |= 1u << kClsTeam;
+  // Strip teams: batches with pairs of two strips or more, unless tile_k
+  // forces another class (then no pair could reach a team).
+  const bool teamForced = e->tile_k == kClsTeam + 1;
+  const int teamW = e->team_warps >= 2 ? team_warps_for(e, sc.P, maxA) : 0;
+  if (teamForced && teamW < 2)
+    return fail(IPUMA_ERR_INVALID_ARG, "tile_k %d (strip teams) needs team_warps >= 2 and room for two warps",
+                kClsTeam + 1);
+  if (teamW >= 2 && maxA > kClasses[kClsTeam].width && e->tile_k == 0) enabled |= 1u << kClsTeam;
   if (e->tile_k > 0) enabled |= 1u << (e->tile_k - 1);
   bp.enabled = enabled;
   bp.team_cls = ((enabled >> kClsTeam) & 1u) ? kClsTeam : -1;
@@ -1737,8 +1742,6 @@ int ipuma_gpu_set_option(ipuma_engine* e, const char* name, int64_t value) {
     if (value < 0 || (value > kNumS16 && value != kClsTeam + 1))
       return fail(IPUMA_ERR_INVALID_ARG, "tile_k must be 0 (automatic), a kernel class 1..%d or %d (strip teams)",
                   kNumS16, kClsTeam + 1);
-    if (value == kClsTeam + 1 && !e->sc.forwardOnly)
-      return fail(IPUMA_ERR_INVALID_ARG, "tile_k %d (strip teams) needs a forward-only engine", kClsTeam + 1);
     e->tile_k = (int)value;
   } else if (k == "team_warps") {
     if (value != 0 && (value < 2 || value > kTeamMaxWarps))

@@ -510,7 +510,7 @@ __device__ __forceinline__ bool sw_pass(const SwConst& sc, uint8_t* s_prof, cons
                                         uint16_t* s_bring, const PassSeq (&ps)[T::NP], int2* scr,
                                         long rowsCap, Best (&out)[T::NP], PassCtl* ctl = nullptr,
                                         PassStop stop = PassStop{}, StripTeam team = StripTeam{}) {
-  static_assert(!TEAM || (LANES == 32 && !HYB && !EARLY), "strip teams run whole-warp forward passes");
+  static_assert(!TEAM || (LANES == 32 && !HYB && !EARLY), "strip teams run whole-warp passes without an early stop");
   using V = typename T::V;
   constexpr int SW = LANES * K;          // columns per strip
   constexpr int KP = ProfileWords<K>::KP;

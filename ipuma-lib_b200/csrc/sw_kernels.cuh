@@ -20,8 +20,7 @@
 //   k_strips<K>       the strip-team kernel: the warps of a block share the
 //                     strips of one item (two pairs in s16x2 halves), each
 //                     strip waiting on the boundary rows of the one before
-//                     (forward pass; long pairs whose latency would end
-//                     the launch).
+//                     (long pairs whose latency would end the launch).
 //   k_bin_*           the cost-binning pre-pass that orders the work list:
 //                     k_bin_total (batch cells), k_bin_bound (main-diagonal
 //                     bounds of the long pairs, a warp per pair), k_bin_count
@@ -376,13 +375,13 @@ __global__ void __launch_bounds__(128, (FWD && !HYB) ? 4 : 3) k_batched(SwConst 
   if (trace && lane32 == 0) atomicMax(&trace[1], global_ns());
 }
 
-// Strip-team kernel (forward pass only): the blockDim.x / 32 warps of a
-// block align one item -- the two pairs of a 32-lane s16x2 group -- taking
+// Strip-team kernel: the blockDim.x / 32 warps of a block align one item -- the two pairs of a 32-lane s16x2 group -- taking
 // its 32 * K wide strips round robin (sw_pass with TEAM), so a long pair
 // finishes up to `warps` times sooner than on one warp.  Each warp keeps
 // the best cell of its own strips; the block merges them with the
 // first-strict-maximum order (better), which is the order-independent
-// total order the one-warp pass applies strip by strip.  A team that gave
+// total order the one-warp pass applies strip by strip.  With start
+// coordinates the team then runs the reverse pass the same way.  A team that gave
 // up (a 16-bit overflow, or a wait past kTeamWaitNs, which also sets
 // ERR_WAIT) sends both pairs to the s32 rerun.  Block scratch: `warps`
 // boundary columns of rowsCap rows.
@@ -407,6 +406,8 @@ __global__ void __launch_bounds__(256, 2) k_strips(SwConst sc, const int8_t* __r
   __shared__ int s_prog[kTeamMaxWarps];
   __shared__ int s_abort, s_item;
   __shared__ Best s_res[kTeamMaxWarps][NP];
+  __shared__ Best s_best[2][NP];  // merged best of the forward / reverse pass
+  __shared__ bool s_ovf[NP];
   const int warps = blockDim.x >> 5;
   const int wib = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -451,28 +452,62 @@ __global__ void __launch_bounds__(256, 2) k_strips(SwConst sc, const int8_t* __r
       const bool empty = d[h].a_len <= 0 || d[h].b_len <= 0;
       ps[h] = PassSeq{codes, d[h].a_off, d[h].b_off, empty ? 0 : d[h].a_len, empty ? 0 : d[h].b_len, 1, 1};
     }
-    Best out[NP];
-    sw_pass<T, K, 32, false, false, true>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, out, nullptr,
-                                          PassStop{}, team);
-    if (lane == 0) {
+    // Pass 0: forward.  Pass 1 (with start coordinates): the same pass over
+    // the reversed reads from each pair's end cell (as align_pairs, without
+    // the early stop), whose first strict maximum gives the start.  One
+    // copy of sw_pass serves both.
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass) {
+      Best out[NP];
+      sw_pass<T, K, 32, false, false, true>(sc, s_prof, s_simp, s_bring, ps, scr, rowsCap, out, nullptr,
+                                            PassStop{}, team);
+      if (lane == 0) {
 #pragma unroll
-      for (int h = 0; h < NP; ++h) s_res[wib][h] = out[h];
-    }
-    __syncthreads();
-    if (threadIdx.x < NP) {
-      const int h = threadIdx.x;
-      if (pid[h] >= 0) {
+        for (int h = 0; h < NP; ++h) s_res[wib][h] = out[h];
+      }
+      __syncthreads();
+      if (threadIdx.x < NP) {
+        const int h = threadIdx.x;
         Best b = s_res[0][h];
         for (int w = 1; w < warps; ++w) {
           const Best c = s_res[w][h];
           if (better(c.s, c.i, c.j, b.s, b.i, b.j)) b = c;
         }
-        if (s_abort != 0 || b.s > Cell<T>::limit(sc)) {
+        s_best[pass][h] = b;
+        // A team that gave up (in either pass) sends the pair to the rerun.
+        if (pass == 0) {
+          s_ovf[h] = s_abort != 0 || b.s > Cell<T>::limit(sc);
+          s_best[1][h] = Best{0, 0, 0};  // the start of a pair without a reverse pass
+        }
+        if (pass == 1 && s_abort != 0) s_ovf[h] = true;
+      }
+      __syncthreads();
+      if (pass == 1 || sc.forwardOnly) break;
+      bool any = false;
+#pragma unroll
+      for (int h = 0; h < NP; ++h) {
+        const Best fw = s_best[0][h];
+        const bool run = pid[h] >= 0 && !s_ovf[h] && fw.s > 0;
+        any |= run;
+        ps[h] = run ? PassSeq{codes, d[h].a_off + fw.j, d[h].b_off + fw.i, fw.j + 1, fw.i + 1, -1, -1}
+                    : PassSeq{codes, d[h].a_off, d[h].b_off, 0, 0, 1, 1};
+      }
+      if (!any) break;  // block-uniform: every thread read the same words
+      // A fresh team for the reverse pass (after every warp read s_ovf).
+      __syncthreads();
+      if (threadIdx.x == 0) s_abort = 0;
+      if (threadIdx.x < warps) s_prog[threadIdx.x] = -1;
+      __syncthreads();
+    }
+    if (threadIdx.x < NP) {
+      const int h = threadIdx.x;
+      if (pid[h] >= 0) {
+        if (s_ovf[h]) {
           const int slot = atomicAdd(&st->overflow_count, 1);
           overflow_list[slot] = pid[h];
           if (rerun_cells) atomicAdd(rerun_cells, (unsigned long long)d[h].a_len * (unsigned long long)d[h].b_len);
         } else {
-          write_result(sc, b, Best{0, 0, 0}, score, arange, brange, pid[h]);
+          write_result(sc, s_best[0][h], s_best[1][h], score, arange, brange, pid[h]);
         }
       }
     }

@@ -1,8 +1,8 @@
 """Strip teams (k_strips<16>): the warps of a block share one item's strips.
 
-Every case calls through the C ABI and compares score and end coordinates
-of every pair with the oracle (forward pass; teams run on forward-only
-engines).  Option tile_k = 24 forces every s16x2 pair into the team class;
+Every case calls through the C ABI and compares score, end coordinates
+and (with the reverse pass) start coordinates of every pair with the
+oracle.  Option tile_k = 24 forces every s16x2 pair into the team class;
 without it the cost model picks teams for long pairs of small batches.
 """
 import time
@@ -79,13 +79,15 @@ def _long_pairs(rng, n, letters, a_lo, a_hi, b_lo, b_hi, related=0.5):
     return a_list, b_list
 
 
+@pytest.mark.parametrize("forward_only", [True, False])
 @pytest.mark.parametrize("warps", [2, 3, 8])
-def test_forced_team_protein_parity(warps):
+def test_forced_team_protein_parity(warps, forward_only):
     """Every pair through strip teams of 2, 3 and 8 warps: ragged couples
     (the two pairs of an item differ in both lengths), pairs of one strip
     (the other warps idle), an odd pair count (the last item holds one
     pair), and a repeat whose two equal maxima lie in different strips
-    (the first in row-major order must win)."""
+    (the first in row-major order must win); forward pass alone and with
+    the reverse pass."""
     rng = np.random.default_rng(700 + warps)
     a_list, b_list = _long_pairs(rng, 36, 20, 513, 3800, 40, 1400)
     short_a, short_b = _long_pairs(rng, 4, 20, 100, 512, 100, 600)
@@ -98,15 +100,16 @@ def test_forced_team_protein_parity(warps):
     codes, a_off, a_len, b_off, b_len = oracle.pack_pairs(a_list, b_list)
     pairs = ib.make_pairs(a_off, a_len, b_off, b_len)
     assert pairs.shape[0] % 2 == 1
-    with _engine(PROTEIN, tile_k=TEAM_TILE_K, team_warps=warps) as e:
+    with _engine(PROTEIN, forward_only, tile_k=TEAM_TILE_K, team_warps=warps) as e:
         got = e.compare(codes, pairs)
-    want = _oracle(PROTEIN, codes, pairs)
-    _assert_same(got, want, "team of %d" % warps)
+    want = _oracle(PROTEIN, codes, pairs, forward_only)
+    _assert_same(got, want, "team of %d, forward_only=%s" % (warps, forward_only))
     # The repeat: equal maxima in columns 699 and 1699; the first one wins.
     assert got[0][-1] == want[0][-1] and (got[1][-1] >> 16) == 699
 
 
-def test_forced_team_dna_bytes_and_2bit():
+@pytest.mark.parametrize("forward_only", [True, False])
+def test_forced_team_dna_bytes_and_2bit(forward_only):
     """DNA through teams of 8: byte codes (16-letter profile) and 2-bit
     packed codes (four-row profile)."""
     rng = np.random.default_rng(711)
@@ -115,14 +118,15 @@ def test_forced_team_dna_bytes_and_2bit():
     b_list = [x + 1 for x in b_list]
     codes, a_off, a_len, b_off, b_len = oracle.pack_pairs(a_list, b_list)
     pairs = ib.make_pairs(a_off, a_len, b_off, b_len)
-    want = _oracle(DNA, codes, pairs)
-    with _engine(DNA, tile_k=TEAM_TILE_K, team_warps=8) as e:
+    want = _oracle(DNA, codes, pairs, forward_only)
+    with _engine(DNA, forward_only, tile_k=TEAM_TILE_K, team_warps=8) as e:
         _assert_same(e.compare(codes, pairs), want, "dna bytes")
         packed = ib.pack_codes(codes, 2)
         _assert_same(e.compare_packed(packed, codes.size, pairs, bits=2), want, "dna 2-bit")
 
 
-def test_team_overflow_goes_to_the_s32_rerun():
+@pytest.mark.parametrize("forward_only", [True, False])
+def test_team_overflow_goes_to_the_s32_rerun(forward_only):
     """A near-identical pair shifted by 500 residues: its main diagonal is
     unrelated (no diagonal bound sends it to 32 bits), so it runs in a
     team, passes int16 there, and the s32 rerun gives the exact result."""
@@ -133,9 +137,9 @@ def test_team_overflow_goes_to_the_s32_rerun():
     a2, b2 = _long_pairs(rng, 3, 20, 3500, 4000, 1000, 2000)
     codes, a_off, a_len, b_off, b_len = oracle.pack_pairs([a] + a2, [b] + b2)
     pairs = ib.make_pairs(a_off, a_len, b_off, b_len)
-    want = _oracle(PROTEIN, codes, pairs)
+    want = _oracle(PROTEIN, codes, pairs, forward_only)
     assert want[0][0] > 32767
-    with _engine(PROTEIN, team_warps=8, time_launches=1) as e:
+    with _engine(PROTEIN, forward_only, team_warps=8, time_launches=1) as e:
         got = e.compare(codes, pairs)
         st = e.stats()
     _assert_same(got, want, "team overflow")
@@ -145,19 +149,20 @@ def test_team_overflow_goes_to_the_s32_rerun():
 
 
 def test_cost_model_picks_teams_for_a_small_batch_of_long_pairs():
-    """Without forcing: |A| above long_a sends s16x2 pairs to teams on a
-    forward-only engine, never on an engine with start coordinates."""
+    """Without forcing: a batch of twelve long pairs, whose one-warp
+    latency is most of the batch's time, runs in teams, with and without
+    start coordinates; with team_warps 0 it does not."""
     rng = np.random.default_rng(713)
     a_list, b_list = _long_pairs(rng, 12, 20, 3200, 6000, 2000, 5000)
     codes, a_off, a_len, b_off, b_len = oracle.pack_pairs(a_list, b_list)
     pairs = ib.make_pairs(a_off, a_len, b_off, b_len)
-    for fwd in (True, False):
-        with _engine(PROTEIN, fwd, time_launches=1) as e:
+    for fwd, warps in ((True, 8), (False, 8), (True, 0)):
+        with _engine(PROTEIN, fwd, time_launches=1, team_warps=warps) as e:
             got = e.compare(codes, pairs)
             st = e.stats()
-        _assert_same(got, _oracle(PROTEIN, codes, pairs, fwd), "auto fwd=%s" % fwd)
+        _assert_same(got, _oracle(PROTEIN, codes, pairs, fwd), "auto fwd=%s warps=%d" % (fwd, warps))
         team = [st.timed_cells[k] for k in range(st.n_timed) if st.timed_kind[k] == KIND_TEAM]
-        if fwd:
+        if warps:
             assert team and sum(team) == int((pairs["a_len"].astype(np.int64) * pairs["b_len"]).sum())
         else:
             assert not team
@@ -170,9 +175,10 @@ def test_team_options_are_checked():
                 e.set_option("team_warps", bad)
         e.set_option("team_warps", 0)
         e.set_option("team_warps", 4)
-    with _engine(PROTEIN, forward_only=False) as e:
-        with pytest.raises(ib.IpumaError):
-            e.set_option("tile_k", TEAM_TILE_K)
+        for bad in (22, 23, 25):
+            with pytest.raises(ib.IpumaError):
+                e.set_option("tile_k", bad)
+        e.set_option("tile_k", TEAM_TILE_K)
 
 
 def test_teams_shorten_a_small_batch_of_long_pairs():
@@ -198,3 +204,21 @@ def test_teams_shorten_a_small_batch_of_long_pairs():
         assert np.array_equal(g, w)
     print("64 pairs 6000 x 6000: one warp %.1f ms, teams of 8 %.1f ms" % (ms[0], ms[8]))
     assert ms[8] * 2.0 < ms[0]
+
+
+def test_forced_team_on_short_pairs_and_without_warps():
+    """tile_k 24 on a batch of one-strip pairs runs teams of two (one warp
+    idles); with team_warps 0 the forced class has no warps and the call is
+    refused."""
+    rng = np.random.default_rng(715)
+    a_list, b_list = _long_pairs(rng, 9, 20, 30, 512, 30, 400)
+    codes, a_off, a_len, b_off, b_len = oracle.pack_pairs(a_list, b_list)
+    pairs = ib.make_pairs(a_off, a_len, b_off, b_len)
+    with _engine(PROTEIN, False, tile_k=TEAM_TILE_K, time_launches=1) as e:
+        got = e.compare(codes, pairs)
+        st = e.stats()
+    _assert_same(got, _oracle(PROTEIN, codes, pairs, False), "short pairs in teams")
+    assert KIND_TEAM in [st.timed_kind[k] for k in range(st.n_timed)]
+    with _engine(PROTEIN, tile_k=TEAM_TILE_K, team_warps=0) as e:
+        with pytest.raises(ib.IpumaError):
+            e.compare(codes, pairs)
