@@ -375,16 +375,16 @@ __global__ void __launch_bounds__(128, (FWD && !HYB) ? 4 : 3) k_batched(SwConst 
   if (trace && lane32 == 0) atomicMax(&trace[1], global_ns());
 }
 
-// Strip-team kernel: the blockDim.x / 32 warps of a block align one item -- the two pairs of a 32-lane s16x2 group -- taking
-// its 32 * K wide strips round robin (sw_pass with TEAM), so a long pair
-// finishes up to `warps` times sooner than on one warp.  Each warp keeps
-// the best cell of its own strips; the block merges them with the
-// first-strict-maximum order (better), which is the order-independent
-// total order the one-warp pass applies strip by strip.  With start
-// coordinates the team then runs the reverse pass the same way.  A team that gave
-// up (a 16-bit overflow, or a wait past kTeamWaitNs, which also sets
-// ERR_WAIT) sends both pairs to the s32 rerun.  Block scratch: `warps`
-// boundary columns of rowsCap rows.
+// Strip-team kernel: the blockDim.x / 32 warps of a block align one item
+// (the two pairs of a 32-lane s16x2 group), taking its 32 * K wide strips
+// round robin (sw_pass with TEAM), so a long pair finishes up to `warps`
+// times sooner than on one warp.  Each warp keeps the best cell of its own
+// strips; the block merges them with the first-strict-maximum order
+// (better), the order-independent total order the one-warp pass applies
+// strip by strip.  With start coordinates the team then runs the reverse
+// pass the same way.  A team that gave up (a 16-bit overflow, or a wait
+// past kTeamWaitNs, which also sets ERR_WAIT) sends both pairs to the s32
+// rerun.  Block scratch: `warps` boundary columns of rowsCap rows.
 constexpr int kTeamMaxWarps = 8;
 template <int K>
 __global__ void __launch_bounds__(256, 2) k_strips(SwConst sc, const int8_t* __restrict__ sim,
