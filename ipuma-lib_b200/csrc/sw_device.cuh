@@ -29,8 +29,10 @@
 // t) and the left neighbour's last-column (HG, E) arrives through
 // __shfl_up_sync.  A longer than one strip is processed strip by strip; the
 // last column of a strip is handed to the next one through per-warp global
-// scratch.  Substitution scores come from a per-strip query profile in
-// shared memory (int8, one row per B letter plus a padding row).
+// scratch (a strip team, StripTeam, spreads one couple's strips over the
+// warps of a block instead).  Substitution scores come from a per-strip
+// query profile in shared memory (int8, one row per B letter plus a
+// padding row).
 //
 // Invalid cells (columns past |A|, rows past |B| of the shorter pair of an
 // s16x2 couple) get the profile value SUB_PAD.  With gI + gE < 0 and
