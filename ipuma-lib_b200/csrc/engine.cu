@@ -1846,7 +1846,7 @@ static int compare_dev(ipuma_engine* e, const uint8_t* d_codes, size_t n_codes, 
                                        (uint64_t)(uintptr_t)e->d_ovf.p, (uint64_t)(uintptr_t)e->d_flag.p,
                                        (uint64_t)e->tile_k, (uint64_t)e->long_a, (uint64_t)e->thread_class,
                                        (uint64_t)e->concurrent, (uint64_t)e->hybrid, (uint64_t)e->trace,
-                                       (uint64_t)(e->latency_share * 1e6f)};
+                                       (uint64_t)(e->latency_share * 1e6f), (uint64_t)e->team_warps};
     auto it = e->graphs_cache.find(key);
     if (it == e->graphs_cache.end()) {
       if (e->graphs_cache.size() >= 16) {
